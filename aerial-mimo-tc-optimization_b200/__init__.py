@@ -1,0 +1,242 @@
+"""B200-native PUSCH receiver equalization path (host-side mirror of the C ABI).
+
+The shared library ``libaerial_eq.so`` (built from ``csrc/`` for sm_100a by the
+``Makefile`` in this directory) holds every kernel; this module only binds its
+C ABI (``include/aerial_eq.h``) with ctypes and passes torch CUDA tensors'
+device pointers and the current stream.  There is no CPU fallback: if the
+library is missing or a call fails, an exception is raised.
+
+Function names and argument order mirror the reference's kernel entries
+(ebaenamar/aerial-mimo-tc-optimization):
+
+  coef_apply(C, Y_rx, Y_eq, nSC, nSym, ...)   coef_apply_v1_scalar, src/aerial_coef_wmma.cu:71-75
+  coef_apply_tc(...)                          coef_apply_v2_wmma,   src/aerial_coef_wmma.cu:146-150
+  gram(H, sigma2, G, nSC, ...)                gram_scalar,          src/aerial_bottleneck.cu:56-60
+  llr(softEst, noiseInv, llrOut, N, nPamBits) llr_v1_baseline,      src/llr/aerial_llr_v3.cu:84-86
+  srs_filter(H_est, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen)
+                                              srs_filter_v1_scalar, src/srs/srs_wmma_bench.cu:57-63
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libaerial_eq.so")
+
+AERIAL_OK = 0
+PREC_FP16, PREC_BF16, PREC_BF16X3, PREC_FP32 = 0, 1, 2, 3
+PREC_NAMES = {"fp16": PREC_FP16, "bf16": PREC_BF16, "bf16x3": PREC_BF16X3, "fp32": PREC_FP32}
+MAX_CELLS = 64
+
+
+class AerialError(RuntimeError):
+    """A non-zero status from the C ABI (the reference would exit(1) here)."""
+
+    def __init__(self, status: int, where: str):
+        self.status = status
+        msg = _lib_handle().aerial_error_string(status).decode() if _LIB is not None else str(status)
+        super().__init__(f"{where}: status {status}: {msg}")
+
+
+class CellDesc(ctypes.Structure):
+    """``aerial_cell_desc``: one cell-slot of the fused chain."""
+
+    _fields_ = [
+        ("H", ctypes.c_void_p),
+        ("Y_rx", ctypes.c_void_p),
+        ("llr", ctypes.c_void_p),
+        ("Y_eq", ctypes.c_void_p),
+        ("sigma2", ctypes.c_float),
+        ("nPRB", ctypes.c_int),
+        ("nAnt", ctypes.c_int),
+        ("nLayers", ctypes.c_int),
+        ("nSym", ctypes.c_int),
+        ("nPamBits", ctypes.c_int),
+    ]
+
+
+class Tuning(ctypes.Structure):
+    """``aerial_tuning``: operand precision and launch shape (0 = default)."""
+
+    _fields_ = [
+        ("precision", ctypes.c_int),
+        ("warps_per_cta", ctypes.c_int),
+        ("ctas_per_sm", ctypes.c_int),
+        ("sc_per_group", ctypes.c_int),
+    ]
+
+
+_LIB = None
+
+# exported symbol -> (restype, argtypes)
+_P, _I, _F, _Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_size_t
+SIGNATURES = {
+    "aerial_error_string": (ctypes.c_char_p, [_I]),
+    "aerial_version": (_I, []),
+    "aerial_coef_apply": (_I, [_P, _P, _P, _I, _I, _I, _I, _P]),
+    "aerial_coef_apply_tc": (_I, [_P, _P, _P, _I, _I, _I, _I, _P]),
+    "aerial_gram": (_I, [_P, _F, _P, _I, _I, _I, _P]),
+    "aerial_mmse_coef": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
+    "aerial_llr": (_I, [_P, _P, _P, _I, _I, _P]),
+    "aerial_llr_f32": (_I, [_P, _P, _P, _I, _I, _I, _P]),
+    "aerial_srs_filter": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
+    "aerial_srs_to_channel": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
+    "aerial_pusch_eq_fused": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), _P]),
+    "aerial_pusch_eq_plain_workspace": (_Z, [ctypes.POINTER(CellDesc), _I]),
+    "aerial_pusch_eq_plain": (_I, [ctypes.POINTER(CellDesc), _I, _P, _Z, _P]),
+    "aerial_autotune": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), ctypes.POINTER(_F), _P]),
+}
+
+
+def _lib_handle():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build the CUDA library first "
+                f"(make -C {_HERE}); there is no CPU fallback")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def lib():
+    """The loaded ``libaerial_eq.so`` (ctypes handle)."""
+    return _lib_handle()
+
+
+def _check(status: int, where: str) -> None:
+    if status != AERIAL_OK:
+        raise AerialError(status, where)
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor (device memory)")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+# ---------------------------------------------------------------------------
+# per-stage entry points (reference kernel names)
+# ---------------------------------------------------------------------------
+
+def coef_apply(C, Y_rx, Y_eq, nSC, nSym, nLayers, nAnt, stream=None):
+    """Y_eq[sc][l][s] = sum_a C[sc][l][a] Y_rx[sc][s][a] (FP32, bit-exact V1)."""
+    _check(lib().aerial_coef_apply(_ptr(C), _ptr(Y_rx), _ptr(Y_eq), nSC, nSym, nLayers, nAnt, _stream(stream)),
+           "coef_apply")
+
+
+def coef_apply_tc(C, Y_rx, Y_eq, nSC, nSym, nLayers, nAnt, stream=None):
+    """coef_apply on the tensor cores (FP16 operands, FP32 accumulation)."""
+    _check(lib().aerial_coef_apply_tc(_ptr(C), _ptr(Y_rx), _ptr(Y_eq), nSC, nSym, nLayers, nAnt,
+                                      _stream(stream)), "coef_apply_tc")
+
+
+def gram(H, sigma2, G, nSC, nAnt, nLayers, stream=None):
+    """G[sc] = H[sc]^H H[sc] + sigma2 I (FP32)."""
+    _check(lib().aerial_gram(_ptr(H), float(sigma2), _ptr(G), nSC, nAnt, nLayers, _stream(stream)), "gram")
+
+
+def mmse_coef(G, H, C, noiseInv, nSC, nAnt, nLayers, stream=None):
+    """C = diag(1/mu) G^-1 H^H and noiseInv = mu/(1-mu) per (sc, layer) (FP32 Cholesky)."""
+    _check(lib().aerial_mmse_coef(_ptr(G), _ptr(H), _ptr(C), _ptr(noiseInv), nSC, nAnt, nLayers,
+                                  _stream(stream)), "mmse_coef")
+
+
+def llr(softEst, noiseInv, llrOut, N, nPamBits, stream=None):
+    """Max-log PAM LLRs, FP16 in / FP16 out (the reference's I/O, bit-exact)."""
+    _check(lib().aerial_llr(_ptr(softEst), _ptr(noiseInv), _ptr(llrOut), N, nPamBits, _stream(stream)), "llr")
+
+
+def llr_f32(softEst, noiseInv, llrOut, N, nPamBits, nSymPerNoise=1, stream=None):
+    """Max-log PAM LLRs, complex64 in / float32 out; noiseInv[idx // nSymPerNoise]."""
+    _check(lib().aerial_llr_f32(_ptr(softEst), _ptr(noiseInv), _ptr(llrOut), N, nPamBits, nSymPerNoise,
+                                _stream(stream)), "llr_f32")
+
+
+def srs_filter(H_est, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, stream=None):
+    """H_est[blk][ant][k_out][p] = sum_k W[k_out][k] FOCC[p][k%F] SRS[blk][ant][k] (FP16 I/O, FP32 sums)."""
+    _check(lib().aerial_srs_filter(_ptr(H_est), _ptr(SRS), _ptr(W), _ptr(FOCC), nAnt, nBlocks, K, nPorts, foccLen,
+                                   _stream(stream)), "srs_filter")
+
+
+def srs_to_channel(H, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, stream=None):
+    """SRS filter multiply written as the PUSCH channel H[blk*K+k_out][ant][port] (complex64)."""
+    _check(lib().aerial_srs_to_channel(_ptr(H), _ptr(SRS), _ptr(W), _ptr(FOCC), nAnt, nBlocks, K, nPorts, foccLen,
+                                       _stream(stream)), "srs_to_channel")
+
+
+# ---------------------------------------------------------------------------
+# fused chain
+# ---------------------------------------------------------------------------
+
+def cell_desc(H, Y_rx, llr_out, sigma2, nPRB, nAnt, nLayers, nSym, nPamBits, Y_eq=None) -> CellDesc:
+    d = CellDesc()
+    d.H = _ptr(H).value
+    d.Y_rx = _ptr(Y_rx).value
+    d.llr = _ptr(llr_out).value
+    d.Y_eq = _ptr(Y_eq).value if Y_eq is not None else None
+    d.sigma2 = float(sigma2)
+    d.nPRB, d.nAnt, d.nLayers, d.nSym, d.nPamBits = int(nPRB), int(nAnt), int(nLayers), int(nSym), int(nPamBits)
+    return d
+
+
+def _cells_array(cells):
+    n = len(cells)
+    if n < 1 or n > MAX_CELLS:
+        raise ValueError(f"1..{MAX_CELLS} cells per launch, got {n}")
+    arr = (CellDesc * n)(*cells)
+    return arr, n
+
+
+def make_tuning(precision=PREC_FP16, warps_per_cta=0, ctas_per_sm=0) -> Tuning:
+    if isinstance(precision, str):
+        precision = PREC_NAMES[precision]
+    return Tuning(int(precision), int(warps_per_cta), int(ctas_per_sm), 0)
+
+
+def pusch_eq_fused(cells, tuning: Tuning | None = None, stream=None):
+    """Fused Gram -> Cholesky MMSE -> apply -> LLR over all cells in one launch."""
+    arr, n = _cells_array(cells)
+    tp = ctypes.pointer(tuning) if tuning is not None else None
+    _check(lib().aerial_pusch_eq_fused(arr, n, tp, _stream(stream)), "pusch_eq_fused")
+
+
+def pusch_eq_plain_workspace(cells) -> int:
+    arr, n = _cells_array(cells)
+    return int(lib().aerial_pusch_eq_plain_workspace(arr, n))
+
+
+def pusch_eq_plain(cells, workspace, stream=None):
+    """The plain FP32 chain (gram, mmse_coef, coef_apply, llr_f32 per cell)."""
+    arr, n = _cells_array(cells)
+    _check(lib().aerial_pusch_eq_plain(arr, n, _ptr(workspace), workspace.numel() * workspace.element_size(),
+                                       _stream(stream)), "pusch_eq_plain")
+
+
+def autotune(cells, precision=PREC_FP16, stream=None):
+    """Pick the fastest launch shape for these cells; returns (Tuning, microseconds)."""
+    arr, n = _cells_array(cells)
+    t = make_tuning(precision)
+    us = ctypes.c_float(0.0)
+    _check(lib().aerial_autotune(arr, n, ctypes.pointer(t), ctypes.pointer(us), _stream(stream)), "autotune")
+    return t, float(us.value)

@@ -1,0 +1,82 @@
+// common.cuh -- shared device/host helpers of the B200 equalization library.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <cmath>
+
+#include "../../include/aerial_eq.h"
+
+namespace aeq {
+
+using cf = float2;  // {re, im}: the reference's struct cf32 (src/aerial_coef_wmma.cu:60)
+
+// Status helper: map the last launch error to an ABI status.
+inline int launch_status() {
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
+inline cudaStream_t to_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// cma() of src/aerial_coef_wmma.cu:61-64 with the contraction nvcc applies to
+// `acc + a*b - c*d`: re = fma(-a.im, b.im, fma(a.re, b.re, acc.re)),
+// im = fma(a.im, b.re, fma(a.re, b.im, acc.im)).  Written with explicit
+// round-to-nearest fmas so the result does not depend on -fmad.
+__device__ __forceinline__ cf cma(cf a, cf b, cf acc) {
+    cf r;
+    r.x = __fmaf_rn(-a.y, b.y, __fmaf_rn(a.x, b.x, acc.x));
+    r.y = __fmaf_rn(a.y, b.x, __fmaf_rn(a.x, b.y, acc.y));
+    return r;
+}
+
+// Per-dimension Gray-PAM decision distances D_i = 2^(n-1-i) / sqrt(2(4^n-1)/3)
+// of unit-energy QAM with 2n bits; D[n-1] is the half spacing `dist`.
+// (The same values as the LUT of src/llr/aerial_llr_v3.cu:42-49, computed.)
+struct PamLut {
+    float d[4];
+};
+inline PamLut pam_lut(int n) {
+    PamLut p{{0.f, 0.f, 0.f, 0.f}};
+    double norm = std::sqrt(2.0 * (double)((1 << (2 * n)) - 1) / 3.0);
+    float r = (float)(1.0 / norm);
+    for (int i = 0; i < n; i++) p.d[i] = r * (float)(1 << (n - 1 - i));
+    return p;
+}
+
+// Max-log PAM LLRs of one complex symbol, the arithmetic of llr_v1_baseline
+// (src/llr/aerial_llr_v3.cu:90-107): soft-bit chain sb[i+1] = D_i - |sb[i]|,
+// pMD[i] = (dist + |sb[i]|)^2, minDist1 = (|sb[n-1]| - dist)^2,
+// llr_i = +-(pMD[i] - minDist1) * noise, clamped to +-65504.
+// out[2*bit + iq].  Operation order matches the reference (no contraction is
+// possible in it), so results are bit-identical.
+template <int N>
+__device__ __forceinline__ void pam_llr(float pamI, float pamQ, float noise, const PamLut& L,
+                                        float* out) {
+    const float dist = L.d[N - 1];
+#pragma unroll
+    for (int iq = 0; iq < 2; iq++) {
+        float sb = iq == 0 ? pamI : pamQ;
+        float pmd[N];
+        unsigned sign = 0;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            float a = fabsf(sb);
+            float m = __fadd_rn(dist, a);
+            pmd[i] = __fmul_rn(m, m);
+            if (sb < 0.f) sign |= 1u << i;
+            if (i < N - 1) sb = __fsub_rn(L.d[i], a);
+        }
+        float md1 = __fsub_rn(fabsf(sb), dist);
+        md1 = __fmul_rn(md1, md1);
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            float llr = __fmul_rn(__fsub_rn(pmd[i], md1), noise);
+            if (sign & (1u << i)) llr = -llr;
+            out[2 * i + iq] = fmaxf(-65504.f, fminf(65504.f, llr));
+        }
+    }
+}
+
+}  // namespace aeq

@@ -1,0 +1,692 @@
+// fused.cu -- the fused PUSCH equalization kernel: Gram + matched filter on
+// the tensor cores, FP32 Cholesky MMSE solve, unbiasing and max-log LLR, in
+// one persistent launch over any mix of cells.  Only H and Y_rx are read
+// from HBM and only LLRs (optionally Y_eq) are written; G, C and Y_eq stay in
+// registers / shared memory.
+//
+// Formulation (per subcarrier, L layers, A antennas, S symbols):
+//   G = H^H H + s2 I          (L x L, Hermitian)
+//   Z = H^H Y^T               (L x S, the matched filter)
+//   X = G^-1 Z                (= C Y^T with C = G^-1 H^H, C never formed)
+//   mu_l = 1 - s2 (G^-1)_ll ; Y_eq = X / mu ; noiseInv_l = mu_l / (s2 (G^-1)_ll)
+// This is algebraically the reference chain gram -> solve -> coef_apply
+// (src/aerial_bottleneck.cu:56-80, src/aerial_coef_wmma.cu:71-104) followed by
+// computePamLlr (src/llr/aerial_llr_v3.cu:84-108); it replaces the L x A
+// coefficient matrix by an L x S right-hand side (S = 11 << A = 64).
+//
+// Tensor-core mapping (mma.sync m16n8k16, FP32 accumulate).  A complex GEMM
+// out[r][n] = sum_k conj(H[k][r]) B[k][n] is embedded as a real GEMM with
+//   A_emb rows 0..7 = (Re, Im) pairs of H[k][r]       -> Re out
+//   A_emb rows 8..15 = (-Im, Re) pairs of H[k][r]     -> Im out
+//   B_emb = (Re, Im) pairs of B[k][n]
+// and the K index interleaving (k, re/im).  With that choice a thread's A
+// fragment register IS the complex tap H[k][layer] packed as a half2 and its
+// B fragment register IS B[k][n] packed, so operands go from global memory
+// to registers with no shared-memory staging or shuffles.  For the Gram
+// n-tile B = H, i.e. the same registers as A.  Thread (g = lane/4, c = lane%4)
+// covers antennas 8j+2c and 8j+2c+1 of k-step j (the K order is permuted
+// inside each k-step; A and B use the same permutation).
+#include "common.cuh"
+
+namespace aeq {
+
+constexpr int kMaxCells = AERIAL_MAX_CELLS;
+
+struct FusedCell {
+    const float2* H;
+    const float2* Y;
+    float* llr;
+    float2* yeq;
+    long group0;     // first global group index of this cell
+    float sigma2;
+    int nSC, A, L, nSym, nPam, LT, vecY;
+    PamLut lut;
+};
+
+struct FusedParams {
+    FusedCell cell[kMaxCells];
+    int nCells;
+    long totalGroups;
+};
+
+// ---------------------------------------------------------------------------
+// operand packing
+// ---------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ uint32_t pack2(float re, float im) {
+    if constexpr (P == AERIAL_PREC_FP16) {
+        __half2 h = __floats2half2_rn(re, im);
+        return *reinterpret_cast<uint32_t*>(&h);
+    } else {
+        __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+}
+// (re, im) -> (-im, re): swap the halves and flip the sign bit of the new low half.
+__device__ __forceinline__ uint32_t jrot(uint32_t p) { return __byte_perm(p, 0, 0x1032) ^ 0x8000u; }
+
+// bf16 hi/lo split of a complex pair: x = hi + lo to ~16 mantissa bits.
+__device__ __forceinline__ void split_bf16(float re, float im, uint32_t& hi, uint32_t& lo) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
+    float2 hf = __bfloat1622float2(h);
+    __nv_bfloat162 l = __floats2bfloat162_rn(re - hf.x, im - hf.y);
+    hi = *reinterpret_cast<uint32_t*>(&h);
+    lo = *reinterpret_cast<uint32_t*>(&l);
+}
+
+template <int P>
+__device__ __forceinline__ void mma16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+    if constexpr (P == AERIAL_PREC_FP16) {
+        asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    } else {
+        asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+    }
+}
+
+// complex helpers (FP32)
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// acc - a * b
+__device__ __forceinline__ float2 csub_mul(float2 acc, float2 a, float2 b) {
+    return make_float2(acc.x - a.x * b.x + a.y * b.y, acc.y - a.x * b.y - a.y * b.x);
+}
+// acc - conj(a) * b
+__device__ __forceinline__ float2 csub_cmul(float2 acc, float2 a, float2 b) {
+    return make_float2(acc.x - a.x * b.x - a.y * b.y, acc.y - a.x * b.y + a.y * b.x);
+}
+// acc - a * conj(b)
+__device__ __forceinline__ float2 csub_mulc(float2 acc, float2 a, float2 b) {
+    return make_float2(acc.x - a.x * b.x - a.y * b.y, acc.y - a.y * b.x + a.x * b.y);
+}
+
+// ---------------------------------------------------------------------------
+// per-warp shared-memory layout for layer tile LT (GS = 32/LT subcarriers)
+// ---------------------------------------------------------------------------
+template <int LT>
+struct WarpSmem {
+    static constexpr int GS = 32 / LT;
+    static constexpr int GP = LT + 1;           // padded G row (complex)
+    static constexpr int RP = 16 + LT + 1;      // padded RHS row: 16 symbols + LT identity columns
+    static constexpr int offG = 0;                                   // float2 [GS][LT][GP]
+    static constexpr int offR = offG + GS * LT * GP;                 // float2 [GS][LT][RP]
+    static constexpr int offAux = offR + GS * LT * RP;               // float2 [32] column buffer
+    static constexpr int offInv = offAux + 32;                       // float  [32] (as float2 slots: 16)
+    static constexpr int offQ = offInv + 16;                         // float  [GS][LT][LT] (as float2)
+    static constexpr int total = offQ + (GS * LT * LT + 1) / 2;      // in float2 units
+};
+
+__host__ __device__ constexpr int warp_smem_bytes(int LT) {
+    return LT == 1 ? WarpSmem<1>::total * 8
+         : LT == 2 ? WarpSmem<2>::total * 8
+         : LT == 4 ? WarpSmem<4>::total * 8
+         : LT == 8 ? WarpSmem<8>::total * 8
+                   : WarpSmem<16>::total * 8;
+}
+
+// Fragment registers of one chunk (4 k-steps = 32 antennas) of one subcarrier.
+template <int NMT>
+struct Frag {
+    float4 h[NMT][4];   // (H[a0][l], H[a0+1][l]) for l = g + 8*mt
+    float4 y[2][4];     // (Y[8nt+g][a0], Y[8nt+g][a0+1])
+};
+
+template <int NMT>
+__device__ __forceinline__ void load_chunk(Frag<NMT>& f, const FusedCell& cl, long sc, int ch, int nK, int g, int c) {
+    const float2* Hs = cl.H + sc * (long)cl.A * cl.L;
+    const float2* Ys = cl.Y + sc * (long)cl.nSym * cl.A;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+        const int j = ch * 4 + kk;
+        const int a0 = 8 * j + 2 * c;
+        const bool k0 = (j < nK) && (a0 < cl.A), k1 = (j < nK) && (a0 + 1 < cl.A);
+#pragma unroll
+        for (int mt = 0; mt < NMT; mt++) {
+            const int l = g + 8 * mt;
+            float4 v = z4;
+            if (l < cl.L) {
+                if (k0) {
+                    float2 t = __ldg(Hs + (long)a0 * cl.L + l);
+                    v.x = t.x; v.y = t.y;
+                }
+                if (k1) {
+                    float2 t = __ldg(Hs + (long)(a0 + 1) * cl.L + l);
+                    v.z = t.x; v.w = t.y;
+                }
+            }
+            f.h[mt][kk] = v;
+        }
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++) {
+            const int s = 8 * nt + g;
+            float4 v = z4;
+            if (s < cl.nSym) {
+                const float2* p = Ys + (long)s * cl.A + a0;
+                if (cl.vecY && k1) {
+                    v = __ldg(reinterpret_cast<const float4*>(p));
+                } else {
+                    if (k0) { float2 t = __ldg(p); v.x = t.x; v.y = t.y; }
+                    if (k1) { float2 t = __ldg(p + 1); v.z = t.x; v.w = t.y; }
+                }
+            }
+            f.y[nt][kk] = v;
+        }
+    }
+}
+
+// Gram blocks kept: (0,0) for LT <= 8; (0,0), (1,0), (1,1) for LT = 16.
+template <int LT, int P>
+__device__ __forceinline__ void mma_chunk(const Frag<(LT > 8 ? 2 : 1)>& f, float (*gacc)[4], float (*zacc)[2][4],
+                                          int ch, int nK, bool z2) {
+    constexpr int NMT = LT > 8 ? 2 : 1;
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+        if (ch * 4 + kk >= nK) break;
+        if constexpr (P == AERIAL_PREC_BF16X3) {
+            uint32_t ah[NMT][2], al[NMT][2];
+#pragma unroll
+            for (int mt = 0; mt < NMT; mt++) {
+                split_bf16(f.h[mt][kk].x, f.h[mt][kk].y, ah[mt][0], al[mt][0]);
+                split_bf16(f.h[mt][kk].z, f.h[mt][kk].w, ah[mt][1], al[mt][1]);
+            }
+            uint32_t yh[2][2], yl[2][2];
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) {
+                split_bf16(f.y[nt][kk].x, f.y[nt][kk].y, yh[nt][0], yl[nt][0]);
+                split_bf16(f.y[nt][kk].z, f.y[nt][kk].w, yh[nt][1], yl[nt][1]);
+            }
+#pragma unroll
+            for (int mt = 0; mt < NMT; mt++) {
+                const uint32_t h0 = ah[mt][0], h1 = jrot(ah[mt][0]), h2 = ah[mt][1], h3 = jrot(ah[mt][1]);
+                const uint32_t l0 = al[mt][0], l1 = jrot(al[mt][0]), l2 = al[mt][1], l3 = jrot(al[mt][1]);
+#pragma unroll
+                for (int nt = 0; nt <= mt; nt++) {
+                    float* d = gacc[mt + nt];  // blocks (0,0)->0, (1,0)->1, (1,1)->2
+                    mma16816<P>(d, h0, h1, h2, h3, ah[nt][0], ah[nt][1]);
+                    mma16816<P>(d, h0, h1, h2, h3, al[nt][0], al[nt][1]);
+                    mma16816<P>(d, l0, l1, l2, l3, ah[nt][0], ah[nt][1]);
+                }
+#pragma unroll
+                for (int nt = 0; nt < 2; nt++) {
+                    if (nt == 1 && !z2) break;
+                    mma16816<P>(zacc[mt][nt], h0, h1, h2, h3, yh[nt][0], yh[nt][1]);
+                    mma16816<P>(zacc[mt][nt], h0, h1, h2, h3, yl[nt][0], yl[nt][1]);
+                    mma16816<P>(zacc[mt][nt], l0, l1, l2, l3, yh[nt][0], yh[nt][1]);
+                }
+            }
+        } else {
+            uint32_t a[NMT][2];
+#pragma unroll
+            for (int mt = 0; mt < NMT; mt++) {
+                a[mt][0] = pack2<P>(f.h[mt][kk].x, f.h[mt][kk].y);
+                a[mt][1] = pack2<P>(f.h[mt][kk].z, f.h[mt][kk].w);
+            }
+            uint32_t b[2][2];
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) {
+                b[nt][0] = pack2<P>(f.y[nt][kk].x, f.y[nt][kk].y);
+                b[nt][1] = pack2<P>(f.y[nt][kk].z, f.y[nt][kk].w);
+            }
+#pragma unroll
+            for (int mt = 0; mt < NMT; mt++) {
+                const uint32_t a0 = a[mt][0], a1 = jrot(a[mt][0]), a2 = a[mt][1], a3 = jrot(a[mt][1]);
+#pragma unroll
+                for (int nt = 0; nt <= mt; nt++) mma16816<P>(gacc[mt + nt], a0, a1, a2, a3, a[nt][0], a[nt][1]);
+#pragma unroll
+                for (int nt = 0; nt < 2; nt++) {
+                    if (nt == 1 && !z2) break;
+                    mma16816<P>(zacc[mt][nt], a0, a1, a2, a3, b[nt][0], b[nt][1]);
+                }
+            }
+        }
+    }
+}
+
+// Accumulators of subcarrier q of the group -> per-warp shared memory.
+// Fragment (row g, cols 2c, 2c+1) and (row g+8, ...) = Re / Im of
+// out[8mt+g][8nt+2c], out[8mt+g][8nt+2c+1].
+template <int LT>
+__device__ __forceinline__ void store_acc(float2* sm, float (*gacc)[4], float (*zacc)[2][4], int q, int g, int c) {
+    using W = WarpSmem<LT>;
+    constexpr int NMT = LT > 8 ? 2 : 1;
+    float2* sG = sm + W::offG + q * LT * W::GP;
+    float2* sR = sm + W::offR + q * LT * W::RP;
+#pragma unroll
+    for (int mt = 0; mt < NMT; mt++) {
+        const int r = 8 * mt + g;
+#pragma unroll
+        for (int nt = 0; nt <= mt; nt++) {
+            const float* d = gacc[mt + nt];
+            const int n = 8 * nt + 2 * c;
+            if (r < LT && n < LT) sG[r * W::GP + n] = make_float2(d[0], d[2]);
+            if (r < LT && n + 1 < LT) sG[r * W::GP + n + 1] = make_float2(d[1], d[3]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++) {
+            const float* d = zacc[mt][nt];
+            const int s = 8 * nt + 2 * c;
+            if (r < LT) {
+                sR[r * W::RP + s] = make_float2(d[0], d[2]);
+                sR[r * W::RP + s + 1] = make_float2(d[1], d[3]);
+            }
+        }
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void write_llr(float* dst, const float* o) {
+    if constexpr (N == 2) {
+        *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
+    } else if constexpr (N == 4) {
+        *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
+        *reinterpret_cast<float4*>(dst + 4) = make_float4(o[4], o[5], o[6], o[7]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 2 * N; j += 2) *reinterpret_cast<float2*>(dst + j) = make_float2(o[j], o[j + 1]);
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void emit(const FusedCell& cl, long sc, int i, const float2* x, float invMu, float nInv) {
+    float* base = cl.llr + ((sc * cl.L + i) * (long)cl.nSym) * (2 * N);
+    float2* ye = cl.yeq ? cl.yeq + (sc * cl.L + i) * (long)cl.nSym : nullptr;
+#pragma unroll
+    for (int s = 0; s < 16; s++) {
+        if (s < cl.nSym) {
+            const float2 v = make_float2(x[s].x * invMu, x[s].y * invMu);
+            if (ye) ye[s] = v;
+            float o[2 * N];
+            pam_llr<N>(v.x, v.y, nInv, cl.lut, o);
+            write_llr<N>(base + s * 2 * N, o);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// one group of GS subcarriers: MMA phase (whole warp per subcarrier), then the
+// FP32 solve with LT lanes per subcarrier.
+// ---------------------------------------------------------------------------
+template <int LT, int P>
+__device__ __noinline__ void process_group(const FusedCell& cl, long grp, float2* sm, int lane) {
+    using W = WarpSmem<LT>;
+    constexpr int NMT = LT > 8 ? 2 : 1;
+    constexpr int GS = W::GS;
+    const int g = lane >> 2, c = lane & 3;
+    const int nK = (cl.A + 7) >> 3;
+    const int nChunk = (nK + 3) >> 2;
+    const bool z2 = cl.nSym > 8;
+    const long sc0 = grp * GS;
+    const int nValid = (int)min((long)GS, (long)cl.nSC - sc0);
+    const int nItems = nValid * nChunk;
+
+    // ---- MMA phase: software-pipelined over (subcarrier, chunk) items ----
+    {
+        float gacc[NMT == 2 ? 3 : 1][4];
+        float zacc[NMT][2][4];
+#pragma unroll
+        for (int b = 0; b < (NMT == 2 ? 3 : 1); b++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
+#pragma unroll
+        for (int mt = 0; mt < NMT; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
+
+        auto finish = [&](int it) {
+            if ((it % nChunk) == nChunk - 1) {
+                store_acc<LT>(sm, gacc, zacc, it / nChunk, g, c);
+#pragma unroll
+                for (int b = 0; b < (NMT == 2 ? 3 : 1); b++)
+#pragma unroll
+                    for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
+#pragma unroll
+                for (int mt = 0; mt < NMT; mt++)
+#pragma unroll
+                    for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+                        for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
+            }
+        };
+        Frag<NMT> fa, fb;
+        if (nItems > 0) load_chunk<NMT>(fa, cl, sc0, 0, nK, g, c);
+        for (int it = 0; it < nItems; it += 2) {
+            if (it + 1 < nItems) load_chunk<NMT>(fb, cl, sc0 + (it + 1) / nChunk, (it + 1) % nChunk, nK, g, c);
+            mma_chunk<LT, P>(fa, gacc, zacc, it % nChunk, nK, z2);
+            finish(it);
+            if (it + 2 < nItems) load_chunk<NMT>(fa, cl, sc0 + (it + 2) / nChunk, (it + 2) % nChunk, nK, g, c);
+            if (it + 1 < nItems) {
+                mma_chunk<LT, P>(fb, gacc, zacc, (it + 1) % nChunk, nK, z2);
+                finish(it + 1);
+            }
+        }
+    }
+    __syncwarp();
+
+    // ---- solve phase: lane = (q, i), LT lanes per subcarrier ----
+    const int q = lane / LT, i = lane % LT;
+    const long sc = sc0 + q;
+    const bool scValid = q < nValid;
+    const bool real = i < cl.L;          // padded layers (i >= L) carry an identity block
+    float2* sG = sm + W::offG + q * LT * W::GP;
+    float2* sR = sm + W::offR + q * LT * W::RP;
+    float2* sCol = sm + W::offAux + q * LT;
+    float* sInv = reinterpret_cast<float*>(sm + W::offInv) + q * LT;
+    float* sQ = reinterpret_cast<float*>(sm + W::offQ) + q * LT * LT;
+    const float s2 = cl.sigma2;
+
+    // row i of the lower triangle of G (+ s2 on the diagonal)
+    float2 gr[LT];
+#pragma unroll
+    for (int m = 0; m < LT; m++) {
+        float2 v = make_float2(0.f, 0.f);
+        if (m <= i && scValid) v = sG[i * W::GP + m];
+        if (m == i) v = real ? make_float2(v.x + s2, 0.f) : make_float2(1.f, 0.f);
+        if (!real && m < i) v = make_float2(0.f, 0.f);
+        gr[m] = v;
+    }
+    float2 z[16];
+#pragma unroll
+    for (int s = 0; s < 16; s++) z[s] = (s < cl.nSym && scValid && real) ? sR[i * W::RP + s] : make_float2(0.f, 0.f);
+    float2 e[LT];
+#pragma unroll
+    for (int m = 0; m < LT; m++) e[m] = make_float2(m == i ? 1.f : 0.f, 0.f);
+    __syncwarp();
+
+    // Cholesky G = Lc Lc^H, right-looking; lane i keeps row i of Lc.
+    float myInv = 1.f;
+#pragma unroll
+    for (int j = 0; j < LT; j++) {
+        if (i == j) {
+            float d = gr[j].x;
+            d = d > 1e-30f ? d : 1e-30f;
+            d = sqrtf(d);
+            myInv = 1.0f / d;
+            gr[j] = make_float2(d, 0.f);
+            sInv[j] = myInv;
+        }
+        __syncwarp();
+        const float ivj = sInv[j];
+        float2 lij = make_float2(0.f, 0.f);
+        if (i > j) {
+            lij = make_float2(gr[j].x * ivj, gr[j].y * ivj);
+            gr[j] = lij;
+            sCol[i] = lij;
+        }
+        __syncwarp();
+        if (i > j) {
+#pragma unroll
+            for (int m = j + 1; m < LT; m++)
+                if (m <= i) gr[m] = csub_mulc(gr[m], lij, sCol[m]);
+        }
+    }
+    // publish Lc rows for the backward solve (column access)
+#pragma unroll
+    for (int m = 0; m < LT; m++)
+        if (m <= i) sG[i * W::GP + m] = gr[m];
+    __syncwarp();
+
+    // Forward solve Lc W = [Z | I]; lane i ends with row i of W.
+#pragma unroll
+    for (int k = 0; k < LT; k++) {
+        if (i == k) {
+#pragma unroll
+            for (int s = 0; s < 16; s++) {
+                z[s].x *= myInv; z[s].y *= myInv;
+                if (s < cl.nSym) sR[k * W::RP + s] = z[s];
+            }
+#pragma unroll
+            for (int m = 0; m < LT; m++) {
+                e[m].x *= myInv; e[m].y *= myInv;
+                if (m <= k) sR[k * W::RP + 16 + m] = e[m];
+            }
+        }
+        __syncwarp();
+        if (i > k) {
+            const float2 lik = gr[k];
+#pragma unroll
+            for (int s = 0; s < 16; s++)
+                if (s < cl.nSym) z[s] = csub_mul(z[s], lik, sR[k * W::RP + s]);
+#pragma unroll
+            for (int m = 0; m < LT; m++)
+                if (m <= k) e[m] = csub_mul(e[m], lik, sR[k * W::RP + 16 + m]);
+        }
+    }
+    // (G^-1)_ii = sum_m |(Lc^-1)[m][i]|^2 : column norms of W_I across lanes
+#pragma unroll
+    for (int m = 0; m < LT; m++) sQ[i * LT + m] = e[m].x * e[m].x + e[m].y * e[m].y;
+    __syncwarp();
+    float gii = 0.f;
+#pragma unroll
+    for (int m = 0; m < LT; m++)
+        if (m >= i) gii += sQ[m * LT + i];
+
+    // Backward solve Lc^H X = W_Z; lane i ends with row i of X.
+#pragma unroll
+    for (int k = LT - 1; k >= 0; k--) {
+        if (i == k) {
+#pragma unroll
+            for (int s = 0; s < 16; s++) {
+                z[s].x *= myInv; z[s].y *= myInv;
+                if (s < cl.nSym) sR[k * W::RP + s] = z[s];
+            }
+        }
+        __syncwarp();
+        if (i < k) {
+            const float2 lki = sG[k * W::GP + i];
+#pragma unroll
+            for (int s = 0; s < 16; s++)
+                if (s < cl.nSym) z[s] = csub_cmul(z[s], lki, sR[k * W::RP + s]);
+        }
+    }
+    __syncwarp();   // shared memory is reused by the next group
+
+    if (scValid && real) {
+        const float t = s2 * gii;            // 1 - mu
+        const float mu = fmaxf(1.0f - t, 1e-30f);
+        const float invMu = 1.0f / mu;
+        const float nInv = mu / fmaxf(t, 1e-30f);
+        switch (cl.nPam) {
+            case 1: emit<1>(cl, sc, i, z, invMu, nInv); break;
+            case 2: emit<2>(cl, sc, i, z, invMu, nInv); break;
+            case 3: emit<3>(cl, sc, i, z, invMu, nInv); break;
+            default: emit<4>(cl, sc, i, z, invMu, nInv); break;
+        }
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(256, 1) fused_eq_kernel(const __grid_constant__ FusedParams p) {
+    extern __shared__ float4 smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warpsPerCta = blockDim.x >> 5;
+    int maxLT = 1;
+    for (int ci = 0; ci < p.nCells; ci++) maxLT = max(maxLT, p.cell[ci].LT);
+    float2* sm = reinterpret_cast<float2*>(smem_raw) + (long)wib * (warp_smem_bytes(maxLT) / 8);
+    const long gw = (long)blockIdx.x * warpsPerCta + wib;
+    const long nw = (long)gridDim.x * warpsPerCta;
+    int ci = 0;
+    for (long grp = gw; grp < p.totalGroups; grp += nw) {
+        while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+        const FusedCell& cl = p.cell[ci];
+        const long lg = grp - cl.group0;
+        switch (cl.LT) {
+            case 1: process_group<1, P>(cl, lg, sm, lane); break;
+            case 2: process_group<2, P>(cl, lg, sm, lane); break;
+            case 4: process_group<4, P>(cl, lg, sm, lane); break;
+            case 8: process_group<8, P>(cl, lg, sm, lane); break;
+            default: process_group<16, P>(cl, lg, sm, lane); break;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static int layer_tile(int L) {
+    int t = 1;
+    while (t < L) t <<= 1;
+    return t;
+}
+
+int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p, int& maxLT) {
+    if (!cells || nCells < 1 || nCells > kMaxCells) return AERIAL_ERR_INVALID_ARG;
+    long g0 = 0;
+    maxLT = 1;
+    for (int i = 0; i < nCells; i++) {
+        const aerial_cell_desc& c = cells[i];
+        const int nSC = c.nPRB * 12;
+        if (!c.H || !c.Y_rx || !c.llr || c.nPRB < 1 || c.nAnt < 1 || c.nAnt > AERIAL_MAX_ANTS || c.nLayers < 1 ||
+            c.nLayers > AERIAL_MAX_LAYERS || c.nSym < 1 || c.nSym > AERIAL_MAX_SYMS || c.nPamBits < 1 ||
+            c.nPamBits > 4 || !(c.sigma2 >= 0.f))
+            return AERIAL_ERR_INVALID_ARG;
+        if (((uintptr_t)c.H & 7) || ((uintptr_t)c.Y_rx & 7) || ((uintptr_t)c.llr & 7) || ((uintptr_t)c.Y_eq & 7))
+            return AERIAL_ERR_INVALID_ARG;
+        FusedCell& f = p.cell[i];
+        f.H = (const float2*)c.H;
+        f.Y = (const float2*)c.Y_rx;
+        f.llr = c.llr;
+        f.yeq = (float2*)c.Y_eq;
+        f.sigma2 = c.sigma2;
+        f.nSC = nSC;
+        f.A = c.nAnt;
+        f.L = c.nLayers;
+        f.nSym = c.nSym;
+        f.nPam = c.nPamBits;
+        f.LT = layer_tile(c.nLayers);
+        f.vecY = ((c.nAnt % 2) == 0 && ((uintptr_t)c.Y_rx & 15) == 0) ? 1 : 0;
+        f.lut = pam_lut(c.nPamBits);
+        f.group0 = g0;
+        // LLR rows of 2*nPam floats are written as float4 for nPam 2/4: need 16 B alignment
+        if ((c.nPamBits == 2 || c.nPamBits == 4) && ((uintptr_t)c.llr & 15)) return AERIAL_ERR_INVALID_ARG;
+        g0 += (nSC + (32 / f.LT) - 1) / (32 / f.LT);
+        if (f.LT > maxLT) maxLT = f.LT;
+    }
+    p.nCells = nCells;
+    p.totalGroups = g0;
+    return AERIAL_OK;
+}
+
+static int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+struct LaunchShape {
+    int warps, ctasPerSm;
+};
+
+static LaunchShape default_shape(int maxLT) {
+    (void)maxLT;
+    return {8, 1};
+}
+
+template <int P>
+static int launch_fused_p(const FusedParams& p, int maxLT, LaunchShape sh, cudaStream_t st) {
+    const int bytes = sh.warps * warp_smem_bytes(maxLT);
+    static int configured = 0;
+    if (bytes > 48 * 1024 && bytes > configured) {
+        cudaError_t e = cudaFuncSetAttribute(fused_eq_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return (int)e;
+        configured = bytes;
+    }
+    long need = (p.totalGroups + sh.warps - 1) / sh.warps;
+    long grid = (long)sm_count() * sh.ctasPerSm;
+    if (grid > need) grid = need;
+    if (grid < 1) grid = 1;
+    fused_eq_kernel<P><<<(unsigned)grid, sh.warps * 32, bytes, st>>>(p);
+    return launch_status();
+}
+
+int launch_fused(const FusedParams& p, int maxLT, int prec, LaunchShape sh, cudaStream_t st) {
+    if (sh.warps < 1 || sh.warps > 8 || sh.ctasPerSm < 1 || sh.ctasPerSm > 8) return AERIAL_ERR_INVALID_ARG;
+    if ((long)sh.warps * warp_smem_bytes(maxLT) * sh.ctasPerSm > 227 * 1024) return AERIAL_ERR_UNSUPPORTED;
+    switch (prec) {
+        case AERIAL_PREC_FP16: return launch_fused_p<AERIAL_PREC_FP16>(p, maxLT, sh, st);
+        case AERIAL_PREC_BF16: return launch_fused_p<AERIAL_PREC_BF16>(p, maxLT, sh, st);
+        case AERIAL_PREC_BF16X3: return launch_fused_p<AERIAL_PREC_BF16X3>(p, maxLT, sh, st);
+        default: return AERIAL_ERR_UNSUPPORTED;
+    }
+}
+
+}  // namespace aeq
+
+using namespace aeq;
+
+extern "C" int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
+                                     void* stream) {
+    FusedParams p;
+    int maxLT = 1;
+    int s = build_fused_params(cells, nCells, p, maxLT);
+    if (s) return s;
+    LaunchShape sh = default_shape(maxLT);
+    int prec = AERIAL_PREC_FP16;
+    if (tuning) {
+        prec = tuning->precision;
+        if (tuning->warps_per_cta) sh.warps = tuning->warps_per_cta;
+        if (tuning->ctas_per_sm) sh.ctasPerSm = tuning->ctas_per_sm;
+    }
+    return launch_fused(p, maxLT, prec, sh, to_stream(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: time each candidate launch shape on the caller's cells and keep
+// the fastest.  Candidates are (warps per CTA, CTAs per SM) pairs whose
+// shared memory fits one SM; each is timed with CUDA events over a few
+// launches after one warm-up launch.
+// ---------------------------------------------------------------------------
+extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial_tuning* best, float* bestUs,
+                               void* stream) {
+    if (!best) return AERIAL_ERR_INVALID_ARG;
+    FusedParams p;
+    int maxLT = 1;
+    int s = build_fused_params(cells, nCells, p, maxLT);
+    if (s) return s;
+    cudaStream_t st = to_stream(stream);
+    const int prec = best->precision;
+    static const LaunchShape cand[] = {{2, 4}, {4, 1}, {4, 2}, {6, 1}, {8, 1}, {2, 8}, {4, 4}};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float bestT = 1e30f;
+    LaunchShape bestS = default_shape(maxLT);
+    for (const LaunchShape& sh : cand) {
+        if ((long)sh.warps * warp_smem_bytes(maxLT) * sh.ctasPerSm > 200 * 1024) continue;
+        if ((s = launch_fused(p, maxLT, prec, sh, st))) break;
+        const int reps = 5;
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < reps && !s; r++) s = launch_fused(p, maxLT, prec, sh, st);
+        cudaEventRecord(e1, st);
+        if (s) break;
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) { s = (int)e; break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= reps;
+        if (ms < bestT) { bestT = ms; bestS = sh; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s) return s;
+    best->warps_per_cta = bestS.warps;
+    best->ctas_per_sm = bestS.ctasPerSm;
+    best->sc_per_group = 0;
+    if (bestUs) *bestUs = bestT * 1000.f;
+    return AERIAL_OK;
+}

@@ -1,0 +1,197 @@
+/*
+ * aerial_eq.h -- C ABI of the B200 PUSCH receiver equalization path.
+ *
+ * Drop-in boundary for the per-subcarrier equalization chain of
+ * ebaenamar/aerial-mimo-tc-optimization: Gram, MMSE coefficient solve,
+ * coef_apply, max-log LLR demapper and SRS filter multiply, plus the fused
+ * chain and a slot-serving loop.  The reference has no library API; its
+ * kernel-entry argument lists and buffer layouts are the interface, and each
+ * entry point below names the reference kernel it replaces (file:line inside
+ * the reference project).
+ *
+ * Conventions (all entry points):
+ *   - Buffers are DEVICE pointers owned by the caller unless stated
+ *     otherwise; nothing is allocated, freed or synchronised by a call.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Work is enqueued asynchronously on it.
+ *   - Return value: AERIAL_OK (0), an AERIAL_ERR_* code for bad arguments,
+ *     or a cudaError_t value (1..999) from the launch.  Nothing calls
+ *     exit(); the reference's CUDA_CHECK -> exit(1) becomes a status.
+ *   - Complex numbers are interleaved {re, im} pairs: aerial_cf32 is the
+ *     reference's `struct cf32 { float re, im; }` (src/aerial_coef_wmma.cu:60);
+ *     aerial_ch2 is `struct half2c` / `struct ch2` of IEEE binary16 bits
+ *     (src/llr/aerial_llr_v3.cu:51, src/srs/srs_wmma_bench.cu:41).
+ *
+ * Layouts (row-major):
+ *   H      [nSC][nAnt][nLayers]      channel      (src/aerial_bottleneck.cu:58)
+ *   Y_rx   [nSC][nSym][nAnt]         received     (src/aerial_coef_wmma.cu:73)
+ *   C      [nSC][nLayers][nAnt]      coefficients (src/aerial_coef_wmma.cu:72)
+ *   G      [nSC][nLayers][nLayers]   Gram         (src/aerial_bottleneck.cu:59)
+ *   Y_eq   [nSC][nLayers][nSym]      equalized    (src/aerial_coef_wmma.cu:74)
+ *   LLR    [nSC*nLayers*nSym][2*nPamBits] in the order
+ *          bit0_I, bit0_Q, bit1_I, bit1_Q, ...  (src/llr/aerial_llr_v3.cu:92,105)
+ *
+ * Noise convention: noiseInv = 1/nu where nu is the complex noise variance of
+ * the (unbiased) equalized symbol, so LLR = (d_opposite^2 - d_nearest^2)/nu
+ * per real dimension of a unit-energy constellation.  The MMSE stages produce
+ * nu_l = sigma2 (G^-1)_ll / (1 - sigma2 (G^-1)_ll) for layer l, where sigma2
+ * is the complex noise variance per receive antenna.
+ */
+#ifndef AERIAL_EQ_H
+#define AERIAL_EQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { float re, im; } aerial_cf32;
+typedef struct { uint16_t re, im; } aerial_ch2;
+
+enum {
+    AERIAL_OK = 0,
+    AERIAL_ERR_INVALID_ARG = 1001,   /* null pointer, non-positive or too-large size */
+    AERIAL_ERR_UNSUPPORTED = 1002,   /* shape outside the supported envelope */
+    AERIAL_ERR_NO_DEVICE = 1003,     /* no usable sm_100 device */
+    AERIAL_ERR_BUDGET = 1004,        /* serving: request exceeds the memory budget */
+    AERIAL_ERR_QUEUE_FULL = 1005,    /* serving: submission queue full */
+    AERIAL_ERR_TIMEOUT = 1006,       /* a bounded wait ran out */
+    AERIAL_ERR_NOT_FOUND = 1007      /* serving: unknown cell or request */
+};
+
+/* Supported envelope: 1 <= nLayers <= 16, 1 <= nSym <= 16, 1 <= nAnt <= 256,
+ * 1 <= nPamBits <= 4 (QPSK..256QAM), nSC >= 1. */
+#define AERIAL_MAX_LAYERS 16
+#define AERIAL_MAX_SYMS 16
+#define AERIAL_MAX_ANTS 256
+#define AERIAL_MAX_CELLS 64
+
+const char* aerial_error_string(int status);
+int aerial_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Per-stage entry points (the plain FP32 chain; bit-exact restatements of   */
+/* the reference's scalar kernels where the reference has the stage).        */
+/* ------------------------------------------------------------------------ */
+
+/* Y_eq[sc][l][s] = sum_a C[sc][l][a] * Y_rx[sc][s][a], FP32, antennas summed
+ * in order with the reference's fused multiply-adds (bit-exact).
+ * Replaces coef_apply_v1_scalar(C, Y_rx, Y_eq, nSC, nSym)
+ * (src/aerial_coef_wmma.cu:71-75); N_LAYERS and N_BS_ANTS become runtime. */
+int aerial_coef_apply(const aerial_cf32* C, const aerial_cf32* Y_rx, aerial_cf32* Y_eq,
+                      int nSC, int nSym, int nLayers, int nAnt, void* stream);
+
+/* Same product on the tensor cores (FP16 operands, FP32 accumulation): the
+ * semantics of coef_apply_v2_wmma (src/aerial_coef_wmma.cu:146-239). */
+int aerial_coef_apply_tc(const aerial_cf32* C, const aerial_cf32* Y_rx, aerial_cf32* Y_eq,
+                         int nSC, int nSym, int nLayers, int nAnt, void* stream);
+
+/* G[sc] = H[sc]^H H[sc] + sigma2 I, FP32 (bit-exact with gram_scalar given
+ * M = H^H, then one FP32 add of sigma2 on the diagonal).
+ * Replaces gram_scalar(M, H, G, nSC) (src/aerial_bottleneck.cu:56-60); M is
+ * dropped because the MMSE Gram is Hermitian, sigma2 is added. */
+int aerial_gram(const aerial_cf32* H, float sigma2, aerial_cf32* G,
+                int nSC, int nAnt, int nLayers, void* stream);
+
+/* MMSE coefficients C[sc] = diag(1/mu) G^-1 H^H (FP32 Cholesky of G, forward
+ * and backward substitution per antenna), mu_l = Re (G^-1 H^H H)_ll, and
+ * noiseInv[sc][l] = mu_l / (1 - mu_l).  No reference counterpart (the
+ * reference's coef_apply consumes a random C). */
+int aerial_mmse_coef(const aerial_cf32* G, const aerial_cf32* H, aerial_cf32* C, float* noiseInv,
+                     int nSC, int nAnt, int nLayers, void* stream);
+
+/* Max-log PAM LLR demapper, FP16 in / FP16 out, bit-exact with the
+ * reference.  Replaces llr_v1_baseline(in, ni, out, N, nPamBits)
+ * (src/llr/aerial_llr_v3.cu:84-86) and llr_v3_reg_template (:219-229). */
+int aerial_llr(const aerial_ch2* softEst, const float* noiseInv, uint16_t* llrOut,
+               int N, int nPamBits, void* stream);
+
+/* Same demapper with complex64 input and float32 output (the layout the
+ * fused chain writes).  noiseInv index = idx / nSymPerNoise (1 = per
+ * symbol, as the reference; nSym = one value per (sc, layer)). */
+int aerial_llr_f32(const aerial_cf32* softEst, const float* noiseInv, float* llrOut,
+                   int N, int nPamBits, int nSymPerNoise, void* stream);
+
+/* SRS filter multiply, FP16 in/out with FP32 accumulation:
+ *   H_est[blk][ant][k_out][p] = sum_k (W[k_out][k] * FOCC[p][k % foccLen]) * SRS[blk][ant][k]
+ * Replaces srs_filter_v1_scalar<K,N_PORTS,FOCC_LENGTH>(H_est, SRS, W, FOCC,
+ * nAnt, nBlocks) (src/srs/srs_wmma_bench.cu:57-63); template arguments are
+ * runtime.  The reference's complex_conjmul (:43-47) computes the plain
+ * product W*FOCC (no conjugate); that behaviour is kept. */
+int aerial_srs_filter(aerial_ch2* H_est, const aerial_ch2* SRS, const aerial_ch2* W,
+                      const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts,
+                      int foccLen, void* stream);
+
+/* SRS filter multiply straight into the PUSCH channel layout: writes
+ * H[sc][ant][layer] (complex64) for sc = blk*K + k_out, layer = port, so a
+ * cell's resident channel is refreshed in place.  FP32 accumulation. */
+int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, const aerial_ch2* W,
+                          const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts,
+                          int foccLen, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Fused chain: Gram -> Cholesky MMSE -> apply -> LLR in one kernel; G, C and */
+/* Y_eq stay on chip, only LLRs (and optionally Y_eq) are written.           */
+/* ------------------------------------------------------------------------ */
+
+/* One cell-slot.  nSC = 12 * nPRB.  Y_eq may be NULL. */
+typedef struct {
+    const aerial_cf32* H;      /* [nSC][nAnt][nLayers] */
+    const aerial_cf32* Y_rx;   /* [nSC][nSym][nAnt] */
+    float* llr;                /* [nSC*nLayers*nSym][2*nPamBits] float32 */
+    aerial_cf32* Y_eq;         /* optional [nSC][nLayers][nSym] (unbiased) */
+    float sigma2;              /* noise variance per receive antenna */
+    int nPRB, nAnt, nLayers, nSym, nPamBits;
+} aerial_cell_desc;
+
+/* Operand precision of the tensor-core products. */
+enum {
+    AERIAL_PREC_FP16 = 0,      /* FP16 operands, FP32 accumulation */
+    AERIAL_PREC_BF16 = 1,      /* BF16 operands, FP32 accumulation */
+    AERIAL_PREC_BF16X3 = 2,    /* BF16 hi/lo split, 3 products, FP32 accumulation */
+    AERIAL_PREC_FP32 = 3       /* FP32 CUDA-core products (no tensor cores) */
+};
+
+/* Launch shape; zero fields take the autotuned / default value. */
+typedef struct {
+    int precision;             /* AERIAL_PREC_* */
+    int warps_per_cta;         /* 0 = default */
+    int ctas_per_sm;           /* 0 = default */
+    int sc_per_group;          /* reserved, 0 */
+} aerial_tuning;
+
+/* Equalize nCells cell-slots in ONE persistent launch (cells may differ in
+ * PRBs, antennas, layers, symbols and modulation).  `cells` is a HOST array
+ * (copied into the launch's parameters); its buffers are device pointers.
+ * Results per subcarrier do not depend on which other cells share the
+ * launch.  nCells <= AERIAL_MAX_CELLS.  tuning may be NULL.
+ * No reference counterpart as one kernel: the reference chains gram_scalar,
+ * coef_apply and a demapper as separate launches (src/pipeline_overlap.cu:293-301). */
+int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
+                          void* stream);
+
+/* The plain FP32 chain for the same cells: aerial_gram, aerial_mmse_coef,
+ * aerial_coef_apply and aerial_llr_f32 per cell, intermediates in the
+ * caller's workspace (size from aerial_pusch_eq_plain_workspace).  This is
+ * the reference's stage-by-stage scalar method on the GPU. */
+size_t aerial_pusch_eq_plain_workspace(const aerial_cell_desc* cells, int nCells);
+int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, void* workspace,
+                          size_t workspaceBytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Autotuner                                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Time the fused kernel on `cells` for each candidate launch shape and
+ * write the fastest into *best (precision is taken from *best on entry).
+ * Runs synchronously on `stream`.  Returns the best time in microseconds via
+ * *bestUs (may be NULL). */
+int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial_tuning* best, float* bestUs,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AERIAL_EQ_H */

@@ -1,0 +1,697 @@
+/*
+ * aerial_oracle.c -- TEST INFRASTRUCTURE ONLY (the checker, never the product).
+ *
+ * CPU restatement of the PUSCH equalization path of
+ * ebaenamar/aerial-mimo-tc-optimization, used by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline / reference arm.
+ * Nothing in the shipped library links or calls this file.
+ *
+ * Two families of functions live here:
+ *
+ *  1. Scalar FP32 restatements of the reference's V1 kernels, written so that
+ *     every floating-point operation happens in the same order and with the
+ *     same fused multiply-adds as the reference's CUDA source compiles to
+ *     (nvcc contracts `acc + a*b - c*d` into fma(-c, d, fma(a, b, acc))).
+ *     They are bit-exact targets for the GPU "plain FP32 chain":
+ *       - coef_apply_v1_scalar      src/aerial_coef_wmma.cu:71-104
+ *       - gram_scalar               src/aerial_bottleneck.cu:56-80
+ *       - llr_v1_baseline           src/llr/aerial_llr_v3.cu:84-108
+ *       - srs_filter_v1_scalar      src/srs/srs_wmma_bench.cu:57-90 (FP16
+ *         arithmetic, emulated with _Float16 rounding of every operation)
+ *     plus the parts the reference does not have (Cholesky MMSE solve,
+ *     unbiasing, post-equalisation noise), specified here once and restated
+ *     identically by the GPU plain chain.
+ *
+ *  2. An FP64 model of the whole chain (G = H^H H + s2 I, Cholesky,
+ *     X = G^-1 H^H Y, unbiased by mu_l = 1 - s2 (G^-1)_ll, max-log LLR in
+ *     double following cpu_ref, src/llr/aerial_llr_v3.cu:61-79).
+ *
+ * Build: gcc -O2 -fPIC -shared -fopenmp -ffp-contract=off (oracle/Makefile).
+ * -ffp-contract=off matters: every fused multiply-add below is explicit.
+ *
+ * Layouts (all row-major, complex = interleaved {re, im} float pairs):
+ *   H    [nSC][nAnt][nLayers]      (src/aerial_bottleneck.cu:58)
+ *   Y_rx [nSC][nSym][nAnt]         (src/aerial_coef_wmma.cu:73)
+ *   C    [nSC][nLayers][nAnt]      (src/aerial_coef_wmma.cu:72)
+ *   G    [nSC][nLayers][nLayers]   (src/aerial_bottleneck.cu:59)
+ *   Y_eq [nSC][nLayers][nSym]      (src/aerial_coef_wmma.cu:74)
+ *   LLR  [nSC*nLayers*nSym][2*nPamBits], order bit0_I, bit0_Q, bit1_I, ...
+ *        (src/llr/aerial_llr_bench_v2.cu:75, aerial_llr_v3.cu:92,105)
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct { float re, im; } cf;
+typedef struct { double re, im; } cd;
+
+#define MAXL 16
+
+/* ------------------------------------------------------------------------- */
+/* threads                                                                    */
+/* ------------------------------------------------------------------------- */
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+int orc_get_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------------- */
+/* Reference input generators (glibc rand(), same call order as the          */
+/* reference's main() functions so its recorded results can be reproduced). */
+/* ------------------------------------------------------------------------- */
+
+/* out[i] = ((float)rand()/RAND_MAX - .5f) * scale, after srand(seed).
+ * src/aerial_coef_wmma.cu:383-387 (scale 1), src/coef_rigor.cu:101-104 (1.4). */
+void orc_ref_uniform(unsigned seed, float scale, float* out, long n) {
+    srand(seed);
+    for (long i = 0; i < n; i++) {
+        float v = (float)rand() / RAND_MAX - .5f;
+        out[i] = (scale == 1.0f) ? v : v * scale;
+    }
+}
+
+static uint16_t f2h_bits(float x) {
+    _Float16 h = (_Float16)x; /* round-to-nearest-even */
+    uint16_t b;
+    memcpy(&b, &h, 2);
+    return b;
+}
+static float h2f(uint16_t b) {
+    _Float16 h;
+    memcpy(&h, &b, 2);
+    return (float)h;
+}
+
+/* LLR bench inputs, src/llr/aerial_llr_v3.cu:267-275: softEst as FP16 pairs
+ * U(-0.7,0.7), noiseInv = 10^(U{0..25}/10) * 2. */
+void orc_ref_llr_inputs(unsigned seed, long n, uint16_t* soft, float* ni) {
+    srand(seed);
+    for (long i = 0; i < n; i++) {
+        float re = ((float)rand() / RAND_MAX - .5f) * 1.4f;
+        float im = ((float)rand() / RAND_MAX - .5f) * 1.4f;
+        soft[2 * i] = f2h_bits(re);
+        soft[2 * i + 1] = f2h_bits(im);
+        ni[i] = powf(10.f, (float)(rand() % 26) / 10.f) * 2.f;
+    }
+}
+
+/* SRS bench inputs, src/srs/srs_wmma_bench.cu:272-277: FP16 U(-0.7,0.7) for
+ * SRS, then W, then FOCC, re before im. */
+void orc_ref_srs_inputs(unsigned seed, long nSrs, long nW, long nFocc,
+                        uint16_t* srs, uint16_t* w, uint16_t* focc) {
+    srand(seed);
+    for (long i = 0; i < 2 * nSrs; i++) srs[i] = f2h_bits(((float)rand() / RAND_MAX - 0.5f) * 1.4f);
+    for (long i = 0; i < 2 * nW; i++) w[i] = f2h_bits(((float)rand() / RAND_MAX - 0.5f) * 1.4f);
+    for (long i = 0; i < 2 * nFocc; i++) focc[i] = f2h_bits(((float)rand() / RAND_MAX - 0.5f) * 1.4f);
+}
+
+/* float <-> binary16 helpers exposed for tests */
+void orc_f32_to_f16(const float* x, uint16_t* y, long n) {
+    for (long i = 0; i < n; i++) y[i] = f2h_bits(x[i]);
+}
+void orc_f16_to_f32(const uint16_t* x, float* y, long n) {
+    for (long i = 0; i < n; i++) y[i] = h2f(x[i]);
+}
+
+/* ------------------------------------------------------------------------- */
+/* PAM soft-bit constants.  D_i = 2^(n-1-i) / sqrt(2 (4^n - 1) / 3):        */
+/* the per-dimension Gray PAM decision distances of unit-energy QAM.         */
+/* They reproduce the LUT of src/llr/aerial_llr_v3.cu:42-49 (computed, not   */
+/* copied).                                                                  */
+/* ------------------------------------------------------------------------- */
+static double pam_d64(int n, int i) {
+    double norm = sqrt(2.0 * (double)((1 << (2 * n)) - 1) / 3.0);
+    return (double)(1 << (n - 1 - i)) / norm;
+}
+static float pam_d32(int n, int i) {
+    /* round 1/norm to float once, then scale by an exact power of two */
+    double norm = sqrt(2.0 * (double)((1 << (2 * n)) - 1) / 3.0);
+    float r = (float)(1.0 / norm);
+    return r * (float)(1 << (n - 1 - i));
+}
+void orc_pam_lut(int nPamBits, float* d32, double* d64) {
+    for (int i = 0; i < nPamBits; i++) {
+        d32[i] = pam_d32(nPamBits, i);
+        d64[i] = pam_d64(nPamBits, i);
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* LLR demapper                                                               */
+/* ------------------------------------------------------------------------- */
+
+/* FP32 restatement of llr_v1_baseline (src/llr/aerial_llr_v3.cu:84-108).
+ * softEst: interleaved float pairs; noise index = idx / symsPerNoise
+ * (1 = one noiseInv per symbol as in the reference).  out[idx*2n + 2b + iq]
+ * receives the clamped FP32 LLR (before the reference's FP16 store). */
+static void llr_one_f32(float pamI, float pamQ, float noise, int n, const float* D, float* o) {
+    float dist = D[n - 1];
+    for (int iq = 0; iq < 2; iq++) {
+        float pSB[4], pMD[4];
+        pSB[0] = (iq == 0) ? pamI : pamQ;
+        unsigned sign = 0;
+        for (int i = 0; i < n - 1; i++) {
+            pSB[i + 1] = D[i] - fabsf(pSB[i]);
+            pMD[i] = dist + fabsf(pSB[i]);
+            pMD[i] *= pMD[i];
+            if (pSB[i] < 0.f) sign |= 1u << i;
+        }
+        pMD[n - 1] = dist + fabsf(pSB[n - 1]);
+        pMD[n - 1] *= pMD[n - 1];
+        if (pSB[n - 1] < 0.f) sign |= 1u << (n - 1);
+        float md1 = fabsf(pSB[n - 1]) - dist;
+        md1 *= md1;
+        for (int i = 0; i < n; i++) {
+            float llr = (pMD[i] - md1) * noise;
+            if (sign & (1u << i)) llr = -llr;
+            o[i * 2 + iq] = fmaxf(-65504.f, fminf(65504.f, llr));
+        }
+    }
+}
+
+void orc_llr_f32(const float* soft, const float* ni, float* out, long N, int nPamBits,
+                 int symsPerNoise) {
+    float D[4];
+    for (int i = 0; i < nPamBits; i++) D[i] = pam_d32(nPamBits, i);
+    if (symsPerNoise < 1) symsPerNoise = 1;
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N; idx++)
+        llr_one_f32(soft[2 * idx], soft[2 * idx + 1], ni[idx / symsPerNoise], nPamBits, D,
+                    out + idx * 2 * nPamBits);
+}
+
+/* Same, FP16 softEst in and FP16 LLR out: the exact reference I/O. */
+void orc_llr_f16io(const uint16_t* soft, const float* ni, uint16_t* out, long N, int nPamBits) {
+    float D[4];
+    for (int i = 0; i < nPamBits; i++) D[i] = pam_d32(nPamBits, i);
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N; idx++) {
+        float o[8];
+        llr_one_f32(h2f(soft[2 * idx]), h2f(soft[2 * idx + 1]), ni[idx], nPamBits, D, o);
+        for (int j = 0; j < 2 * nPamBits; j++) out[idx * 2 * nPamBits + j] = f2h_bits(o[j]);
+    }
+}
+
+/* FP64 demapper following cpu_ref (src/llr/aerial_llr_v3.cu:61-79) and
+ * cpu_computePamLlr_ref (src/llr/aerial_llr_bench_v2.cu:72-107). */
+static void llr_one_f64(double pamI, double pamQ, double noise, int n, const double* D, double* o) {
+    double dist = D[n - 1];
+    for (int iq = 0; iq < 2; iq++) {
+        double pSB[4], pMD[4];
+        pSB[0] = (iq == 0) ? pamI : pamQ;
+        unsigned sign = 0;
+        for (int i = 0; i < n - 1; i++) {
+            pSB[i + 1] = D[i] - fabs(pSB[i]);
+            pMD[i] = dist + fabs(pSB[i]);
+            pMD[i] *= pMD[i];
+            if (pSB[i] < 0) sign |= 1u << i;
+        }
+        pMD[n - 1] = dist + fabs(pSB[n - 1]);
+        pMD[n - 1] *= pMD[n - 1];
+        if (pSB[n - 1] < 0) sign |= 1u << (n - 1);
+        double md1 = fabs(pSB[n - 1]) - dist;
+        md1 *= md1;
+        for (int i = 0; i < n; i++) {
+            double llr = (pMD[i] - md1) * noise;
+            if (sign & (1u << i)) llr = -llr;
+            o[i * 2 + iq] = fmax(-65504.0, fmin(65504.0, llr));
+        }
+    }
+}
+
+/* softEst as float pairs (the reference feeds FP16 values widened to float). */
+void orc_llr_f64(const float* soft, const float* ni, double* out, long N, int nPamBits,
+                 int symsPerNoise) {
+    double D[4];
+    for (int i = 0; i < nPamBits; i++) D[i] = pam_d64(nPamBits, i);
+    if (symsPerNoise < 1) symsPerNoise = 1;
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N; idx++)
+        llr_one_f64(soft[2 * idx], soft[2 * idx + 1], ni[idx / symsPerNoise], nPamBits, D,
+                    out + idx * 2 * nPamBits);
+}
+
+/* ------------------------------------------------------------------------- */
+/* complex FP32 helpers with the reference's contraction                      */
+/* ------------------------------------------------------------------------- */
+
+/* cma() of src/aerial_coef_wmma.cu:61-64 as nvcc contracts it:
+ *   re = fma(-a.im, b.im, fma(a.re, b.re, acc.re))
+ *   im = fma( a.im, b.re, fma(a.re, b.im, acc.im)) */
+static inline cf cma(cf a, cf b, cf acc) {
+    cf r;
+    r.re = fmaf(-a.im, b.im, fmaf(a.re, b.re, acc.re));
+    r.im = fmaf(a.im, b.re, fmaf(a.re, b.im, acc.im));
+    return r;
+}
+
+/* ------------------------------------------------------------------------- */
+/* coef_apply                                                                 */
+/* ------------------------------------------------------------------------- */
+
+/* coef_apply_v1_scalar, src/aerial_coef_wmma.cu:71-104: sequential antenna
+ * loop, acc = cma(C[a], Y[a], acc). */
+void orc_coef_apply_v1(const float* C_, const float* Y_, float* O_, long nSC, int nSym, int L,
+                       int A) {
+    const cf* C = (const cf*)C_;
+    const cf* Y = (const cf*)Y_;
+    cf* O = (cf*)O_;
+#pragma omp parallel for schedule(static)
+    for (long sc = 0; sc < nSC; sc++)
+        for (int l = 0; l < L; l++)
+            for (int s = 0; s < nSym; s++) {
+                cf acc = {0.f, 0.f};
+                const cf* c = C + (sc * L + l) * (long)A;
+                const cf* y = Y + (sc * nSym + s) * (long)A;
+                for (int a = 0; a < A; a++) acc = cma(c[a], y[a], acc);
+                O[(sc * L + l) * (long)nSym + s] = acc;
+            }
+}
+
+/* Model of coef_apply_v2_wmma (src/aerial_coef_wmma.cu:146-239): operands
+ * rounded to FP16, the four real products rr, ri, ir, ii summed exactly and
+ * rounded to FP32, then re = rr - ir, im = ri + ii in FP32 (:235-236). */
+void orc_coef_apply_v2_model(const float* C_, const float* Y_, float* O_, long nSC, int nSym,
+                             int L, int A) {
+    const cf* C = (const cf*)C_;
+    const cf* Y = (const cf*)Y_;
+    cf* O = (cf*)O_;
+#pragma omp parallel for schedule(static)
+    for (long sc = 0; sc < nSC; sc++)
+        for (int l = 0; l < L; l++)
+            for (int s = 0; s < nSym; s++) {
+                double rr = 0, ri = 0, ir = 0, ii = 0;
+                const cf* c = C + (sc * L + l) * (long)A;
+                const cf* y = Y + (sc * nSym + s) * (long)A;
+                for (int a = 0; a < A; a++) {
+                    double cr = h2f(f2h_bits(c[a].re)), ci = h2f(f2h_bits(c[a].im));
+                    double yr = h2f(f2h_bits(y[a].re)), yi = h2f(f2h_bits(y[a].im));
+                    rr += cr * yr;
+                    ri += cr * yi;
+                    ir += ci * yi;
+                    ii += ci * yr;
+                }
+                cf o;
+                o.re = (float)rr - (float)ir;
+                o.im = (float)ri + (float)ii;
+                O[(sc * L + l) * (long)nSym + s] = o;
+            }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Gram                                                                       */
+/* ------------------------------------------------------------------------- */
+
+/* gram_scalar, src/aerial_bottleneck.cu:56-80, with its separate M operand:
+ * G[r][c] = sum_k cma(M[r][k], H[k][c]). */
+void orc_gram_ref(const float* M_, const float* H_, float* G_, long nSC, int L, int A) {
+    const cf* M = (const cf*)M_;
+    const cf* H = (const cf*)H_;
+    cf* G = (cf*)G_;
+#pragma omp parallel for schedule(static)
+    for (long sc = 0; sc < nSC; sc++)
+        for (int r = 0; r < L; r++)
+            for (int c = 0; c < L; c++) {
+                cf acc = {0.f, 0.f};
+                const cf* m = M + (sc * L + r) * (long)A;
+                const cf* h = H + sc * (long)A * L + c;
+                for (int k = 0; k < A; k++) acc = cma(m[k], h[(long)k * L], acc);
+                G[(sc * L + r) * (long)L + c] = acc;
+            }
+}
+
+/* The MMSE Gram of the path: M := H^H (so G is Hermitian), then + sigma2 on
+ * the diagonal in one FP32 add. */
+static void gram_sc_f32(const cf* H, float sigma2, int L, int A, cf* G) {
+    for (int r = 0; r < L; r++)
+        for (int c = 0; c < L; c++) {
+            cf acc = {0.f, 0.f};
+            for (int k = 0; k < A; k++) {
+                cf m = H[k * L + r];
+                m.im = -m.im;
+                acc = cma(m, H[k * L + c], acc);
+            }
+            if (r == c) acc.re = acc.re + sigma2;
+            G[r * L + c] = acc;
+        }
+}
+
+void orc_gram(const float* H_, float sigma2, float* G_, long nSC, int A, int L) {
+    const cf* H = (const cf*)H_;
+    cf* G = (cf*)G_;
+#pragma omp parallel for schedule(static)
+    for (long sc = 0; sc < nSC; sc++) gram_sc_f32(H + sc * (long)A * L, sigma2, L, A, G + sc * (long)L * L);
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP32 MMSE coefficient solve (no reference counterpart; this is the       */
+/* specification the GPU plain chain restates operation for operation).     */
+/*                                                                          */
+/*   Cholesky G = Lc Lc^H from the lower triangle of G, column by column:   */
+/*     s = G[j][j].re - sum_k |Lc[j][k]|^2   (fma(-x,x,s), re then im)      */
+/*     d = sqrtf(s), inv[j] = 1/d (s <= 0 is replaced by 1e-30f)            */
+/*     Lc[i][j] = (G[i][j] - sum_k Lc[i][k] conj(Lc[j][k])) * inv[j]        */
+/*   C[:,a] = G^-1 conj(H[a][:]) by forward then backward substitution.     */
+/*   mu_l   = Re sum_a C[l][a] H[a][l]          (= (C H)_ll)                */
+/*   C[l][:] *= 1/mu_l ; noiseInv_l = mu_l / (1 - mu_l)                     */
+/* ------------------------------------------------------------------------- */
+static void chol_f32(const cf* G, int L, cf* Lc, float* inv) {
+    for (int j = 0; j < L; j++) {
+        float s = G[j * L + j].re;
+        for (int k = 0; k < j; k++) {
+            cf x = Lc[j * L + k];
+            s = fmaf(-x.re, x.re, s);
+            s = fmaf(-x.im, x.im, s);
+        }
+        if (!(s > 0.f)) s = 1e-30f;
+        float d = sqrtf(s);
+        float iv = 1.0f / d;
+        inv[j] = iv;
+        Lc[j * L + j].re = d;
+        Lc[j * L + j].im = 0.f;
+        for (int i = j + 1; i < L; i++) {
+            cf acc = G[i * L + j];
+            for (int k = 0; k < j; k++) {
+                cf a = Lc[i * L + k], b = Lc[j * L + k];
+                /* acc -= a * conj(b) */
+                acc.re = fmaf(-a.re, b.re, acc.re);
+                acc.re = fmaf(-a.im, b.im, acc.re);
+                acc.im = fmaf(-a.im, b.re, acc.im);
+                acc.im = fmaf(a.re, b.im, acc.im);
+            }
+            Lc[i * L + j].re = acc.re * iv;
+            Lc[i * L + j].im = acc.im * iv;
+        }
+    }
+}
+
+/* Solve G x = b with the factor: Lc w = b, then Lc^H x = w. */
+static void chol_solve_f32(const cf* Lc, const float* inv, int L, const cf* b, cf* x) {
+    cf w[MAXL];
+    for (int i = 0; i < L; i++) {
+        cf acc = b[i];
+        for (int k = 0; k < i; k++) {
+            cf a = Lc[i * L + k], y = w[k];
+            /* acc -= a * y */
+            acc.re = fmaf(-a.re, y.re, acc.re);
+            acc.re = fmaf(a.im, y.im, acc.re);
+            acc.im = fmaf(-a.re, y.im, acc.im);
+            acc.im = fmaf(-a.im, y.re, acc.im);
+        }
+        w[i].re = acc.re * inv[i];
+        w[i].im = acc.im * inv[i];
+    }
+    for (int i = L - 1; i >= 0; i--) {
+        cf acc = w[i];
+        for (int k = i + 1; k < L; k++) {
+            cf a = Lc[k * L + i], y = x[k];
+            /* acc -= conj(a) * y */
+            acc.re = fmaf(-a.re, y.re, acc.re);
+            acc.re = fmaf(-a.im, y.im, acc.re);
+            acc.im = fmaf(-a.re, y.im, acc.im);
+            acc.im = fmaf(a.im, y.re, acc.im);
+        }
+        x[i].re = acc.re * inv[i];
+        x[i].im = acc.im * inv[i];
+    }
+}
+
+static void mmse_coef_sc_f32(const cf* G, const cf* H, int A, int L, cf* C, float* nI) {
+    cf Lc[MAXL * MAXL];
+    float inv[MAXL];
+    chol_f32(G, L, Lc, inv);
+    for (int a = 0; a < A; a++) {
+        cf b[MAXL], x[MAXL];
+        for (int l = 0; l < L; l++) {
+            b[l].re = H[a * L + l].re;
+            b[l].im = -H[a * L + l].im;
+        }
+        chol_solve_f32(Lc, inv, L, b, x);
+        for (int l = 0; l < L; l++) C[l * A + a] = x[l];
+    }
+    for (int l = 0; l < L; l++) {
+        float mu = 0.f;
+        for (int a = 0; a < A; a++) {
+            cf c = C[l * A + a], h = H[a * L + l];
+            mu = fmaf(c.re, h.re, mu);
+            mu = fmaf(-c.im, h.im, mu);
+        }
+        float im = 1.0f / mu;
+        for (int a = 0; a < A; a++) {
+            C[l * A + a].re *= im;
+            C[l * A + a].im *= im;
+        }
+        nI[l] = mu / (1.0f - mu);
+    }
+}
+
+void orc_mmse_coef(const float* G_, const float* H_, float* C_, float* nI, long nSC, int A, int L) {
+    const cf* G = (const cf*)G_;
+    const cf* H = (const cf*)H_;
+    cf* C = (cf*)C_;
+#pragma omp parallel for schedule(static)
+    for (long sc = 0; sc < nSC; sc++)
+        mmse_coef_sc_f32(G + sc * (long)L * L, H + sc * (long)A * L, A, L, C + sc * (long)L * A,
+                         nI + sc * (long)L);
+}
+
+/* ------------------------------------------------------------------------- */
+/* The plain FP32 chain (the reference's scalar method, stage by stage):     */
+/* gram -> mmse_coef -> coef_apply_v1 -> llr_v1, all FP32.  Outputs Y_eq     */
+/* (unbiased), noiseInv per (sc, layer) and FP32 LLRs.                       */
+/* ------------------------------------------------------------------------- */
+void orc_chain_f32(const float* H_, const float* Y_, float sigma2, long nSC, int A, int L,
+                   int nSym, int nPamBits, float* Yeq_, float* nI, float* llr) {
+    const cf* H = (const cf*)H_;
+    const cf* Y = (const cf*)Y_;
+    cf* Yeq = (cf*)Yeq_;
+    float D[4];
+    for (int i = 0; i < nPamBits; i++) D[i] = pam_d32(nPamBits, i);
+#pragma omp parallel for schedule(static)
+    for (long sc = 0; sc < nSC; sc++) {
+        cf G[MAXL * MAXL];
+        cf* C = (cf*)malloc(sizeof(cf) * (size_t)L * A);
+        const cf* h = H + sc * (long)A * L;
+        const cf* y = Y + sc * (long)nSym * A;
+        gram_sc_f32(h, sigma2, L, A, G);
+        mmse_coef_sc_f32(G, h, A, L, C, nI + sc * (long)L);
+        for (int l = 0; l < L; l++)
+            for (int s = 0; s < nSym; s++) {
+                cf acc = {0.f, 0.f};
+                for (int a = 0; a < A; a++) acc = cma(C[l * A + a], y[s * A + a], acc);
+                long idx = (sc * L + l) * (long)nSym + s;
+                Yeq[idx] = acc;
+                if (llr)
+                    llr_one_f32(acc.re, acc.im, nI[sc * L + l], nPamBits, D, llr + idx * 2 * nPamBits);
+            }
+        free(C);
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP64 model of the chain.                                                  */
+/*   G = H^H H + s2 I;  Cholesky;  X = G^-1 (H^H Y^T);                       */
+/*   gii = (G^-1)_ll;  mu = 1 - s2 gii;  Y_eq = X / mu;                      */
+/*   noiseInv = mu / (1 - mu) = (1 - s2 gii) / (s2 gii);  LLR max-log.       */
+/* ------------------------------------------------------------------------- */
+static void chain_sc_f64(const cf* H, const cf* Y, double s2, int A, int L, int nSym, int n,
+                         const double* D, cd* Yeq, double* nI, double* llr) {
+    cd G[MAXL * MAXL], Lc[MAXL * MAXL];
+    double inv[MAXL];
+    for (int r = 0; r < L; r++)
+        for (int c = 0; c < L; c++) {
+            double re = 0, im = 0;
+            for (int k = 0; k < A; k++) {
+                double ar = H[k * L + r].re, ai = -(double)H[k * L + r].im;
+                double br = H[k * L + c].re, bi = H[k * L + c].im;
+                re += ar * br - ai * bi;
+                im += ar * bi + ai * br;
+            }
+            if (r == c) re += s2;
+            G[r * L + c].re = re;
+            G[r * L + c].im = im;
+        }
+    for (int j = 0; j < L; j++) {
+        double s = G[j * L + j].re;
+        for (int k = 0; k < j; k++) s -= Lc[j * L + k].re * Lc[j * L + k].re + Lc[j * L + k].im * Lc[j * L + k].im;
+        if (!(s > 0)) s = 1e-300;
+        double d = sqrt(s);
+        inv[j] = 1.0 / d;
+        Lc[j * L + j].re = d;
+        Lc[j * L + j].im = 0;
+        for (int i = j + 1; i < L; i++) {
+            double re = G[i * L + j].re, im = G[i * L + j].im;
+            for (int k = 0; k < j; k++) {
+                cd a = Lc[i * L + k], b = Lc[j * L + k];
+                re -= a.re * b.re + a.im * b.im;
+                im -= a.im * b.re - a.re * b.im;
+            }
+            Lc[i * L + j].re = re * inv[j];
+            Lc[i * L + j].im = im * inv[j];
+        }
+    }
+    /* diag(G^-1): (G^-1)_ll = sum_m |(Lc^-1)[m][l]|^2 */
+    double gii[MAXL];
+    for (int l = 0; l < L; l++) {
+        cd w[MAXL];
+        for (int i = 0; i < L; i++) {
+            double re = (i == l) ? 1.0 : 0.0, im = 0.0;
+            for (int k = 0; k < i; k++) {
+                cd a = Lc[i * L + k], y = w[k];
+                re -= a.re * y.re - a.im * y.im;
+                im -= a.re * y.im + a.im * y.re;
+            }
+            w[i].re = re * inv[i];
+            w[i].im = im * inv[i];
+        }
+        double acc = 0;
+        for (int i = 0; i < L; i++) acc += w[i].re * w[i].re + w[i].im * w[i].im;
+        gii[l] = acc;
+    }
+    for (int s = 0; s < nSym; s++) {
+        cd z[MAXL], w[MAXL], x[MAXL];
+        for (int l = 0; l < L; l++) {
+            double re = 0, im = 0;
+            for (int k = 0; k < A; k++) {
+                double ar = H[k * L + l].re, ai = -(double)H[k * L + l].im;
+                double br = Y[s * A + k].re, bi = Y[s * A + k].im;
+                re += ar * br - ai * bi;
+                im += ar * bi + ai * br;
+            }
+            z[l].re = re;
+            z[l].im = im;
+        }
+        for (int i = 0; i < L; i++) {
+            double re = z[i].re, im = z[i].im;
+            for (int k = 0; k < i; k++) {
+                cd a = Lc[i * L + k], y = w[k];
+                re -= a.re * y.re - a.im * y.im;
+                im -= a.re * y.im + a.im * y.re;
+            }
+            w[i].re = re * inv[i];
+            w[i].im = im * inv[i];
+        }
+        for (int i = L - 1; i >= 0; i--) {
+            double re = w[i].re, im = w[i].im;
+            for (int k = i + 1; k < L; k++) {
+                cd a = Lc[k * L + i], y = x[k];
+                re -= a.re * y.re + a.im * y.im;
+                im -= a.re * y.im - a.im * y.re;
+            }
+            x[i].re = re * inv[i];
+            x[i].im = im * inv[i];
+        }
+        for (int l = 0; l < L; l++) {
+            double mu = 1.0 - s2 * gii[l];
+            cd v;
+            v.re = x[l].re / mu;
+            v.im = x[l].im / mu;
+            Yeq[l * nSym + s] = v;
+        }
+    }
+    for (int l = 0; l < L; l++) {
+        double t = s2 * gii[l];
+        nI[l] = (1.0 - t) / t;
+    }
+    if (llr)
+        for (int l = 0; l < L; l++)
+            for (int s = 0; s < nSym; s++)
+                llr_one_f64(Yeq[l * nSym + s].re, Yeq[l * nSym + s].im, nI[l], n, D,
+                            llr + ((long)l * nSym + s) * 2 * n);
+}
+
+void orc_chain_f64(const float* H_, const float* Y_, double sigma2, long nSC, int A, int L,
+                   int nSym, int nPamBits, double* Yeq_, double* nI, double* llr) {
+    const cf* H = (const cf*)H_;
+    const cf* Y = (const cf*)Y_;
+    cd* Yeq = (cd*)Yeq_;
+    double D[4];
+    for (int i = 0; i < nPamBits; i++) D[i] = pam_d64(nPamBits, i);
+#pragma omp parallel for schedule(static)
+    for (long sc = 0; sc < nSC; sc++)
+        chain_sc_f64(H + sc * (long)A * L, Y + sc * (long)nSym * A, sigma2, A, L, nSym, nPamBits, D,
+                     Yeq + sc * (long)L * nSym, nI + sc * (long)L,
+                     llr ? llr + sc * (long)L * nSym * 2 * nPamBits : NULL);
+}
+
+/* ------------------------------------------------------------------------- */
+/* SRS filter multiply                                                        */
+/*   H_est[blk][ant][k_out][p] = sum_k (W[k_out][k] * FOCC[p][k % F])        */
+/*                                      * SRS[blk][ant][k]                   */
+/* complex_conjmul() of src/srs/srs_wmma_bench.cu:43-47 is documented as     */
+/* conj(a)*b but computes the plain product a*b; both reference kernels use  */
+/* it, so the path's behaviour is the plain product and that is what is      */
+/* restated here.                                                            */
+/* ------------------------------------------------------------------------- */
+
+/* FP16-arithmetic restatement of srs_filter_v1_scalar (:57-90): every
+ * __hmul/__hsub/__hadd/__hfma rounded once to binary16. */
+static inline double hr(double x) { return (double)(_Float16)x; }
+void orc_srs_v1_f16(const uint16_t* srs, const uint16_t* W, const uint16_t* focc, uint16_t* out,
+                    int nAnt, int nBlocks, int K, int P, int F) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nBlocks * nAnt * K * P; i++) {
+        int p = (int)(i % P);
+        int ko = (int)((i / P) % K);
+        long ant = (i / ((long)P * K)) % nAnt;
+        long blk = i / ((long)P * K * nAnt);
+        const uint16_t* s = srs + 2 * ((blk * nAnt + ant) * K);
+        const uint16_t* w = W + 2 * ((long)ko * K);
+        const uint16_t* f = focc + 2 * ((long)p * F);
+        double er = 0, ei = 0;
+        for (int k = 0; k < K; k++) {
+            double ar = h2f(w[2 * k]), ai = h2f(w[2 * k + 1]);
+            double br = h2f(f[2 * (k % F)]), bi = h2f(f[2 * (k % F) + 1]);
+            double wr = hr(hr(ar * br) - hr(ai * bi));
+            double wi = hr(hr(ar * bi) + hr(ai * br));
+            double sr = h2f(s[2 * k]), si = h2f(s[2 * k + 1]);
+            /* hcmadd: re = hfma(wr, sr, hfma(-wi, si, er)); im = hfma(wr, si, hfma(wi, sr, ei)) */
+            double t = hr(fma(-wi, si, er));
+            er = hr(fma(wr, sr, t));
+            double u = hr(fma(wi, sr, ei));
+            ei = hr(fma(wr, si, u));
+        }
+        out[2 * i] = f2h_bits((float)er);
+        out[2 * i + 1] = f2h_bits((float)ei);
+    }
+}
+
+/* FP64 SRS filter multiply on the FP16 inputs; output double pairs. */
+void orc_srs_f64(const uint16_t* srs, const uint16_t* W, const uint16_t* focc, double* out, int nAnt,
+                 int nBlocks, int K, int P, int F) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nBlocks * nAnt * K * P; i++) {
+        int p = (int)(i % P);
+        int ko = (int)((i / P) % K);
+        long ant = (i / ((long)P * K)) % nAnt;
+        long blk = i / ((long)P * K * nAnt);
+        const uint16_t* s = srs + 2 * ((blk * nAnt + ant) * K);
+        const uint16_t* w = W + 2 * ((long)ko * K);
+        const uint16_t* f = focc + 2 * ((long)p * F);
+        double er = 0, ei = 0;
+        for (int k = 0; k < K; k++) {
+            double ar = h2f(w[2 * k]), ai = h2f(w[2 * k + 1]);
+            double br = h2f(f[2 * (k % F)]), bi = h2f(f[2 * (k % F) + 1]);
+            double wr = ar * br - ai * bi, wi = ar * bi + ai * br;
+            double sr = h2f(s[2 * k]), si = h2f(s[2 * k + 1]);
+            er += wr * sr - wi * si;
+            ei += wr * si + wi * sr;
+        }
+        out[2 * i] = er;
+        out[2 * i + 1] = ei;
+    }
+}

@@ -1,0 +1,25 @@
+// Checker shim (test infrastructure): compiles the reference's
+// src/srs/srs_wmma_bench.cu unchanged from the reference tree and exposes
+// srs_filter_v1_scalar<K,P,F> (:57-90) and srs_filter_v2_wmma<K,P,F>
+// (:102-231) for the four configurations its main() runs (:347-353), with
+// its launch shape (1,1,nBlocks) x 256 (:289-290).
+#define main srs_wmma_bench_reference_main
+#include "src/srs/srs_wmma_bench.cu"
+#undef main
+
+template <int K, int P, int F>
+static int run_srs(int v, ch2* out, const ch2* srs, const ch2* W, const ch2* focc, int nAnt, int nBlocks) {
+    dim3 blk(256), grd(1, 1, nBlocks);
+    if (v == 1) srs_filter_v1_scalar<K, P, F><<<grd, blk>>>(out, srs, W, focc, nAnt, nBlocks);
+    else srs_filter_v2_wmma<K, P, F><<<grd, blk>>>(out, srs, W, focc, nAnt, nBlocks);
+    return (int)cudaDeviceSynchronize();
+}
+extern "C" int ref_srs(int version, void* out, const void* srs, const void* W, const void* focc,
+                       int nAnt, int nBlocks, int K, int P, int F) {
+    ch2* o = (ch2*)out; const ch2* s = (const ch2*)srs; const ch2* w = (const ch2*)W; const ch2* f = (const ch2*)focc;
+    if (K == 24 && P == 4 && F == 8) return run_srs<24, 4, 8>(version, o, s, w, f, nAnt, nBlocks);
+    if (K == 24 && P == 2 && F == 8) return run_srs<24, 2, 8>(version, o, s, w, f, nAnt, nBlocks);
+    if (K == 12 && P == 4 && F == 12) return run_srs<12, 4, 12>(version, o, s, w, f, nAnt, nBlocks);
+    if (K == 12 && P == 2 && F == 12) return run_srs<12, 2, 12>(version, o, s, w, f, nAnt, nBlocks);
+    return -1;
+}

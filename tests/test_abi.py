@@ -1,0 +1,60 @@
+"""CPU tests of the C-ABI boundary: the library loads and exports every symbol
+declared in include/aerial_eq.h; no kernel is launched."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+from conftest import ROOT, load_pkg
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "aerial_eq.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(aerial_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("aerial_coef_apply", "aerial_gram", "aerial_mmse_coef", "aerial_llr", "aerial_llr_f32",
+              "aerial_srs_filter", "aerial_pusch_eq_fused", "aerial_pusch_eq_plain"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    pkg = load_pkg()
+    lib = ctypes.CDLL(pkg.LIB_PATH)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_python_mirror_binds_every_declared_symbol():
+    pkg = load_pkg()
+    assert set(declared_symbols()) <= set(pkg.SIGNATURES)
+    pkg.lib()  # binds all signatures (raises if a symbol is absent)
+
+
+def test_error_strings_and_version_without_gpu():
+    pkg = load_pkg()
+    lib = pkg.lib()
+    assert lib.aerial_version() >= 10000
+    assert b"invalid" in lib.aerial_error_string(1001)
+    assert lib.aerial_error_string(0) == b"ok"
+
+
+def test_invalid_arguments_rejected_before_any_launch():
+    """Null pointers and out-of-envelope shapes return a status, never exit()."""
+    pkg = load_pkg()
+    lib = pkg.lib()
+    assert lib.aerial_coef_apply(None, None, None, 10, 11, 8, 64, None) == 1001
+    assert lib.aerial_gram(None, 0.1, None, 10, 64, 8, None) == 1001
+    assert lib.aerial_llr(None, None, None, 10, 4, None) == 1001
+    fake = ctypes.c_void_p(0x100000)
+    assert lib.aerial_llr(fake, fake, fake, 10, 5, None) == 1001       # nPamBits > 4
+    assert lib.aerial_coef_apply(fake, fake, fake, 10, 17, 8, 64, None) == 1001   # nSym > 16
+    assert lib.aerial_coef_apply(fake, fake, fake, 10, 11, 17, 64, None) == 1001  # nLayers > 16
+    cells = (pkg.CellDesc * 1)()
+    assert lib.aerial_pusch_eq_fused(cells, 1, None, None) == 1001     # null buffers
+    assert lib.aerial_pusch_eq_fused(cells, 0, None, None) == 1001
+    assert lib.aerial_pusch_eq_fused(cells, 65, None, None) == 1001

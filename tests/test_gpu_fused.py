@@ -1,0 +1,148 @@
+"""GPU parity of the fused chain (tensor-core Gram / matched filter, FP32
+Cholesky, LLR epilogue) against the FP64 model and the plain FP32 chain.
+
+Tolerances (stated per precision):
+  FP16 / BF16x3 operands: EVM of Y_eq vs FP64 <= -45 dB (the target bar);
+  observed margins are tighter and asserted where stated.
+  LLR: max |LLR - LLR64| <= 2e-3 * max|LLR64| (relative to the LLR scale);
+  hard decisions identical to FP64 wherever |LLR64| > 1e-2 * max|LLR64|.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import evm_db
+
+pytestmark = pytest.mark.gpu
+
+
+def run_fused(aeq, cells, cuda, precision="fp16", want_yeq=True, tuning=None):
+    descs, outs = [], []
+    for c in cells:
+        H, Y = c.H.to(cuda), c.Y.to(cuda)
+        llr = torch.full((c.llr_numel,), float("nan"), dtype=torch.float32, device=cuda)
+        yeq = torch.full((c.nSC * c.nLayers * c.nSym,), float("nan"), dtype=torch.complex64, device=cuda) \
+            if want_yeq else None
+        descs.append(aeq.cell_desc(H, Y, llr, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, Y_eq=yeq))
+        outs.append((H, Y, llr, yeq))
+    t = tuning if tuning is not None else aeq.make_tuning(precision)
+    aeq.pusch_eq_fused(descs, t)
+    torch.cuda.synchronize()
+    return [(o[2].cpu().numpy(), o[3].cpu().numpy() if o[3] is not None else None) for o in outs]
+
+
+def oracle64(orc, c):
+    return orc.chain_f64(c.H.numpy(), c.Y.numpy(), c.sigma2, c.nSC, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+
+
+def check_against_fp64(orc, c, llr, yeq, evm_max=-45.0):
+    y64, n64, l64 = oracle64(orc, c)
+    assert np.all(np.isfinite(llr)), "unwritten LLRs"
+    e = evm_db(yeq, y64)
+    assert e <= evm_max, f"EVM {e:.1f} dB > {evm_max} dB"
+    scale = np.abs(l64).max()
+    err = np.abs(llr.astype(np.float64) - l64)
+    assert err.max() <= 2e-3 * scale, (err.max(), scale)
+    sure = np.abs(l64) > 1e-2 * scale
+    assert np.array_equal((llr < 0)[sure], (l64 < 0)[sure])
+    return e
+
+
+@pytest.mark.parametrize("cfg,prec,evm_max", [(1, "fp16", -55.0), (2, "fp16", -55.0), (1, "bf16x3", -80.0),
+                                               (2, "bf16x3", -80.0), (2, "bf16", -40.0)])
+def test_fused_configs_vs_fp64(aeq, wl, orc, cuda, cfg, prec, evm_max):
+    c = wl.config_cell(cfg, seed=11)
+    (llr, yeq), = run_fused(aeq, [c], cuda, prec)
+    if prec == "bf16":  # 8-bit mantissa operands: report, bound loosely
+        y64, _, _ = oracle64(orc, c)
+        assert evm_db(yeq, y64) <= evm_max
+        return
+    check_against_fp64(orc, c, llr, yeq, evm_max)
+
+
+@pytest.mark.parametrize("prec,evm_max", [("bf16x3", -60.0), ("fp16", -45.0)])
+def test_fused_cfg3_correlated_channel(aeq, wl, orc, cuda, prec, evm_max):
+    """273 PRB x 128 ant x 16 layers, rho = 0.7 correlated, SNR 30 dB."""
+    c = wl.config_cell(3, seed=13)
+    (llr, yeq), = run_fused(aeq, [c], cuda, prec)
+    check_against_fp64(orc, c, llr, yeq, evm_max)
+
+
+EDGE = [  # (nPRB, nAnt, nLayers, nSym, qam)
+    (1, 8, 1, 1, 4),
+    (1, 16, 2, 7, 16),
+    (1, 32, 3, 8, 64),
+    (2, 64, 4, 9, 256),
+    (1, 33, 5, 14, 16),
+    (1, 7, 6, 16, 4),
+    (3, 128, 8, 11, 64),
+    (1, 64, 12, 11, 256),
+    (1, 256, 16, 16, 16),
+    (5, 24, 7, 3, 256),
+]
+
+
+@pytest.mark.parametrize("shape", EDGE)
+def test_fused_edge_shapes(aeq, wl, orc, cuda, shape):
+    nPRB, A, L, S, q = shape
+    c = wl.make_cell(nPRB, A, L, S, q, 25.0, seed=17)
+    (llr, yeq), = run_fused(aeq, [c], cuda, "bf16x3")
+    check_against_fp64(orc, c, llr, yeq, -60.0)
+
+
+def test_fused_vs_plain_chain(aeq, wl, orc, cuda):
+    """The fused FP16 path and the plain FP32 chain agree at the EVM bar."""
+    c = wl.config_cell(2, seed=19)
+    (llr, yeq), = run_fused(aeq, [c], cuda, "fp16")
+    y32, _, l32 = orc.chain_f32(c.H.numpy(), c.Y.numpy(), c.sigma2, c.nSC, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+    assert evm_db(yeq, y32) <= -50.0
+
+
+def test_multicell_same_alone_and_in_mix(aeq, wl, cuda):
+    """Per-cell results are bit-identical whether a cell runs alone or inside
+    a 16-cell uneven batch (one persistent launch)."""
+    cells = wl.multicell(16, seed=23)
+    mixed = run_fused(aeq, cells, cuda, "fp16")
+    for i in (0, 5, 15):
+        alone = run_fused(aeq, [cells[i]], cuda, "fp16")[0]
+        np.testing.assert_array_equal(alone[0], mixed[i][0])
+        np.testing.assert_array_equal(alone[1], mixed[i][1])
+
+
+def test_multicell_vs_fp64(aeq, wl, orc, cuda):
+    cells = wl.multicell(16, seed=29)
+    res = run_fused(aeq, cells, cuda, "fp16")
+    for c, (llr, yeq) in zip(cells, res):
+        check_against_fp64(orc, c, llr, yeq, -45.0)
+
+
+def test_fused_without_yeq_and_launch_shapes(aeq, wl, cuda):
+    c = wl.config_cell(1, seed=31)
+    ref = run_fused(aeq, [c], cuda, "fp16")[0][0]
+    for w, k in ((2, 4), (4, 1), (4, 2), (8, 1)):
+        got = run_fused(aeq, [c], cuda, "fp16", want_yeq=False,
+                        tuning=aeq.make_tuning("fp16", w, k))[0][0]
+        np.testing.assert_array_equal(got, ref)
+
+
+def test_autotune_returns_valid_shape(aeq, wl, cuda):
+    c = wl.config_cell(2, seed=37)
+    H, Y = c.H.to(cuda), c.Y.to(cuda)
+    llr = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+    d = aeq.cell_desc(H, Y, llr, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+    t, us = aeq.autotune([d], "fp16")
+    assert t.warps_per_cta in (2, 4, 6, 8) and t.ctas_per_sm >= 1 and us > 0
+
+
+def test_fused_rejects_bad_cells(aeq, wl, cuda):
+    c = wl.config_cell(1, seed=41)
+    H, Y = c.H.to(cuda), c.Y.to(cuda)
+    llr = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+    d = aeq.cell_desc(H, Y, llr, c.sigma2, c.nPRB, c.nAnt, 17, c.nSym, c.nPamBits)
+    with pytest.raises(aeq.AerialError):
+        aeq.pusch_eq_fused([d])
+    d = aeq.cell_desc(H, Y, llr, c.sigma2, c.nPRB, c.nAnt, c.nLayers, 17, c.nPamBits)
+    with pytest.raises(aeq.AerialError):
+        aeq.pusch_eq_fused([d])

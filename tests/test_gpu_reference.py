@@ -1,0 +1,113 @@
+"""GPU parity against the reference's OWN kernels, compiled unchanged from its
+sources for sm_100a into oracle/_ref/ (oracle/Makefile, target `ref`).
+Skipped when those checker libraries were not built (e.g. no reference tree
+was available where the repository was built)."""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+REFLIB = os.path.join(ROOT, "oracle", "_ref")
+VP, CI = ctypes.c_void_p, ctypes.c_int
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+import make_golden as MG  # noqa: E402
+
+
+def _ref(name):
+    p = os.path.join(REFLIB, f"libref_{name}.so")
+    if not os.path.exists(p):
+        pytest.skip(f"{p} not built")
+    return ctypes.CDLL(p)
+
+
+def _d(x, dev):
+    return torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+
+
+def test_coef_apply_bit_exact_vs_reference_v1(aeq, orc, cuda):
+    lib = _ref("coef")
+    lib.ref_coef_v1.argtypes = [VP, VP, VP, CI, CI]
+    nSC, S = 1584, 11
+    C, Y = MG.coef_inputs(7, nSC, S)
+    dC, dY = _d(C, cuda), _d(Y, cuda)
+    ref = torch.empty(nSC * 8 * S, dtype=torch.complex64, device=cuda)
+    assert lib.ref_coef_v1(dC.data_ptr(), dY.data_ptr(), ref.data_ptr(), nSC, S) == 0
+    mine = torch.empty_like(ref)
+    aeq.coef_apply(dC, dY, mine, nSC, S, 8, 64)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(mine.cpu().numpy(), ref.cpu().numpy())
+    np.testing.assert_array_equal(orc.coef_apply_v1(C.view(np.complex64), Y.view(np.complex64), nSC, S, 8, 64),
+                                  ref.cpu().numpy())
+
+
+def test_coef_apply_tc_vs_reference_v2(aeq, cuda):
+    lib = _ref("coef")
+    lib.ref_coef_v2.argtypes = [VP, VP, VP, CI, CI]
+    nSC, S = 1584, 11
+    C, Y = MG.coef_inputs(7, nSC, S)
+    dC, dY = _d(C, cuda), _d(Y, cuda)
+    ref = torch.empty(nSC * 8 * S, dtype=torch.complex64, device=cuda)
+    assert lib.ref_coef_v2(dC.data_ptr(), dY.data_ptr(), ref.data_ptr(), nSC, S) == 0
+    mine = torch.empty_like(ref)
+    aeq.coef_apply_tc(dC, dY, mine, nSC, S, 8, 64)
+    torch.cuda.synchronize()
+    a, b = mine.cpu().numpy().astype(np.complex128), ref.cpu().numpy().astype(np.complex128)
+    assert 10 * np.log10(np.sum(np.abs(a - b) ** 2) / np.sum(np.abs(b) ** 2)) < -110
+
+
+def test_gram_bit_exact_vs_reference(aeq, cuda):
+    lib = _ref("gram")
+    lib.ref_gram.argtypes = [VP, VP, VP, CI]
+    nSC = 1584
+    H, M = MG.gram_inputs(11, nSC)
+    dH = _d(H, cuda)
+    ref = torch.empty(nSC * 64, dtype=torch.complex64, device=cuda)
+    assert lib.ref_gram(_d(M, cuda).data_ptr(), dH.data_ptr(), ref.data_ptr(), nSC) == 0
+    mine = torch.empty_like(ref)
+    aeq.gram(dH, 0.0, mine, nSC, 64, 8)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(mine.cpu().numpy(), ref.cpu().numpy())
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4])
+def test_llr_bit_exact_vs_reference_v1_v3(aeq, orc, cuda, n):
+    lib = _ref("llr_v3")
+    lib.ref_llr_v3_v1.argtypes = [VP, VP, VP, CI, CI]
+    lib.ref_llr_v3_v3.argtypes = [VP, VP, VP, CI, CI]
+    N = 139392
+    soft, ni = orc.ref_llr_inputs(42, N)
+    ds, dn = _d(soft.view(np.int16), cuda), _d(ni, cuda)
+    r1 = torch.empty(N * 2 * n, dtype=torch.int16, device=cuda)
+    assert lib.ref_llr_v3_v1(ds.data_ptr(), dn.data_ptr(), r1.data_ptr(), N, n) == 0
+    mine = torch.empty_like(r1)
+    aeq.llr(ds, dn, mine, N, n)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(mine.cpu().numpy(), r1.cpu().numpy())
+    if n >= 2:
+        r3 = torch.empty_like(r1)
+        assert lib.ref_llr_v3_v3(ds.data_ptr(), dn.data_ptr(), r3.data_ptr(), N, n) == 0
+        np.testing.assert_array_equal(mine.cpu().numpy(), r3.cpu().numpy())
+    np.testing.assert_array_equal(orc.llr_f16io(soft, ni, n), r1.cpu().numpy().view(np.uint16))
+
+
+@pytest.mark.parametrize("K,P,F", MG.SRS_CFGS)
+def test_srs_oracle_bit_exact_vs_reference_v1(orc, cuda, K, P, F):
+    """The oracle's FP16-arithmetic restatement equals srs_filter_v1_scalar."""
+    lib = _ref("srs")
+    lib.ref_srs.argtypes = [CI, VP, VP, VP, VP, CI, CI, CI, CI, CI]
+    nBlk, nAnt = 66, 64
+    s, w, f = orc.ref_srs_inputs(42, nBlk * nAnt * K, K * K, P * F)
+    o = torch.empty(nBlk * nAnt * K * P * 2, dtype=torch.int16, device=cuda)
+    assert lib.ref_srs(1, o.data_ptr(), _d(s.view(np.int16), cuda).data_ptr(), _d(w.view(np.int16), cuda).data_ptr(),
+                       _d(f.view(np.int16), cuda).data_ptr(), nAnt, nBlk, K, P, F) == 0
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(orc.srs_v1_f16(s, w, f, nAnt, nBlk, K, P, F), o.cpu().numpy().view(np.uint16))

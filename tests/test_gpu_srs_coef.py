@@ -1,0 +1,69 @@
+"""GPU parity of the SRS filter multiply and the tensor-core coef_apply."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import cosine, evm_db
+
+pytestmark = pytest.mark.gpu
+
+
+def _d(x, dev):
+    return torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+
+
+SRS_CFGS = [(24, 4, 8), (24, 2, 8), (12, 4, 12), (12, 2, 12), (8, 1, 4)]
+
+
+@pytest.mark.parametrize("K,P,F", SRS_CFGS)
+def test_srs_filter_vs_fp64(aeq, orc, cuda, K, P, F):
+    nBlk, nAnt = 66, 64
+    s, w, f = orc.ref_srs_inputs(42, nBlk * nAnt * K, K * K, P * F)
+    out = torch.empty(nBlk * nAnt * K * P * 2, dtype=torch.int16, device=cuda)
+    aeq.srs_filter(out, _d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda),
+                   nAnt, nBlk, K, P, F)
+    torch.cuda.synchronize()
+    got16 = out.cpu().numpy().view(np.uint16)
+    got = np.empty(got16.size, np.float32)
+    orc.lib().orc_f16_to_f32(got16, got, got.size)
+    ref = orc.srs_f64(s, w, f, nAnt, nBlk, K, P, F)
+    g = got.view(np.complex64).astype(np.complex128)
+    # FP32 sums rounded once to FP16: error <= half an FP16 ulp of each component
+    tol = np.maximum(np.abs(ref.real), np.abs(ref.imag)) * 2.0 ** -11 + 2.0 ** -24
+    assert np.all(np.abs(g.real - ref.real) <= tol + 1e-6 * np.abs(ref).max())
+    assert np.all(np.abs(g.imag - ref.imag) <= tol + 1e-6 * np.abs(ref).max())
+    # and close to the reference's FP16-arithmetic V1 (its own check is cosine, :328)
+    v1 = orc.srs_v1_f16(s, w, f, nAnt, nBlk, K, P, F)
+    v1f = np.empty(v1.size, np.float32)
+    orc.lib().orc_f16_to_f32(v1, v1f, v1f.size)
+    assert cosine(v1f.view(np.complex64), g) > 0.9999
+
+
+def test_srs_to_channel_layout(aeq, orc, cuda):
+    K, P, F, nBlk, nAnt = 24, 4, 8, 66, 64
+    s, w, f = orc.ref_srs_inputs(43, nBlk * nAnt * K, K * K, P * F)
+    H = torch.empty(nBlk * K, nAnt, P, dtype=torch.complex64, device=cuda)
+    aeq.srs_to_channel(H, _d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda),
+                       nAnt, nBlk, K, P, F)
+    torch.cuda.synchronize()
+    ref = orc.srs_f64(s, w, f, nAnt, nBlk, K, P, F).reshape(nBlk, nAnt, K, P)
+    ref = ref.transpose(0, 2, 1, 3).reshape(nBlk * K, nAnt, P)   # [sc][ant][layer]
+    assert evm_db(H.cpu().numpy(), ref) < -120
+
+
+@pytest.mark.parametrize("shape", [(1584, 11, 8, 64), (288, 11, 4, 32), (48, 14, 16, 128), (12, 3, 5, 33)])
+def test_coef_apply_tc_vs_v2_model(aeq, orc, cuda, shape):
+    nSC, S, L, A = shape
+    v = orc.ref_uniform(7, nSC * L * A * 2 + nSC * S * A * 2, 1.4)
+    C = v[: nSC * L * A * 2].view(np.complex64)
+    Y = v[nSC * L * A * 2:].view(np.complex64)
+    O = torch.empty(nSC * L * S, dtype=torch.complex64, device=cuda)
+    aeq.coef_apply_tc(_d(C, cuda), _d(Y, cuda), O, nSC, S, L, A)
+    torch.cuda.synchronize()
+    got = O.cpu().numpy()
+    v2 = orc.coef_apply_v2_model(C, Y, nSC, S, L, A)
+    v1 = orc.coef_apply_v1(C, Y, nSC, S, L, A)
+    assert evm_db(got, v2) < -110          # same FP16 operands, only accumulation order differs
+    assert evm_db(got, v1) < -65           # the reference's V2-vs-V1 bar is -70.3 dB at 64 ant
