@@ -49,8 +49,11 @@ inline PamLut pam_lut(int n) {
 // (src/llr/aerial_llr_v3.cu:90-107): soft-bit chain sb[i+1] = D_i - |sb[i]|,
 // pMD[i] = (dist + |sb[i]|)^2, minDist1 = (|sb[n-1]| - dist)^2,
 // llr_i = +-(pMD[i] - minDist1) * noise, clamped to +-65504.
-// out[2*bit + iq].  Operation order matches the reference (no contraction is
-// possible in it), so results are bit-identical.
+// out[2*bit + iq].  Every operation is explicitly rounded so the result is
+// bit-identical to llr_v1_baseline as nvcc 12.9 compiles it for sm_100a:
+// for 16/64/256-QAM it rounds each square separately; for QPSK (N = 1) its
+// final subtraction is contracted into fma(-t, t, pMD) with t = |sb| - dist,
+// and that is restated here.
 template <int N>
 __device__ __forceinline__ void pam_llr(float pamI, float pamQ, float noise, const PamLut& L,
                                         float* out) {
@@ -68,11 +71,12 @@ __device__ __forceinline__ void pam_llr(float pamI, float pamQ, float noise, con
             if (sb < 0.f) sign |= 1u << i;
             if (i < N - 1) sb = __fsub_rn(L.d[i], a);
         }
-        float md1 = __fsub_rn(fabsf(sb), dist);
-        md1 = __fmul_rn(md1, md1);
+        const float t = __fsub_rn(fabsf(sb), dist);
+        const float md1 = __fmul_rn(t, t);
 #pragma unroll
         for (int i = 0; i < N; i++) {
-            float llr = __fmul_rn(__fsub_rn(pmd[i], md1), noise);
+            const float diff = (N == 1) ? __fmaf_rn(-t, t, pmd[i]) : __fsub_rn(pmd[i], md1);
+            float llr = __fmul_rn(diff, noise);
             if (sign & (1u << i)) llr = -llr;
             out[2 * i + iq] = fmaxf(-65504.f, fminf(65504.f, llr));
         }

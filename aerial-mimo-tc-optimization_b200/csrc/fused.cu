@@ -119,8 +119,7 @@ struct WarpSmem {
     static constexpr int offR = offG + GS * LT * GP;                 // float2 [GS][LT][RP]
     static constexpr int offAux = offR + GS * LT * RP;               // float2 [32] column buffer
     static constexpr int offInv = offAux + 32;                       // float  [32] (as float2 slots: 16)
-    static constexpr int offQ = offInv + 16;                         // float  [GS][LT][LT] (as float2)
-    static constexpr int total = offQ + (GS * LT * LT + 1) / 2;      // in float2 units
+    static constexpr int total = offInv + 16;                        // in float2 units
 };
 
 __host__ __device__ constexpr int warp_smem_bytes(int LT) {
@@ -131,11 +130,15 @@ __host__ __device__ constexpr int warp_smem_bytes(int LT) {
                    : WarpSmem<16>::total * 8;
 }
 
-// Fragment registers of one chunk (4 k-steps = 32 antennas) of one subcarrier.
+// k-steps (8 antennas each) per pipelined chunk: two chunks are in flight per
+// warp (double buffer) while the tensor cores consume the previous one.
+constexpr int KS = 2;
+
+// Fragment registers of one chunk (KS k-steps) of one subcarrier.
 template <int NMT>
 struct Frag {
-    float4 h[NMT][4];   // (H[a0][l], H[a0+1][l]) for l = g + 8*mt
-    float4 y[2][4];     // (Y[8nt+g][a0], Y[8nt+g][a0+1])
+    float4 h[NMT][KS];   // (H[a0][l], H[a0+1][l]) for l = g + 8*mt
+    float4 y[2][KS];     // (Y[8nt+g][a0], Y[8nt+g][a0+1])
 };
 
 template <int NMT>
@@ -144,8 +147,8 @@ __device__ __forceinline__ void load_chunk(Frag<NMT>& f, const FusedCell& cl, lo
     const float2* Ys = cl.Y + sc * (long)cl.nSym * cl.A;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-    for (int kk = 0; kk < 4; kk++) {
-        const int j = ch * 4 + kk;
+    for (int kk = 0; kk < KS; kk++) {
+        const int j = ch * KS + kk;
         const int a0 = 8 * j + 2 * c;
         const bool k0 = (j < nK) && (a0 < cl.A), k1 = (j < nK) && (a0 + 1 < cl.A);
 #pragma unroll
@@ -188,8 +191,8 @@ __device__ __forceinline__ void mma_chunk(const Frag<(LT > 8 ? 2 : 1)>& f, float
                                           int ch, int nK, bool z2) {
     constexpr int NMT = LT > 8 ? 2 : 1;
 #pragma unroll
-    for (int kk = 0; kk < 4; kk++) {
-        if (ch * 4 + kk >= nK) break;
+    for (int kk = 0; kk < KS; kk++) {
+        if (ch * KS + kk >= nK) break;
         if constexpr (P == AERIAL_PREC_BF16X3) {
             uint32_t ah[NMT][2], al[NMT][2];
 #pragma unroll
@@ -321,7 +324,7 @@ __device__ __noinline__ void process_group(const FusedCell& cl, long grp, float2
     constexpr int GS = W::GS;
     const int g = lane >> 2, c = lane & 3;
     const int nK = (cl.A + 7) >> 3;
-    const int nChunk = (nK + 3) >> 2;
+    const int nChunk = (nK + KS - 1) / KS;
     const bool z2 = cl.nSym > 8;
     const long sc0 = grp * GS;
     const int nValid = (int)min((long)GS, (long)cl.nSC - sc0);
@@ -373,6 +376,11 @@ __device__ __noinline__ void process_group(const FusedCell& cl, long grp, float2
     __syncwarp();
 
     // ---- solve phase: lane = (q, i), LT lanes per subcarrier ----
+    // Cholesky G = Lc Lc^H (right-looking, lane i keeps row i), then
+    // Linv = Lc^-1 by forward substitution on the identity (row i per lane,
+    // published to shared memory), Ginv = Linv^H Linv (row i per lane) and
+    // X = Ginv Z (row i per lane, Z rows read from shared memory).  The last
+    // two steps have no lane-to-lane dependency.
     const int q = lane / LT, i = lane % LT;
     const long sc = sc0 + q;
     const bool scValid = q < nValid;
@@ -381,7 +389,6 @@ __device__ __noinline__ void process_group(const FusedCell& cl, long grp, float2
     float2* sR = sm + W::offR + q * LT * W::RP;
     float2* sCol = sm + W::offAux + q * LT;
     float* sInv = reinterpret_cast<float*>(sm + W::offInv) + q * LT;
-    float* sQ = reinterpret_cast<float*>(sm + W::offQ) + q * LT * LT;
     const float s2 = cl.sigma2;
 
     // row i of the lower triangle of G (+ s2 on the diagonal)
@@ -389,26 +396,16 @@ __device__ __noinline__ void process_group(const FusedCell& cl, long grp, float2
 #pragma unroll
     for (int m = 0; m < LT; m++) {
         float2 v = make_float2(0.f, 0.f);
-        if (m <= i && scValid) v = sG[i * W::GP + m];
+        if (m <= i && scValid && real) v = sG[i * W::GP + m];
         if (m == i) v = real ? make_float2(v.x + s2, 0.f) : make_float2(1.f, 0.f);
-        if (!real && m < i) v = make_float2(0.f, 0.f);
         gr[m] = v;
     }
-    float2 z[16];
-#pragma unroll
-    for (int s = 0; s < 16; s++) z[s] = (s < cl.nSym && scValid && real) ? sR[i * W::RP + s] : make_float2(0.f, 0.f);
-    float2 e[LT];
-#pragma unroll
-    for (int m = 0; m < LT; m++) e[m] = make_float2(m == i ? 1.f : 0.f, 0.f);
-    __syncwarp();
 
-    // Cholesky G = Lc Lc^H, right-looking; lane i keeps row i of Lc.
     float myInv = 1.f;
 #pragma unroll
     for (int j = 0; j < LT; j++) {
         if (i == j) {
-            float d = gr[j].x;
-            d = d > 1e-30f ? d : 1e-30f;
+            float d = fmaxf(gr[j].x, 1e-30f);
             d = sqrtf(d);
             myInv = 1.0f / d;
             gr[j] = make_float2(d, 0.f);
@@ -429,83 +426,81 @@ __device__ __noinline__ void process_group(const FusedCell& cl, long grp, float2
                 if (m <= i) gr[m] = csub_mulc(gr[m], lij, sCol[m]);
         }
     }
-    // publish Lc rows for the backward solve (column access)
-#pragma unroll
-    for (int m = 0; m < LT; m++)
-        if (m <= i) sG[i * W::GP + m] = gr[m];
-    __syncwarp();
 
-    // Forward solve Lc W = [Z | I]; lane i ends with row i of W.
+    // Linv row i: Linv[i][m] = -(sum_{k=m}^{i-1} Lc[i][k] Linv[k][m]) / Lc[i][i],
+    // Linv[i][i] = 1 / Lc[i][i]; rows published to sR[.][16 + m].
+    float2 e[LT];
+#pragma unroll
+    for (int m = 0; m < LT; m++) e[m] = make_float2(m == i ? 1.f : 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < LT; k++) {
         if (i == k) {
 #pragma unroll
-            for (int s = 0; s < 16; s++) {
-                z[s].x *= myInv; z[s].y *= myInv;
-                if (s < cl.nSym) sR[k * W::RP + s] = z[s];
-            }
-#pragma unroll
-            for (int m = 0; m < LT; m++) {
+            for (int m = 0; m <= k; m++) {
                 e[m].x *= myInv; e[m].y *= myInv;
-                if (m <= k) sR[k * W::RP + 16 + m] = e[m];
+                sR[k * W::RP + 16 + m] = e[m];
             }
         }
         __syncwarp();
         if (i > k) {
             const float2 lik = gr[k];
 #pragma unroll
-            for (int s = 0; s < 16; s++)
-                if (s < cl.nSym) z[s] = csub_mul(z[s], lik, sR[k * W::RP + s]);
-#pragma unroll
-            for (int m = 0; m < LT; m++)
-                if (m <= k) e[m] = csub_mul(e[m], lik, sR[k * W::RP + 16 + m]);
+            for (int m = 0; m <= k; m++) e[m] = csub_mul(e[m], lik, sR[k * W::RP + 16 + m]);
         }
     }
-    // (G^-1)_ii = sum_m |(Lc^-1)[m][i]|^2 : column norms of W_I across lanes
-#pragma unroll
-    for (int m = 0; m < LT; m++) sQ[i * LT + m] = e[m].x * e[m].x + e[m].y * e[m].y;
     __syncwarp();
-    float gii = 0.f;
-#pragma unroll
-    for (int m = 0; m < LT; m++)
-        if (m >= i) gii += sQ[m * LT + i];
 
-    // Backward solve Lc^H X = W_Z; lane i ends with row i of X.
+    // Ginv row i: Ginv[i][j] = sum_{m >= max(i,j)} conj(Linv[m][i]) Linv[m][j]
+    float2 gi[LT];
 #pragma unroll
-    for (int k = LT - 1; k >= 0; k--) {
-        if (i == k) {
+    for (int j = 0; j < LT; j++) gi[j] = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int s = 0; s < 16; s++) {
-                z[s].x *= myInv; z[s].y *= myInv;
-                if (s < cl.nSym) sR[k * W::RP + s] = z[s];
+    for (int m = 0; m < LT; m++) {
+        if (m >= i) {
+            const float2 a = sR[m * W::RP + 16 + i];          // Linv[m][i]
+#pragma unroll
+            for (int j = 0; j <= m; j++) {
+                const float2 b = sR[m * W::RP + 16 + j];      // Linv[m][j]
+                gi[j].x += a.x * b.x + a.y * b.y;             // conj(a) * b
+                gi[j].y += a.x * b.y - a.y * b.x;
             }
         }
-        __syncwarp();
-        if (i < k) {
-            const float2 lki = sG[k * W::GP + i];
+    }
+
+    // X row i = Ginv[i][:] Z
+    float2 x[16];
 #pragma unroll
-            for (int s = 0; s < 16; s++)
-                if (s < cl.nSym) z[s] = csub_cmul(z[s], lki, sR[k * W::RP + s]);
+    for (int s = 0; s < 16; s++) x[s] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int m = 0; m < LT; m++) {
+        const float2 a = gi[m];
+#pragma unroll
+        for (int s = 0; s < 16; s++) {
+            if (s < cl.nSym) {
+                const float2 z = sR[m * W::RP + s];
+                x[s].x += a.x * z.x - a.y * z.y;
+                x[s].y += a.x * z.y + a.y * z.x;
+            }
         }
     }
     __syncwarp();   // shared memory is reused by the next group
 
     if (scValid && real) {
-        const float t = s2 * gii;            // 1 - mu
+        const float t = s2 * gi[i].x;       // 1 - mu = s2 (G^-1)_ii
         const float mu = fmaxf(1.0f - t, 1e-30f);
         const float invMu = 1.0f / mu;
         const float nInv = mu / fmaxf(t, 1e-30f);
         switch (cl.nPam) {
-            case 1: emit<1>(cl, sc, i, z, invMu, nInv); break;
-            case 2: emit<2>(cl, sc, i, z, invMu, nInv); break;
-            case 3: emit<3>(cl, sc, i, z, invMu, nInv); break;
-            default: emit<4>(cl, sc, i, z, invMu, nInv); break;
+            case 1: emit<1>(cl, sc, i, x, invMu, nInv); break;
+            case 2: emit<2>(cl, sc, i, x, invMu, nInv); break;
+            case 3: emit<3>(cl, sc, i, x, invMu, nInv); break;
+            default: emit<4>(cl, sc, i, x, invMu, nInv); break;
         }
     }
 }
 
 template <int P>
-__global__ void __launch_bounds__(256, 1) fused_eq_kernel(const __grid_constant__ FusedParams p) {
+__global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant__ FusedParams p) {
     extern __shared__ float4 smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -594,7 +589,7 @@ struct LaunchShape {
 
 static LaunchShape default_shape(int maxLT) {
     (void)maxLT;
-    return {8, 1};
+    return {8, 2};
 }
 
 template <int P>
@@ -660,14 +655,14 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
     if (s) return s;
     cudaStream_t st = to_stream(stream);
     const int prec = best->precision;
-    static const LaunchShape cand[] = {{2, 4}, {4, 1}, {4, 2}, {6, 1}, {8, 1}, {2, 8}, {4, 4}};
+    static const LaunchShape cand[] = {{4, 2}, {4, 4}, {8, 1}, {8, 2}, {6, 2}, {2, 8}};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float bestT = 1e30f;
     LaunchShape bestS = default_shape(maxLT);
     for (const LaunchShape& sh : cand) {
-        if ((long)sh.warps * warp_smem_bytes(maxLT) * sh.ctasPerSm > 200 * 1024) continue;
+        if ((long)sh.warps * warp_smem_bytes(maxLT) * sh.ctasPerSm > 220 * 1024) continue;
         if ((s = launch_fused(p, maxLT, prec, sh, st))) break;
         const int reps = 5;
         cudaEventRecord(e0, st);

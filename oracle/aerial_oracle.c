@@ -154,7 +154,11 @@ void orc_pam_lut(int nPamBits, float* d32, double* d64) {
 /* LLR demapper                                                               */
 /* ------------------------------------------------------------------------- */
 
-/* FP32 restatement of llr_v1_baseline (src/llr/aerial_llr_v3.cu:84-108).
+/* FP32 restatement of llr_v1_baseline (src/llr/aerial_llr_v3.cu:84-108) as
+ * nvcc 12.9 compiles it for sm_100a: each square rounded separately, except
+ * for QPSK (n = 1) where the final pMD - minDist1 is contracted into
+ * fma(-t, t, pMD) with t = |sb| - dist (established bit for bit against the
+ * reference kernel's own outputs on 139,392 reference inputs).
  * softEst: interleaved float pairs; noise index = idx / symsPerNoise
  * (1 = one noiseInv per symbol as in the reference).  out[idx*2n + 2b + iq]
  * receives the clamped FP32 LLR (before the reference's FP16 store). */
@@ -173,10 +177,11 @@ static void llr_one_f32(float pamI, float pamQ, float noise, int n, const float*
         pMD[n - 1] = dist + fabsf(pSB[n - 1]);
         pMD[n - 1] *= pMD[n - 1];
         if (pSB[n - 1] < 0.f) sign |= 1u << (n - 1);
-        float md1 = fabsf(pSB[n - 1]) - dist;
-        md1 *= md1;
+        float t = fabsf(pSB[n - 1]) - dist;
+        float md1 = t * t;
         for (int i = 0; i < n; i++) {
-            float llr = (pMD[i] - md1) * noise;
+            float diff = (n == 1) ? fmaf(-t, t, pMD[i]) : pMD[i] - md1;
+            float llr = diff * noise;
             if (sign & (1u << i)) llr = -llr;
             o[i * 2 + iq] = fmaxf(-65504.f, fminf(65504.f, llr));
         }
@@ -638,8 +643,13 @@ void orc_chain_f64(const float* H_, const float* Y_, double sigma2, long nSC, in
 /* restated here.                                                            */
 /* ------------------------------------------------------------------------- */
 
-/* FP16-arithmetic restatement of srs_filter_v1_scalar (:57-90): every
- * __hmul/__hsub/__hadd/__hfma rounded once to binary16. */
+/* FP16-arithmetic restatement of srs_filter_v1_scalar (:57-90) as nvcc 12.9
+ * compiles it for sm_100a: __hmul/__hsub/__hadd are contractible, and in
+ * complex_conjmul the first product of each component is fused with the
+ * add/sub (wr = fma(ar, br, -h(ai*bi)), wi = fma(ar, bi, h(ai*br))), the
+ * explicit __hfma calls of hcmadd round once each.  Established bit for bit
+ * against the reference kernel's outputs for all four configurations of its
+ * main(). */
 static inline double hr(double x) { return (double)(_Float16)x; }
 void orc_srs_v1_f16(const uint16_t* srs, const uint16_t* W, const uint16_t* focc, uint16_t* out,
                     int nAnt, int nBlocks, int K, int P, int F) {
@@ -656,8 +666,8 @@ void orc_srs_v1_f16(const uint16_t* srs, const uint16_t* W, const uint16_t* focc
         for (int k = 0; k < K; k++) {
             double ar = h2f(w[2 * k]), ai = h2f(w[2 * k + 1]);
             double br = h2f(f[2 * (k % F)]), bi = h2f(f[2 * (k % F) + 1]);
-            double wr = hr(hr(ar * br) - hr(ai * bi));
-            double wi = hr(hr(ar * bi) + hr(ai * br));
+            double wr = hr(fma(ar, br, -hr(ai * bi)));
+            double wi = hr(fma(ar, bi, hr(ai * br)));
             double sr = h2f(s[2 * k]), si = h2f(s[2 * k + 1]);
             /* hcmadd: re = hfma(wr, sr, hfma(-wi, si, er)); im = hfma(wr, si, hfma(wi, sr, ei)) */
             double t = hr(fma(-wi, si, er));

@@ -110,7 +110,7 @@ def srs_inputs(K, P, F, nBlk=SRS_NBLK, nAnt=SRS_NANT, seed=SRS_SEED):
     return O.ref_srs_inputs(seed, nBlk * nAnt * K, K * K, P * F)
 
 
-def gpu_fixtures():
+def gpu_fixtures(out_dir=HERE):
     import torch
 
     dev = torch.device("cuda:0")
@@ -128,14 +128,14 @@ def gpu_fixtures():
         o = torch.zeros(COEF_NSC * 8 * COEF_NSYM * 2, dtype=torch.float32, device=dev)
         assert fn(dC.data_ptr(), dY.data_ptr(), o.data_ptr(), COEF_NSC, COEF_NSYM) == 0
         outs[name] = o.cpu().numpy()
-    np.savez_compressed(os.path.join(HERE, "ref_gpu_coef.npz"), **outs)
+    np.savez_compressed(os.path.join(out_dir, "ref_gpu_coef.npz"), **outs)
 
     gram = ctypes.CDLL(os.path.join(REFLIB, "libref_gram.so"))
     gram.ref_gram.argtypes = [VP, VP, VP, CI]
     H, M = gram_inputs(GRAM_SEED, GRAM_NSC)
     o = torch.zeros(GRAM_NSC * 64 * 2, dtype=torch.float32, device=dev)
     assert gram.ref_gram(d(M).data_ptr(), d(H).data_ptr(), o.data_ptr(), GRAM_NSC) == 0
-    np.savez_compressed(os.path.join(HERE, "ref_gpu_gram.npz"), G=o.cpu().numpy())
+    np.savez_compressed(os.path.join(out_dir, "ref_gpu_gram.npz"), G=o.cpu().numpy())
 
     llr = ctypes.CDLL(os.path.join(REFLIB, "libref_llr_v3.so"))
     for fn in (llr.ref_llr_v3_v1, llr.ref_llr_v3_v3):
@@ -151,7 +151,7 @@ def gpu_fixtures():
             o = torch.zeros(LLR_GPU_N * 2 * n, dtype=torch.int16, device=dev)
             assert fn(ds.data_ptr(), dn.data_ptr(), o.data_ptr(), LLR_GPU_N, n) == 0
             outs[f"{name}_n{n}"] = o.cpu().numpy().view(np.uint16)
-    np.savez_compressed(os.path.join(HERE, "ref_gpu_llr.npz"), **outs)
+    np.savez_compressed(os.path.join(out_dir, "ref_gpu_llr.npz"), **outs)
 
     srs = ctypes.CDLL(os.path.join(REFLIB, "libref_srs.so"))
     srs.ref_srs.argtypes = [CI, VP, VP, VP, VP, CI, CI, CI, CI, CI]
@@ -164,7 +164,7 @@ def gpu_fixtures():
             assert srs.ref_srs(v, o.data_ptr(), ds_.data_ptr(), dw.data_ptr(), df.data_ptr(), SRS_NANT, SRS_NBLK,
                                K, P, F) == 0
             outs[f"v{v}_K{K}_P{P}_F{F}"] = o.cpu().numpy().view(np.uint16)
-    np.savez_compressed(os.path.join(HERE, "ref_gpu_srs.npz"), **outs)
+    np.savez_compressed(os.path.join(out_dir, "ref_gpu_srs.npz"), **outs)
     print("wrote GPU fixtures")
 
 
@@ -172,8 +172,10 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpu", action="store_true", help="also run the reference's kernels (needs a GPU)")
     ap.add_argument("--gpu-only", action="store_true")
+    ap.add_argument("--out", default=HERE, help="directory for the GPU fixtures")
     a = ap.parse_args()
     if not a.gpu_only:
         cpu_fixtures()
     if a.gpu or a.gpu_only:
-        gpu_fixtures()
+        os.makedirs(a.out, exist_ok=True)
+        gpu_fixtures(a.out)

@@ -121,7 +121,7 @@ def test_multicell_vs_fp64(aeq, wl, orc, cuda):
 def test_fused_without_yeq_and_launch_shapes(aeq, wl, cuda):
     c = wl.config_cell(1, seed=31)
     ref = run_fused(aeq, [c], cuda, "fp16")[0][0]
-    for w, k in ((2, 4), (4, 1), (4, 2), (8, 1)):
+    for w, k in ((2, 4), (4, 1), (4, 2), (8, 1), (8, 2), (6, 2)):
         got = run_fused(aeq, [c], cuda, "fp16", want_yeq=False,
                         tuning=aeq.make_tuning("fp16", w, k))[0][0]
         np.testing.assert_array_equal(got, ref)
