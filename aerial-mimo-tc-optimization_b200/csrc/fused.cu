@@ -108,18 +108,26 @@ __device__ __forceinline__ float2 csub_mulc(float2 acc, float2 a, float2 b) {
 }
 
 // ---------------------------------------------------------------------------
-// per-warp shared-memory layout for layer tile LT (GS = 32/LT subcarriers)
+// per-warp shared-memory layout for layer tile LT (GS = 32/LT subcarriers), in
+// float2 units.  G rows (later Lc^-1 rows) and Z rows of each subcarrier;
+// row strides are even so pairs of complex values are one 16-byte access,
+// and each subcarrier's block is offset by 16 bytes so the GS blocks that a
+// warp reads in the same instruction fall in different banks.
 // ---------------------------------------------------------------------------
 template <int LT>
 struct WarpSmem {
     static constexpr int GS = 32 / LT;
-    static constexpr int GP = LT + 1;           // padded G row (complex)
-    static constexpr int RP = 16 + LT + 1;      // padded RHS row: 16 symbols + LT identity columns
-    static constexpr int offG = 0;                                   // float2 [GS][LT][GP]
-    static constexpr int offR = offG + GS * LT * GP;                 // float2 [GS][LT][RP]
-    static constexpr int offAux = offR + GS * LT * RP;               // float2 [32] column buffer
-    static constexpr int offInv = offAux + 32;                       // float  [32] (as float2 slots: 16)
-    static constexpr int total = offInv + 16;                        // in float2 units
+    static constexpr int RS = (LT + 3) & ~1;         // G / Linv row stride (even: float4-aligned)
+    static constexpr int ZS = 16 + 2;                // Z row stride (16 symbols)
+    static constexpr int GB = LT * RS + 2;           // per-subcarrier G block
+    static constexpr int ZB = LT * ZS + 2;           // per-subcarrier Z block
+    static constexpr int offG = 0;
+    static constexpr int offZ = GS * GB;
+    static constexpr int total = offZ + GS * ZB;
+    // every float4 access (row starts, pair offsets, block and warp offsets)
+    // must stay 16-byte aligned
+    static_assert(RS % 2 == 0 && ZS % 2 == 0 && GB % 2 == 0 && ZB % 2 == 0 && offZ % 2 == 0 && total % 2 == 0,
+                  "shared-memory layout must keep 16-byte alignment");
 };
 
 __host__ __device__ constexpr int warp_smem_bytes(int LT) {
@@ -130,19 +138,42 @@ __host__ __device__ constexpr int warp_smem_bytes(int LT) {
                    : WarpSmem<16>::total * 8;
 }
 
+// The fields of a cell a warp needs, read once from kernel-parameter space.
+struct CellView {
+    const float2* H;
+    const float2* Y;
+    float* llr;
+    float2* yeq;
+    float s2;
+    int nSC, A, L, nSym, nPam, vecY;
+    PamLut lut;
+};
+
+__device__ __forceinline__ CellView view_of(const FusedCell& c) {
+    CellView v;
+    v.H = c.H; v.Y = c.Y; v.llr = c.llr; v.yeq = c.yeq; v.s2 = c.sigma2;
+    v.nSC = c.nSC; v.A = c.A; v.L = c.L; v.nSym = c.nSym; v.nPam = c.nPam; v.vecY = c.vecY;
+    v.lut = c.lut;
+    return v;
+}
+
 // k-steps (8 antennas each) per pipelined chunk: two chunks are in flight per
-// warp (double buffer) while the tensor cores consume the previous one.
-constexpr int KS = 2;
+// warp (double buffer) while the tensor cores consume the previous one.  The
+// 16-layer tile loads twice the channel taps per k-step, so it uses one.
+template <int NMT>
+struct KSteps { static constexpr int value = NMT == 2 ? 1 : 2; };
 
 // Fragment registers of one chunk (KS k-steps) of one subcarrier.
 template <int NMT>
 struct Frag {
+    static constexpr int KS = KSteps<NMT>::value;
     float4 h[NMT][KS];   // (H[a0][l], H[a0+1][l]) for l = g + 8*mt
     float4 y[2][KS];     // (Y[8nt+g][a0], Y[8nt+g][a0+1])
 };
 
 template <int NMT>
-__device__ __forceinline__ void load_chunk(Frag<NMT>& f, const FusedCell& cl, long sc, int ch, int nK, int g, int c) {
+__device__ __forceinline__ void load_chunk(Frag<NMT>& f, const CellView& cl, long sc, int ch, int nK, int g, int c) {
+    constexpr int KS = Frag<NMT>::KS;
     const float2* Hs = cl.H + sc * (long)cl.A * cl.L;
     const float2* Ys = cl.Y + sc * (long)cl.nSym * cl.A;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -156,14 +187,9 @@ __device__ __forceinline__ void load_chunk(Frag<NMT>& f, const FusedCell& cl, lo
             const int l = g + 8 * mt;
             float4 v = z4;
             if (l < cl.L) {
-                if (k0) {
-                    float2 t = __ldg(Hs + (long)a0 * cl.L + l);
-                    v.x = t.x; v.y = t.y;
-                }
-                if (k1) {
-                    float2 t = __ldg(Hs + (long)(a0 + 1) * cl.L + l);
-                    v.z = t.x; v.w = t.y;
-                }
+                const float2* p = Hs + (long)a0 * cl.L + l;
+                if (k0) { float2 t = __ldg(p); v.x = t.x; v.y = t.y; }
+                if (k1) { float2 t = __ldg(p + cl.L); v.z = t.x; v.w = t.y; }
             }
             f.h[mt][kk] = v;
         }
@@ -190,6 +216,7 @@ template <int LT, int P>
 __device__ __forceinline__ void mma_chunk(const Frag<(LT > 8 ? 2 : 1)>& f, float (*gacc)[4], float (*zacc)[2][4],
                                           int ch, int nK, bool z2) {
     constexpr int NMT = LT > 8 ? 2 : 1;
+    constexpr int KS = Frag<NMT>::KS;
 #pragma unroll
     for (int kk = 0; kk < KS; kk++) {
         if (ch * KS + kk >= nK) break;
@@ -255,13 +282,13 @@ __device__ __forceinline__ void mma_chunk(const Frag<(LT > 8 ? 2 : 1)>& f, float
 
 // Accumulators of subcarrier q of the group -> per-warp shared memory.
 // Fragment (row g, cols 2c, 2c+1) and (row g+8, ...) = Re / Im of
-// out[8mt+g][8nt+2c], out[8mt+g][8nt+2c+1].
+// out[8mt+g][8nt+2c], out[8mt+g][8nt+2c+1]: one 16-byte store each.
 template <int LT>
 __device__ __forceinline__ void store_acc(float2* sm, float (*gacc)[4], float (*zacc)[2][4], int q, int g, int c) {
     using W = WarpSmem<LT>;
     constexpr int NMT = LT > 8 ? 2 : 1;
-    float2* sG = sm + W::offG + q * LT * W::GP;
-    float2* sR = sm + W::offR + q * LT * W::RP;
+    float2* sG = sm + W::offG + q * W::GB;
+    float2* sZ = sm + W::offZ + q * W::ZB;
 #pragma unroll
     for (int mt = 0; mt < NMT; mt++) {
         const int r = 8 * mt + g;
@@ -269,17 +296,14 @@ __device__ __forceinline__ void store_acc(float2* sm, float (*gacc)[4], float (*
         for (int nt = 0; nt <= mt; nt++) {
             const float* d = gacc[mt + nt];
             const int n = 8 * nt + 2 * c;
-            if (r < LT && n < LT) sG[r * W::GP + n] = make_float2(d[0], d[2]);
-            if (r < LT && n + 1 < LT) sG[r * W::GP + n + 1] = make_float2(d[1], d[3]);
+            if (r < LT && n < LT)
+                *reinterpret_cast<float4*>(sG + r * W::RS + n) = make_float4(d[0], d[2], d[1], d[3]);
         }
 #pragma unroll
         for (int nt = 0; nt < 2; nt++) {
             const float* d = zacc[mt][nt];
             const int s = 8 * nt + 2 * c;
-            if (r < LT) {
-                sR[r * W::RP + s] = make_float2(d[0], d[2]);
-                sR[r * W::RP + s + 1] = make_float2(d[1], d[3]);
-            }
+            if (r < LT) *reinterpret_cast<float4*>(sZ + r * W::ZS + s) = make_float4(d[0], d[2], d[1], d[3]);
         }
     }
 }
@@ -287,30 +311,59 @@ __device__ __forceinline__ void store_acc(float2* sm, float (*gacc)[4], float (*
 template <int N>
 __device__ __forceinline__ void write_llr(float* dst, const float* o) {
     if constexpr (N == 2) {
-        *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
+        __stcs(reinterpret_cast<float4*>(dst), make_float4(o[0], o[1], o[2], o[3]));
     } else if constexpr (N == 4) {
-        *reinterpret_cast<float4*>(dst) = make_float4(o[0], o[1], o[2], o[3]);
-        *reinterpret_cast<float4*>(dst + 4) = make_float4(o[4], o[5], o[6], o[7]);
+        __stcs(reinterpret_cast<float4*>(dst), make_float4(o[0], o[1], o[2], o[3]));
+        __stcs(reinterpret_cast<float4*>(dst + 4), make_float4(o[4], o[5], o[6], o[7]));
     } else {
 #pragma unroll
-        for (int j = 0; j < 2 * N; j += 2) *reinterpret_cast<float2*>(dst + j) = make_float2(o[j], o[j + 1]);
+        for (int j = 0; j < 2 * N; j += 2) __stcs(reinterpret_cast<float2*>(dst + j), make_float2(o[j], o[j + 1]));
     }
 }
 
 template <int N>
-__device__ __forceinline__ void emit(const FusedCell& cl, long sc, int i, const float2* x, float invMu, float nInv) {
+__device__ __forceinline__ void emit1(const CellView& cl, float* base, float2* ye, int s, float2 x, float invMu,
+                                      float nInv) {
+    const float2 v = make_float2(x.x * invMu, x.y * invMu);
+    if (ye) __stcs(ye + s, v);
+    float o[2 * N];
+    pam_llr<N>(v.x, v.y, nInv, cl.lut, o);
+    write_llr<N>(base + s * 2 * N, o);
+}
+
+// X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs, then unbias and demap.
+template <int LT, int N>
+__device__ __forceinline__ void solve_emit(const CellView& cl, const float2* sZ, const float2* gi, long sc, int i,
+                                           bool out, float invMu, float nInv) {
+    using W = WarpSmem<LT>;
     float* base = cl.llr + ((sc * cl.L + i) * (long)cl.nSym) * (2 * N);
     float2* ye = cl.yeq ? cl.yeq + (sc * cl.L + i) * (long)cl.nSym : nullptr;
 #pragma unroll
-    for (int s = 0; s < 16; s++) {
+    for (int s = 0; s < 16; s += 2) {
         if (s < cl.nSym) {
-            const float2 v = make_float2(x[s].x * invMu, x[s].y * invMu);
-            if (ye) ye[s] = v;
-            float o[2 * N];
-            pam_llr<N>(v.x, v.y, nInv, cl.lut, o);
-            write_llr<N>(base + s * 2 * N, o);
+            float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int m = 0; m < LT; m++) {
+                const float2 a = gi[m];
+                const float4 z = *reinterpret_cast<const float4*>(sZ + m * W::ZS + s);
+                x0.x += a.x * z.x - a.y * z.y;
+                x0.y += a.x * z.y + a.y * z.x;
+                x1.x += a.x * z.z - a.y * z.w;
+                x1.y += a.x * z.w + a.y * z.z;
+            }
+            if (out) {
+                emit1<N>(cl, base, ye, s, x0, invMu, nInv);
+                if (s + 1 < cl.nSym) emit1<N>(cl, base, ye, s + 1, x1, invMu, nInv);
+            }
         }
     }
+}
+
+__device__ __forceinline__ float shfl_f(float v, int src, int width) {
+    return __shfl_sync(0xffffffffu, v, src, width);
+}
+__device__ __forceinline__ float2 shfl_c(float2 v, int src, int width) {
+    return make_float2(__shfl_sync(0xffffffffu, v.x, src, width), __shfl_sync(0xffffffffu, v.y, src, width));
 }
 
 // ---------------------------------------------------------------------------
@@ -318,11 +371,15 @@ __device__ __forceinline__ void emit(const FusedCell& cl, long sc, int i, const 
 // FP32 solve with LT lanes per subcarrier.
 // ---------------------------------------------------------------------------
 template <int LT, int P>
-__device__ __noinline__ void process_group(const FusedCell& cl, long grp, float2* sm, int lane) {
+__device__ __noinline__ void process_group(const FusedCell& cref, long grp, int smemOff, int lane) {
     using W = WarpSmem<LT>;
     constexpr int NMT = LT > 8 ? 2 : 1;
     constexpr int GS = W::GS;
+    extern __shared__ float4 smem_raw[];
+    float2* sm = reinterpret_cast<float2*>(smem_raw) + smemOff;
+    const CellView cl = view_of(cref);
     const int g = lane >> 2, c = lane & 3;
+    constexpr int KS = Frag<NMT>::KS;
     const int nK = (cl.A + 7) >> 3;
     const int nChunk = (nK + KS - 1) / KS;
     const bool z2 = cl.nSym > 8;
@@ -376,138 +433,105 @@ __device__ __noinline__ void process_group(const FusedCell& cl, long grp, float2
     __syncwarp();
 
     // ---- solve phase: lane = (q, i), LT lanes per subcarrier ----
-    // Cholesky G = Lc Lc^H (right-looking, lane i keeps row i), then
-    // Linv = Lc^-1 by forward substitution on the identity (row i per lane,
-    // published to shared memory), Ginv = Linv^H Linv (row i per lane) and
-    // X = Ginv Z (row i per lane, Z rows read from shared memory).  The last
-    // two steps have no lane-to-lane dependency.
+    // Cholesky G = Lc Lc^H and Linv = Lc^-1 with rows in registers and the
+    // column / row broadcasts done by width-LT shuffles (no branches, no
+    // shared memory); then Ginv = Linv^H Linv and X = Ginv Z from shared
+    // memory (no lane-to-lane dependency).
     const int q = lane / LT, i = lane % LT;
     const long sc = sc0 + q;
     const bool scValid = q < nValid;
     const bool real = i < cl.L;          // padded layers (i >= L) carry an identity block
-    float2* sG = sm + W::offG + q * LT * W::GP;
-    float2* sR = sm + W::offR + q * LT * W::RP;
-    float2* sCol = sm + W::offAux + q * LT;
-    float* sInv = reinterpret_cast<float*>(sm + W::offInv) + q * LT;
-    const float s2 = cl.sigma2;
+    float2* sG = sm + W::offG + q * W::GB;
+    const float2* sZ = sm + W::offZ + q * W::ZB;
+    const float s2 = cl.s2;
 
-    // row i of the lower triangle of G (+ s2 on the diagonal)
     float2 gr[LT];
 #pragma unroll
     for (int m = 0; m < LT; m++) {
-        float2 v = make_float2(0.f, 0.f);
-        if (m <= i && scValid && real) v = sG[i * W::GP + m];
+        float2 v = (scValid && real) ? sG[i * W::RS + m] : make_float2(0.f, 0.f);
+        if (m > i) v = make_float2(0.f, 0.f);
         if (m == i) v = real ? make_float2(v.x + s2, 0.f) : make_float2(1.f, 0.f);
         gr[m] = v;
     }
 
+    // Cholesky, right-looking.  1/sqrt by rsqrt plus one Newton step.
     float myInv = 1.f;
 #pragma unroll
     for (int j = 0; j < LT; j++) {
-        if (i == j) {
-            float d = fmaxf(gr[j].x, 1e-30f);
-            d = sqrtf(d);
-            myInv = 1.0f / d;
-            gr[j] = make_float2(d, 0.f);
-            sInv[j] = myInv;
-        }
-        __syncwarp();
-        const float ivj = sInv[j];
-        float2 lij = make_float2(0.f, 0.f);
-        if (i > j) {
-            lij = make_float2(gr[j].x * ivj, gr[j].y * ivj);
-            gr[j] = lij;
-            sCol[i] = lij;
-        }
-        __syncwarp();
-        if (i > j) {
+        const float djj = fmaxf(shfl_f(gr[j].x, j, LT), 1e-30f);
+        float ivj = rsqrtf(djj);
+        ivj = ivj * (1.5f - 0.5f * djj * ivj * ivj);
+        const float2 scaled = make_float2(gr[j].x * ivj, gr[j].y * ivj);
+        const float2 lij = (i > j) ? scaled : make_float2(0.f, 0.f);
+        if (i == j) myInv = ivj;
+        gr[j] = (i > j) ? scaled : ((i == j) ? make_float2(djj * ivj, 0.f) : gr[j]);
 #pragma unroll
-            for (int m = j + 1; m < LT; m++)
-                if (m <= i) gr[m] = csub_mulc(gr[m], lij, sCol[m]);
-        }
+        for (int m = j + 1; m < LT; m++) gr[m] = csub_mulc(gr[m], lij, shfl_c(lij, m, LT));
     }
 
-    // Linv row i: Linv[i][m] = -(sum_{k=m}^{i-1} Lc[i][k] Linv[k][m]) / Lc[i][i],
-    // Linv[i][i] = 1 / Lc[i][i]; rows published to sR[.][16 + m].
+    // Linv row i by forward substitution on the identity.
     float2 e[LT];
 #pragma unroll
     for (int m = 0; m < LT; m++) e[m] = make_float2(m == i ? 1.f : 0.f, 0.f);
 #pragma unroll
     for (int k = 0; k < LT; k++) {
-        if (i == k) {
+        const float sck = (i == k) ? myInv : 1.f;
 #pragma unroll
-            for (int m = 0; m <= k; m++) {
-                e[m].x *= myInv; e[m].y *= myInv;
-                sR[k * W::RP + 16 + m] = e[m];
-            }
-        }
-        __syncwarp();
-        if (i > k) {
-            const float2 lik = gr[k];
+        for (int m = 0; m <= k; m++) { e[m].x *= sck; e[m].y *= sck; }
+        const float2 lik = (i > k) ? gr[k] : make_float2(0.f, 0.f);
 #pragma unroll
-            for (int m = 0; m <= k; m++) e[m] = csub_mul(e[m], lik, sR[k * W::RP + 16 + m]);
-        }
+        for (int m = 0; m <= k; m++) e[m] = csub_mul(e[m], lik, shfl_c(e[m], k, LT));
     }
+    // publish Linv rows (upper part zero) over the G block
+#pragma unroll
+    for (int m = 0; m < LT; m += 2)
+        *reinterpret_cast<float4*>(sG + i * W::RS + m) = make_float4(e[m].x, e[m].y, e[m + 1 < LT ? m + 1 : m].x * (m + 1 < LT), e[m + 1 < LT ? m + 1 : m].y * (m + 1 < LT));
     __syncwarp();
 
-    // Ginv row i: Ginv[i][j] = sum_{m >= max(i,j)} conj(Linv[m][i]) Linv[m][j]
+    // Ginv row i: Ginv[i][j] = sum_m conj(Linv[m][i]) Linv[m][j]
     float2 gi[LT];
 #pragma unroll
     for (int j = 0; j < LT; j++) gi[j] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int m = 0; m < LT; m++) {
-        if (m >= i) {
-            const float2 a = sR[m * W::RP + 16 + i];          // Linv[m][i]
+        const float2 a = sG[m * W::RS + i];
 #pragma unroll
-            for (int j = 0; j <= m; j++) {
-                const float2 b = sR[m * W::RP + 16 + j];      // Linv[m][j]
-                gi[j].x += a.x * b.x + a.y * b.y;             // conj(a) * b
-                gi[j].y += a.x * b.y - a.y * b.x;
+        for (int j = 0; j < LT; j += 2) {
+            const float4 b = *reinterpret_cast<const float4*>(sG + m * W::RS + j);
+            gi[j].x += a.x * b.x + a.y * b.y;
+            gi[j].y += a.x * b.y - a.y * b.x;
+            if (j + 1 < LT) {
+                gi[j + 1].x += a.x * b.z + a.y * b.w;
+                gi[j + 1].y += a.x * b.w - a.y * b.z;
             }
         }
     }
 
-    // X row i = Ginv[i][:] Z
-    float2 x[16];
-#pragma unroll
-    for (int s = 0; s < 16; s++) x[s] = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int m = 0; m < LT; m++) {
-        const float2 a = gi[m];
-#pragma unroll
-        for (int s = 0; s < 16; s++) {
-            if (s < cl.nSym) {
-                const float2 z = sR[m * W::RP + s];
-                x[s].x += a.x * z.x - a.y * z.y;
-                x[s].y += a.x * z.y + a.y * z.x;
-            }
-        }
+    // X row i = Ginv[i][:] Z, two symbols at a time, each pair demapped and
+    // stored as soon as it is complete.
+    const float t = s2 * gi[i].x;       // 1 - mu = s2 (G^-1)_ii
+    const float mu = fmaxf(1.0f - t, 1e-30f);
+    const float invMu = 1.0f / mu;
+    const float nInv = mu / fmaxf(t, 1e-30f);
+    const bool out = scValid && real;
+    switch (cl.nPam) {
+        case 1: solve_emit<LT, 1>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
+        case 2: solve_emit<LT, 2>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
+        case 3: solve_emit<LT, 3>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
+        default: solve_emit<LT, 4>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
     }
     __syncwarp();   // shared memory is reused by the next group
-
-    if (scValid && real) {
-        const float t = s2 * gi[i].x;       // 1 - mu = s2 (G^-1)_ii
-        const float mu = fmaxf(1.0f - t, 1e-30f);
-        const float invMu = 1.0f / mu;
-        const float nInv = mu / fmaxf(t, 1e-30f);
-        switch (cl.nPam) {
-            case 1: emit<1>(cl, sc, i, x, invMu, nInv); break;
-            case 2: emit<2>(cl, sc, i, x, invMu, nInv); break;
-            case 3: emit<3>(cl, sc, i, x, invMu, nInv); break;
-            default: emit<4>(cl, sc, i, x, invMu, nInv); break;
-        }
-    }
 }
 
 template <int P>
 __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant__ FusedParams p) {
-    extern __shared__ float4 smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int warpsPerCta = blockDim.x >> 5;
-    int maxLT = 1;
-    for (int ci = 0; ci < p.nCells; ci++) maxLT = max(maxLT, p.cell[ci].LT);
-    float2* sm = reinterpret_cast<float2*>(smem_raw) + (long)wib * (warp_smem_bytes(maxLT) / 8);
+    // per-warp shared memory: the largest footprint of the layer tiles present
+    int warpBytes = 0;
+    for (int ci = 0; ci < p.nCells; ci++) warpBytes = max(warpBytes, warp_smem_bytes(p.cell[ci].LT));
+    const int smemOff = wib * (warpBytes / 8);
     const long gw = (long)blockIdx.x * warpsPerCta + wib;
     const long nw = (long)gridDim.x * warpsPerCta;
     int ci = 0;
@@ -516,11 +540,11 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
         const FusedCell& cl = p.cell[ci];
         const long lg = grp - cl.group0;
         switch (cl.LT) {
-            case 1: process_group<1, P>(cl, lg, sm, lane); break;
-            case 2: process_group<2, P>(cl, lg, sm, lane); break;
-            case 4: process_group<4, P>(cl, lg, sm, lane); break;
-            case 8: process_group<8, P>(cl, lg, sm, lane); break;
-            default: process_group<16, P>(cl, lg, sm, lane); break;
+            case 1: process_group<1, P>(cl, lg, smemOff, lane); break;
+            case 2: process_group<2, P>(cl, lg, smemOff, lane); break;
+            case 4: process_group<4, P>(cl, lg, smemOff, lane); break;
+            case 8: process_group<8, P>(cl, lg, smemOff, lane); break;
+            default: process_group<16, P>(cl, lg, smemOff, lane); break;
         }
     }
 }
@@ -534,10 +558,12 @@ static int layer_tile(int L) {
     return t;
 }
 
-int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p, int& maxLT) {
+// warpBytes: the per-warp shared memory of the launch (largest footprint of
+// the layer tiles present; the footprint is not monotonic in the tile).
+int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p, int& warpBytes) {
     if (!cells || nCells < 1 || nCells > kMaxCells) return AERIAL_ERR_INVALID_ARG;
     long g0 = 0;
-    maxLT = 1;
+    warpBytes = 0;
     for (int i = 0; i < nCells; i++) {
         const aerial_cell_desc& c = cells[i];
         const int nSC = c.nPRB * 12;
@@ -565,7 +591,7 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
         // LLR rows of 2*nPam floats are written as float4 for nPam 2/4: need 16 B alignment
         if ((c.nPamBits == 2 || c.nPamBits == 4) && ((uintptr_t)c.llr & 15)) return AERIAL_ERR_INVALID_ARG;
         g0 += (nSC + (32 / f.LT) - 1) / (32 / f.LT);
-        if (f.LT > maxLT) maxLT = f.LT;
+        if (warp_smem_bytes(f.LT) > warpBytes) warpBytes = warp_smem_bytes(f.LT);
     }
     p.nCells = nCells;
     p.totalGroups = g0;
@@ -587,14 +613,11 @@ struct LaunchShape {
     int warps, ctasPerSm;
 };
 
-static LaunchShape default_shape(int maxLT) {
-    (void)maxLT;
-    return {8, 2};
-}
+static LaunchShape default_shape() { return {8, 2}; }
 
 template <int P>
-static int launch_fused_p(const FusedParams& p, int maxLT, LaunchShape sh, cudaStream_t st) {
-    const int bytes = sh.warps * warp_smem_bytes(maxLT);
+static int launch_fused_p(const FusedParams& p, int warpBytes, LaunchShape sh, cudaStream_t st) {
+    const int bytes = sh.warps * warpBytes;
     static int configured = 0;
     if (bytes > 48 * 1024 && bytes > configured) {
         cudaError_t e = cudaFuncSetAttribute(fused_eq_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -609,13 +632,13 @@ static int launch_fused_p(const FusedParams& p, int maxLT, LaunchShape sh, cudaS
     return launch_status();
 }
 
-int launch_fused(const FusedParams& p, int maxLT, int prec, LaunchShape sh, cudaStream_t st) {
+int launch_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, cudaStream_t st) {
     if (sh.warps < 1 || sh.warps > 8 || sh.ctasPerSm < 1 || sh.ctasPerSm > 8) return AERIAL_ERR_INVALID_ARG;
-    if ((long)sh.warps * warp_smem_bytes(maxLT) * sh.ctasPerSm > 227 * 1024) return AERIAL_ERR_UNSUPPORTED;
+    if ((long)sh.warps * warpBytes * sh.ctasPerSm > 227 * 1024) return AERIAL_ERR_UNSUPPORTED;
     switch (prec) {
-        case AERIAL_PREC_FP16: return launch_fused_p<AERIAL_PREC_FP16>(p, maxLT, sh, st);
-        case AERIAL_PREC_BF16: return launch_fused_p<AERIAL_PREC_BF16>(p, maxLT, sh, st);
-        case AERIAL_PREC_BF16X3: return launch_fused_p<AERIAL_PREC_BF16X3>(p, maxLT, sh, st);
+        case AERIAL_PREC_FP16: return launch_fused_p<AERIAL_PREC_FP16>(p, warpBytes, sh, st);
+        case AERIAL_PREC_BF16: return launch_fused_p<AERIAL_PREC_BF16>(p, warpBytes, sh, st);
+        case AERIAL_PREC_BF16X3: return launch_fused_p<AERIAL_PREC_BF16X3>(p, warpBytes, sh, st);
         default: return AERIAL_ERR_UNSUPPORTED;
     }
 }
@@ -627,17 +650,17 @@ using namespace aeq;
 extern "C" int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
                                      void* stream) {
     FusedParams p;
-    int maxLT = 1;
-    int s = build_fused_params(cells, nCells, p, maxLT);
+    int warpBytes = 0;
+    int s = build_fused_params(cells, nCells, p, warpBytes);
     if (s) return s;
-    LaunchShape sh = default_shape(maxLT);
+    LaunchShape sh = default_shape();
     int prec = AERIAL_PREC_FP16;
     if (tuning) {
         prec = tuning->precision;
         if (tuning->warps_per_cta) sh.warps = tuning->warps_per_cta;
         if (tuning->ctas_per_sm) sh.ctasPerSm = tuning->ctas_per_sm;
     }
-    return launch_fused(p, maxLT, prec, sh, to_stream(stream));
+    return launch_fused(p, warpBytes, prec, sh, to_stream(stream));
 }
 
 // ---------------------------------------------------------------------------
@@ -650,8 +673,8 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
                                void* stream) {
     if (!best) return AERIAL_ERR_INVALID_ARG;
     FusedParams p;
-    int maxLT = 1;
-    int s = build_fused_params(cells, nCells, p, maxLT);
+    int warpBytes = 0;
+    int s = build_fused_params(cells, nCells, p, warpBytes);
     if (s) return s;
     cudaStream_t st = to_stream(stream);
     const int prec = best->precision;
@@ -660,13 +683,13 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float bestT = 1e30f;
-    LaunchShape bestS = default_shape(maxLT);
+    LaunchShape bestS = default_shape();
     for (const LaunchShape& sh : cand) {
-        if ((long)sh.warps * warp_smem_bytes(maxLT) * sh.ctasPerSm > 220 * 1024) continue;
-        if ((s = launch_fused(p, maxLT, prec, sh, st))) break;
+        if ((long)sh.warps * warpBytes * sh.ctasPerSm > 220 * 1024) continue;
+        if ((s = launch_fused(p, warpBytes, prec, sh, st))) break;
         const int reps = 5;
         cudaEventRecord(e0, st);
-        for (int r = 0; r < reps && !s; r++) s = launch_fused(p, maxLT, prec, sh, st);
+        for (int r = 0; r < reps && !s; r++) s = launch_fused(p, warpBytes, prec, sh, st);
         cudaEventRecord(e1, st);
         if (s) break;
         cudaError_t e = cudaEventSynchronize(e1);

@@ -16,11 +16,11 @@ sources into oracle/_ref/ by oracle/Makefile):
   known_answers.json  the recorded coef_apply results (results/coef_rigor_results.txt,
                       README.md) with the data recipes that produced them
 GPU fixtures (the reference's kernels compiled unchanged for sm_100a, run on
-reference-generated inputs; inputs are regenerated from the seeds by the test):
-  ref_gpu_coef.npz    coef_apply_v1_scalar / v2_wmma outputs
-  ref_gpu_gram.npz    gram_scalar outputs (M = H^H)
-  ref_gpu_llr.npz     llr_v1_baseline / llr_v3_reg_template outputs
-  ref_gpu_srs.npz     srs_filter_v1_scalar / v2_wmma outputs
+the full-size reference inputs, which the tests regenerate from the seeds):
+  ref_gpu.json        SHA-256 of the outputs of coef_apply_v1_scalar / v2_wmma,
+                      gram_scalar (M = H^H), llr_v1_baseline / llr_v3 (nPamBits
+                      1..4) and srs_filter_v1_scalar / v2_wmma (4 configurations)
+  ref_gpu_slices.npz  the first 4096 values of each of those outputs
 """
 from __future__ import annotations
 
@@ -110,7 +110,23 @@ def srs_inputs(K, P, F, nBlk=SRS_NBLK, nAnt=SRS_NANT, seed=SRS_SEED):
     return O.ref_srs_inputs(seed, nBlk * nAnt * K, K * K, P * F)
 
 
+def digest(a) -> str:
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+# full-size recipes of the reference kernels' runs (shapes of the reference's main()s)
+COEF_FULL = dict(seed=7, nSC=1584, nSym=11)
+GRAM_FULL = dict(seed=11, nSC=1584)
+LLR_FULL_N = 139392
+SRS_FULL = dict(nBlk=66, nAnt=64, seed=42)
+
+
 def gpu_fixtures(out_dir=HERE):
+    """Run the reference's own kernels (compiled unchanged for sm_100a) on the
+    full-size reference inputs; record SHA-256 digests of their outputs plus
+    small value slices in ref_gpu.json / ref_gpu_slices.npz."""
     import torch
 
     dev = torch.device("cuda:0")
@@ -118,54 +134,63 @@ def gpu_fixtures(out_dir=HERE):
     def d(a):
         return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
 
+    rec, slices = {}, {}
     coef = ctypes.CDLL(os.path.join(REFLIB, "libref_coef.so"))
     for fn in (coef.ref_coef_v1, coef.ref_coef_v2):
         fn.argtypes = [VP, VP, VP, CI, CI]
-    C, Y = coef_inputs(COEF_SEED, COEF_NSC, COEF_NSYM)
+    C, Y = coef_inputs(COEF_FULL["seed"], COEF_FULL["nSC"], COEF_FULL["nSym"])
     dC, dY = d(C), d(Y)
-    outs = {}
-    for name, fn in (("v1", coef.ref_coef_v1), ("v2", coef.ref_coef_v2)):
-        o = torch.zeros(COEF_NSC * 8 * COEF_NSYM * 2, dtype=torch.float32, device=dev)
-        assert fn(dC.data_ptr(), dY.data_ptr(), o.data_ptr(), COEF_NSC, COEF_NSYM) == 0
-        outs[name] = o.cpu().numpy()
-    np.savez_compressed(os.path.join(out_dir, "ref_gpu_coef.npz"), **outs)
+    for name, fn in (("coef_v1", coef.ref_coef_v1), ("coef_v2", coef.ref_coef_v2)):
+        o = torch.zeros(COEF_FULL["nSC"] * 8 * COEF_FULL["nSym"] * 2, dtype=torch.float32, device=dev)
+        assert fn(dC.data_ptr(), dY.data_ptr(), o.data_ptr(), COEF_FULL["nSC"], COEF_FULL["nSym"]) == 0
+        o = o.cpu().numpy()
+        rec[name] = {"sha256": digest(o), "recipe": COEF_FULL}
+        slices[name] = o[:4096]
 
     gram = ctypes.CDLL(os.path.join(REFLIB, "libref_gram.so"))
     gram.ref_gram.argtypes = [VP, VP, VP, CI]
-    H, M = gram_inputs(GRAM_SEED, GRAM_NSC)
-    o = torch.zeros(GRAM_NSC * 64 * 2, dtype=torch.float32, device=dev)
-    assert gram.ref_gram(d(M).data_ptr(), d(H).data_ptr(), o.data_ptr(), GRAM_NSC) == 0
-    np.savez_compressed(os.path.join(out_dir, "ref_gpu_gram.npz"), G=o.cpu().numpy())
+    H, M = gram_inputs(GRAM_FULL["seed"], GRAM_FULL["nSC"])
+    dM, dH = d(M), d(H)      # keep both alive across the call
+    o = torch.zeros(GRAM_FULL["nSC"] * 64 * 2, dtype=torch.float32, device=dev)
+    assert gram.ref_gram(dM.data_ptr(), dH.data_ptr(), o.data_ptr(), GRAM_FULL["nSC"]) == 0
+    torch.cuda.synchronize()
+    o = o.cpu().numpy()
+    rec["gram"] = {"sha256": digest(o), "recipe": GRAM_FULL}
+    slices["gram"] = o[:4096]
 
     llr = ctypes.CDLL(os.path.join(REFLIB, "libref_llr_v3.so"))
     for fn in (llr.ref_llr_v3_v1, llr.ref_llr_v3_v3):
         fn.argtypes = [VP, VP, VP, CI, CI]
-    soft, ni = O.ref_llr_inputs(42, 139392)
-    soft, ni = soft[: 2 * LLR_GPU_N].copy(), ni[:LLR_GPU_N].copy()
+    soft, ni = O.ref_llr_inputs(42, LLR_FULL_N)
     ds, dn = d(soft.view(np.int16)), d(ni)
-    outs = {}
     for n in (1, 2, 3, 4):
         for name, fn in (("v1", llr.ref_llr_v3_v1), ("v3", llr.ref_llr_v3_v3)):
             if name == "v3" and n == 1:
                 continue
-            o = torch.zeros(LLR_GPU_N * 2 * n, dtype=torch.int16, device=dev)
-            assert fn(ds.data_ptr(), dn.data_ptr(), o.data_ptr(), LLR_GPU_N, n) == 0
-            outs[f"{name}_n{n}"] = o.cpu().numpy().view(np.uint16)
-    np.savez_compressed(os.path.join(out_dir, "ref_gpu_llr.npz"), **outs)
+            o = torch.zeros(LLR_FULL_N * 2 * n, dtype=torch.int16, device=dev)
+            assert fn(ds.data_ptr(), dn.data_ptr(), o.data_ptr(), LLR_FULL_N, n) == 0
+            o = o.cpu().numpy().view(np.uint16)
+            rec[f"llr_{name}_n{n}"] = {"sha256": digest(o), "recipe": {"seed": 42, "N": LLR_FULL_N}}
+            slices[f"llr_{name}_n{n}"] = o[:4096]
 
     srs = ctypes.CDLL(os.path.join(REFLIB, "libref_srs.so"))
     srs.ref_srs.argtypes = [CI, VP, VP, VP, VP, CI, CI, CI, CI, CI]
-    outs = {}
     for (K, P, F) in SRS_CFGS:
-        s, w, f = srs_inputs(K, P, F)
+        s, w, f = srs_inputs(K, P, F, SRS_FULL["nBlk"], SRS_FULL["nAnt"], SRS_FULL["seed"])
         ds_, dw, df = d(s.view(np.int16)), d(w.view(np.int16)), d(f.view(np.int16))
         for v in (1, 2):
-            o = torch.zeros(SRS_NBLK * SRS_NANT * K * P * 2, dtype=torch.int16, device=dev)
-            assert srs.ref_srs(v, o.data_ptr(), ds_.data_ptr(), dw.data_ptr(), df.data_ptr(), SRS_NANT, SRS_NBLK,
-                               K, P, F) == 0
-            outs[f"v{v}_K{K}_P{P}_F{F}"] = o.cpu().numpy().view(np.uint16)
-    np.savez_compressed(os.path.join(out_dir, "ref_gpu_srs.npz"), **outs)
-    print("wrote GPU fixtures")
+            o = torch.zeros(SRS_FULL["nBlk"] * SRS_FULL["nAnt"] * K * P * 2, dtype=torch.int16, device=dev)
+            assert srs.ref_srs(v, o.data_ptr(), ds_.data_ptr(), dw.data_ptr(), df.data_ptr(), SRS_FULL["nAnt"],
+                               SRS_FULL["nBlk"], K, P, F) == 0
+            o = o.cpu().numpy().view(np.uint16)
+            rec[f"srs_v{v}_K{K}_P{P}_F{F}"] = {"sha256": digest(o), "recipe": dict(SRS_FULL, K=K, P=P, F=F)}
+            slices[f"srs_v{v}_K{K}_P{P}_F{F}"] = o[:4096]
+    props = torch.cuda.get_device_properties(dev)
+    meta = {"device": props.name, "cc": f"{props.major}.{props.minor}", "nvcc": "12.9, -O3 -gencode sm_100a "
+            "(LLR files with --use_fast_math, their documented build line)"}
+    json.dump({"meta": meta, "outputs": rec}, open(os.path.join(out_dir, "ref_gpu.json"), "w"), indent=1)
+    np.savez_compressed(os.path.join(out_dir, "ref_gpu_slices.npz"), **slices)
+    print("wrote GPU fixtures to", out_dir)
 
 
 if __name__ == "__main__":

@@ -146,3 +146,16 @@ def test_fused_rejects_bad_cells(aeq, wl, cuda):
     d = aeq.cell_desc(H, Y, llr, c.sigma2, c.nPRB, c.nAnt, c.nLayers, 17, c.nPamBits)
     with pytest.raises(aeq.AerialError):
         aeq.pusch_eq_fused([d])
+
+
+def test_multicell_mixed_layer_tiles(aeq, wl, orc, cuda):
+    """Cells of every layer tile (1, 2, 4, 8, 16 and padded 3, 5, 12) in one
+    launch: each matches FP64 and its own single-cell run bit for bit."""
+    shapes = [(2, 16, 1, 11, 4), (1, 32, 2, 11, 16), (3, 24, 3, 9, 64), (1, 16, 4, 14, 256), (2, 64, 5, 11, 16),
+              (1, 64, 8, 11, 256), (1, 128, 12, 11, 64), (1, 128, 16, 11, 256)]
+    cells = [wl.make_cell(p, a, l, s, q, 25.0, seed=50 + k) for k, (p, a, l, s, q) in enumerate(shapes)]
+    mixed = run_fused(aeq, cells, cuda, "bf16x3")
+    for k, c in enumerate(cells):
+        check_against_fp64(orc, c, mixed[k][0], mixed[k][1], -60.0)
+        alone = run_fused(aeq, [c], cuda, "bf16x3")[0]
+        np.testing.assert_array_equal(alone[0], mixed[k][0])

@@ -69,9 +69,9 @@ def test_gram_bit_exact_vs_reference(aeq, cuda):
     lib.ref_gram.argtypes = [VP, VP, VP, CI]
     nSC = 1584
     H, M = MG.gram_inputs(11, nSC)
-    dH = _d(H, cuda)
+    dH, dM = _d(H, cuda), _d(M, cuda)     # both stay alive across the call
     ref = torch.empty(nSC * 64, dtype=torch.complex64, device=cuda)
-    assert lib.ref_gram(_d(M, cuda).data_ptr(), dH.data_ptr(), ref.data_ptr(), nSC) == 0
+    assert lib.ref_gram(dM.data_ptr(), dH.data_ptr(), ref.data_ptr(), nSC) == 0
     mine = torch.empty_like(ref)
     aeq.gram(dH, 0.0, mine, nSC, 64, 8)
     torch.cuda.synchronize()
@@ -115,7 +115,7 @@ def test_srs_oracle_bit_exact_vs_reference_v1(orc, cuda, K, P, F):
     nBlk, nAnt = 66, 64
     s, w, f = orc.ref_srs_inputs(42, nBlk * nAnt * K, K * K, P * F)
     o = torch.empty(nBlk * nAnt * K * P * 2, dtype=torch.int16, device=cuda)
-    assert lib.ref_srs(1, o.data_ptr(), _d(s.view(np.int16), cuda).data_ptr(), _d(w.view(np.int16), cuda).data_ptr(),
-                       _d(f.view(np.int16), cuda).data_ptr(), nAnt, nBlk, K, P, F) == 0
+    ds, dw, df = _d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda)
+    assert lib.ref_srs(1, o.data_ptr(), ds.data_ptr(), dw.data_ptr(), df.data_ptr(), nAnt, nBlk, K, P, F) == 0
     torch.cuda.synchronize()
     np.testing.assert_array_equal(orc.srs_v1_f16(s, w, f, nAnt, nBlk, K, P, F), o.cpu().numpy().view(np.uint16))

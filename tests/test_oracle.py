@@ -134,3 +134,66 @@ def test_srs_f16_restatement_close_to_fp64(orc, K, P, F):
     v16 = np.empty(o16.size, np.float32)
     orc.lib().orc_f16_to_f32(o16, v16, v16.size)
     assert cosine(v16.view(np.complex64), o64) > 0.9999
+
+
+# ---------------------------------------------------------------------------
+# The oracle against the reference's OWN kernels run on a B200 (compiled
+# unchanged for sm_100a): SHA-256 of the full-size outputs, regenerated here
+# from the same seeds (tests/golden/make_golden.py --gpu wrote ref_gpu.json).
+# ---------------------------------------------------------------------------
+import hashlib  # noqa: E402
+import sys  # noqa: E402
+
+sys.path.insert(0, GOLDEN)
+import make_golden as MG  # noqa: E402
+
+
+def _ref_gpu():
+    return json.load(open(os.path.join(GOLDEN, "ref_gpu.json")))["outputs"]
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_coef_apply_v1_oracle_matches_reference_kernel_digest(orc):
+    r = _ref_gpu()["coef_v1"]
+    C, Y = MG.coef_inputs(r["recipe"]["seed"], r["recipe"]["nSC"], r["recipe"]["nSym"])
+    o = orc.coef_apply_v1(C.view(np.complex64), Y.view(np.complex64), r["recipe"]["nSC"], r["recipe"]["nSym"], 8, 64)
+    assert _sha(o.view(np.float32)) == r["sha256"]
+    sl = np.load(os.path.join(GOLDEN, "ref_gpu_slices.npz"))["coef_v1"]
+    np.testing.assert_array_equal(o.view(np.float32)[: sl.size], sl)
+
+
+def test_coef_apply_v2_model_vs_reference_kernel(orc):
+    """The FP16 model of coef_apply_v2_wmma agrees with the kernel's run to -120 dB."""
+    r = _ref_gpu()["coef_v2"]
+    sl = np.load(os.path.join(GOLDEN, "ref_gpu_slices.npz"))["coef_v2"]
+    nsc = sl.size // (8 * 11 * 2)
+    C, Y = MG.coef_inputs(r["recipe"]["seed"], r["recipe"]["nSC"], r["recipe"]["nSym"])
+    o = orc.coef_apply_v2_model(C.view(np.complex64)[: nsc * 8 * 64], Y.view(np.complex64)[: nsc * 11 * 64],
+                                nsc, 11, 8, 64)
+    assert evm_db(o, sl.view(np.complex64)[: o.size]) < -120
+
+
+def test_gram_oracle_matches_reference_kernel_digest(orc):
+    r = _ref_gpu()["gram"]
+    H, M = MG.gram_inputs(r["recipe"]["seed"], r["recipe"]["nSC"])
+    assert _sha(orc.gram_ref(M, H, r["recipe"]["nSC"], 8, 64).view(np.float32)) == r["sha256"]
+    # and the Hermitian entry point (M = H^H implied, sigma2 = 0) is the same computation
+    assert _sha(orc.gram(H, 0.0, r["recipe"]["nSC"], 64, 8).view(np.float32)) == r["sha256"]
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4])
+def test_llr_oracle_matches_reference_kernel_digest(orc, n):
+    r = _ref_gpu()[f"llr_v1_n{n}"]
+    soft, ni = orc.ref_llr_inputs(r["recipe"]["seed"], r["recipe"]["N"])
+    assert _sha(orc.llr_f16io(soft, ni, n)) == r["sha256"]
+
+
+@pytest.mark.parametrize("K,P,F", MG.SRS_CFGS)
+def test_srs_oracle_matches_reference_kernel_digest(orc, K, P, F):
+    r = _ref_gpu()[f"srs_v1_K{K}_P{P}_F{F}"]
+    rc = r["recipe"]
+    s, w, f = MG.srs_inputs(K, P, F, rc["nBlk"], rc["nAnt"], rc["seed"])
+    assert _sha(orc.srs_v1_f16(s, w, f, rc["nAnt"], rc["nBlk"], K, P, F)) == r["sha256"]
