@@ -39,13 +39,18 @@ struct FusedCell {
     float2* yeq;
     long group0;     // first global group index of this cell
     float sigma2;
-    int nSC, A, L, nSym, nPam, LT, vecY;
+    int nSC, A, L, nSym, nPam, LT, vecY, vecH, lgHalfL;
+    int GS;          // subcarriers per group = 32 / LT
+    int nChunk;      // 16-antenna chunks per subcarrier
+    int hrs;         // staged channel-row stride (bytes)
     PamLut lut;
 };
 
 struct FusedParams {
     FusedCell cell[kMaxCells];
     int nCells;
+    int epiBytes;    // per-warp epilogue region (bytes)
+    int stageBytes;  // per operand stage (bytes)
     long totalGroups;
 };
 
@@ -157,81 +162,94 @@ __device__ __forceinline__ CellView view_of(const FusedCell& c) {
     return v;
 }
 
-// k-steps (8 antennas each) per pipelined chunk: two chunks are in flight per
-// warp (double buffer) while the tensor cores consume the previous one.  The
-// 16-layer tile loads twice the channel taps per k-step, so it uses one.
-template <int NMT>
-struct KSteps { static constexpr int value = NMT == 2 ? 1 : 2; };
+// ---------------------------------------------------------------------------
+// Operand staging.  Each warp streams its (subcarrier, 16-antenna chunk)
+// items through a ring of NST shared-memory stages with cp.async (16-byte
+// global -> shared copies that need no registers).  The ring runs ahead
+// across group boundaries, so while a warp does the FP32 solve and the LLR
+// epilogue of one group, the first chunks of its next group are in flight.
+//
+// Stage layout (bytes): 16 channel rows H[a][0..L-1] at a stride HRS (padded
+// so the fragment reads H[2c][g] of a warp hit distinct banks), then up to
+// 16 received rows Y[s][a0..a0+15] of 128 bytes whose 16-byte pieces are
+// XOR-swizzled by (s & 1) * 4 (conflict-free 16-byte fragment reads).
+// ---------------------------------------------------------------------------
+constexpr int NST = 3;          // stages per warp
+constexpr int CHUNK = 16;       // antennas per stage (two k-steps)
 
-// Fragment registers of one chunk (KS k-steps) of one subcarrier.
-template <int NMT>
-struct Frag {
-    static constexpr int KS = KSteps<NMT>::value;
-    float4 h[NMT][KS];   // (H[a0][l], H[a0+1][l]) for l = g + 8*mt
-    float4 y[2][KS];     // (Y[8nt+g][a0], Y[8nt+g][a0+1])
-};
+__host__ __device__ constexpr int hrs_of(int L) {
+    return (((8 * L + 15) & ~15) + 16) < 48 ? 48 : (((8 * L + 15) & ~15) + 16);
+}
 
-template <int NMT>
-__device__ __forceinline__ void load_chunk(Frag<NMT>& f, const CellView& cl, long sc, int ch, int nK, int g, int c) {
-    constexpr int KS = Frag<NMT>::KS;
-    const float2* Hs = cl.H + sc * (long)cl.A * cl.L;
-    const float2* Ys = cl.Y + sc * (long)cl.nSym * cl.A;
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-    for (int kk = 0; kk < KS; kk++) {
-        const int j = ch * KS + kk;
-        const int a0 = 8 * j + 2 * c;
-        const bool k0 = (j < nK) && (a0 < cl.A), k1 = (j < nK) && (a0 + 1 < cl.A);
-#pragma unroll
-        for (int mt = 0; mt < NMT; mt++) {
-            const int l = g + 8 * mt;
-            float4 v = z4;
-            if (l < cl.L) {
-                const float2* p = Hs + (long)a0 * cl.L + l;
-                if (k0) { float2 t = __ldg(p); v.x = t.x; v.y = t.y; }
-                if (k1) { float2 t = __ldg(p + cl.L); v.z = t.x; v.w = t.y; }
-            }
-            f.h[mt][kk] = v;
-        }
-#pragma unroll
-        for (int nt = 0; nt < 2; nt++) {
-            const int s = 8 * nt + g;
-            float4 v = z4;
-            if (s < cl.nSym) {
-                const float2* p = Ys + (long)s * cl.A + a0;
-                if (cl.vecY && k1) {
-                    v = __ldg(reinterpret_cast<const float4*>(p));
-                } else {
-                    if (k0) { float2 t = __ldg(p); v.x = t.x; v.y = t.y; }
-                    if (k1) { float2 t = __ldg(p + 1); v.z = t.x; v.w = t.y; }
-                }
-            }
-            f.y[nt][kk] = v;
-        }
-    }
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(__cvta_generic_to_global(src))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(__cvta_generic_to_global(src))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ float2 lds64(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ float4 lds128(uint32_t a) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
 }
 
 // Gram blocks kept: (0,0) for LT <= 8; (0,0), (1,0), (1,1) for LT = 16.
+// Fragment reads of one staged chunk (two k-steps) and their MMAs.  Thread
+// (g, c) of k-step kk owns the antenna pair 8kk + 2c, +1 of the chunk.
 template <int LT, int P>
-__device__ __forceinline__ void mma_chunk(const Frag<(LT > 8 ? 2 : 1)>& f, float (*gacc)[4], float (*zacc)[2][4],
-                                          int ch, int nK, bool z2) {
+__device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L, int nSym, float (*gacc)[4],
+                                          float (*zacc)[2][4], bool z2, int g, int c) {
     constexpr int NMT = LT > 8 ? 2 : 1;
-    constexpr int KS = Frag<NMT>::KS;
+    const uint32_t ys = st + CHUNK * hrs;
 #pragma unroll
-    for (int kk = 0; kk < KS; kk++) {
-        if (ch * KS + kk >= nK) break;
+    for (int kk = 0; kk < 2; kk++) {
+        const int a0 = 8 * kk + 2 * c;
+        if (8 * kk >= nRows) break;                      // uniform: tail chunk of 8 antennas
+        const bool v0 = a0 < nRows, v1 = a0 + 1 < nRows;
+        float4 hv[NMT];
+#pragma unroll
+        for (int mt = 0; mt < NMT; mt++) {
+            const int l = g + 8 * mt;
+            const bool lv = l < L;
+            const int la = lv ? l : 0;                   // padded layers read row data they then discard
+            const float2 h0 = lds64(st + a0 * hrs + la * 8);
+            const float2 h1 = lds64(st + (a0 + 1) * hrs + la * 8);
+            hv[mt] = make_float4((lv && v0) ? h0.x : 0.f, (lv && v0) ? h0.y : 0.f, (lv && v1) ? h1.x : 0.f,
+                                 (lv && v1) ? h1.y : 0.f);
+        }
+        float4 yv[2];
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++) {
+            const int s = 8 * nt + g;
+            const bool sv = s < nSym;
+            const int sa = sv ? s : 0;                   // rows past nSym are not staged: read row 0, discard
+            const float4 y = lds128(ys + sa * 128 + (((a0 >> 1) ^ ((sa & 1) << 2)) << 4));
+            yv[nt] = make_float4((sv && v0) ? y.x : 0.f, (sv && v0) ? y.y : 0.f, (sv && v1) ? y.z : 0.f,
+                                 (sv && v1) ? y.w : 0.f);
+        }
         if constexpr (P == AERIAL_PREC_BF16X3) {
             uint32_t ah[NMT][2], al[NMT][2];
 #pragma unroll
             for (int mt = 0; mt < NMT; mt++) {
-                split_bf16(f.h[mt][kk].x, f.h[mt][kk].y, ah[mt][0], al[mt][0]);
-                split_bf16(f.h[mt][kk].z, f.h[mt][kk].w, ah[mt][1], al[mt][1]);
+                split_bf16(hv[mt].x, hv[mt].y, ah[mt][0], al[mt][0]);
+                split_bf16(hv[mt].z, hv[mt].w, ah[mt][1], al[mt][1]);
             }
             uint32_t yh[2][2], yl[2][2];
 #pragma unroll
             for (int nt = 0; nt < 2; nt++) {
-                split_bf16(f.y[nt][kk].x, f.y[nt][kk].y, yh[nt][0], yl[nt][0]);
-                split_bf16(f.y[nt][kk].z, f.y[nt][kk].w, yh[nt][1], yl[nt][1]);
+                split_bf16(yv[nt].x, yv[nt].y, yh[nt][0], yl[nt][0]);
+                split_bf16(yv[nt].z, yv[nt].w, yh[nt][1], yl[nt][1]);
             }
 #pragma unroll
             for (int mt = 0; mt < NMT; mt++) {
@@ -239,7 +257,7 @@ __device__ __forceinline__ void mma_chunk(const Frag<(LT > 8 ? 2 : 1)>& f, float
                 const uint32_t l0 = al[mt][0], l1 = jrot(al[mt][0]), l2 = al[mt][1], l3 = jrot(al[mt][1]);
 #pragma unroll
                 for (int nt = 0; nt <= mt; nt++) {
-                    float* d = gacc[mt + nt];  // blocks (0,0)->0, (1,0)->1, (1,1)->2
+                    float* d = gacc[mt + nt];
                     mma16816<P>(d, h0, h1, h2, h3, ah[nt][0], ah[nt][1]);
                     mma16816<P>(d, h0, h1, h2, h3, al[nt][0], al[nt][1]);
                     mma16816<P>(d, l0, l1, l2, l3, ah[nt][0], ah[nt][1]);
@@ -256,24 +274,24 @@ __device__ __forceinline__ void mma_chunk(const Frag<(LT > 8 ? 2 : 1)>& f, float
             uint32_t a[NMT][2];
 #pragma unroll
             for (int mt = 0; mt < NMT; mt++) {
-                a[mt][0] = pack2<P>(f.h[mt][kk].x, f.h[mt][kk].y);
-                a[mt][1] = pack2<P>(f.h[mt][kk].z, f.h[mt][kk].w);
+                a[mt][0] = pack2<P>(hv[mt].x, hv[mt].y);
+                a[mt][1] = pack2<P>(hv[mt].z, hv[mt].w);
             }
             uint32_t b[2][2];
 #pragma unroll
             for (int nt = 0; nt < 2; nt++) {
-                b[nt][0] = pack2<P>(f.y[nt][kk].x, f.y[nt][kk].y);
-                b[nt][1] = pack2<P>(f.y[nt][kk].z, f.y[nt][kk].w);
+                b[nt][0] = pack2<P>(yv[nt].x, yv[nt].y);
+                b[nt][1] = pack2<P>(yv[nt].z, yv[nt].w);
             }
 #pragma unroll
             for (int mt = 0; mt < NMT; mt++) {
-                const uint32_t a0 = a[mt][0], a1 = jrot(a[mt][0]), a2 = a[mt][1], a3 = jrot(a[mt][1]);
+                const uint32_t a0r = a[mt][0], a1r = jrot(a[mt][0]), a2r = a[mt][1], a3r = jrot(a[mt][1]);
 #pragma unroll
-                for (int nt = 0; nt <= mt; nt++) mma16816<P>(gacc[mt + nt], a0, a1, a2, a3, a[nt][0], a[nt][1]);
+                for (int nt = 0; nt <= mt; nt++) mma16816<P>(gacc[mt + nt], a0r, a1r, a2r, a3r, a[nt][0], a[nt][1]);
 #pragma unroll
                 for (int nt = 0; nt < 2; nt++) {
                     if (nt == 1 && !z2) break;
-                    mma16816<P>(zacc[mt][nt], a0, a1, a2, a3, b[nt][0], b[nt][1]);
+                    mma16816<P>(zacc[mt][nt], a0r, a1r, a2r, a3r, b[nt][0], b[nt][1]);
                 }
             }
         }
@@ -367,71 +385,14 @@ __device__ __forceinline__ float2 shfl_c(float2 v, int src, int width) {
 }
 
 // ---------------------------------------------------------------------------
-// one group of GS subcarriers: MMA phase (whole warp per subcarrier), then the
-// FP32 solve with LT lanes per subcarrier.
+// The FP32 solve of one group of GS subcarriers whose G and Z are in the
+// warp's epilogue region: LT lanes per subcarrier.
 // ---------------------------------------------------------------------------
 template <int LT, int P>
-__device__ __noinline__ void process_group(const FusedCell& cref, long grp, int smemOff, int lane) {
+__device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid, int smemOff, int lane) {
     using W = WarpSmem<LT>;
-    constexpr int NMT = LT > 8 ? 2 : 1;
-    constexpr int GS = W::GS;
     extern __shared__ float4 smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw) + smemOff;
-    const CellView cl = view_of(cref);
-    const int g = lane >> 2, c = lane & 3;
-    constexpr int KS = Frag<NMT>::KS;
-    const int nK = (cl.A + 7) >> 3;
-    const int nChunk = (nK + KS - 1) / KS;
-    const bool z2 = cl.nSym > 8;
-    const long sc0 = grp * GS;
-    const int nValid = (int)min((long)GS, (long)cl.nSC - sc0);
-    const int nItems = nValid * nChunk;
-
-    // ---- MMA phase: software-pipelined over (subcarrier, chunk) items ----
-    {
-        float gacc[NMT == 2 ? 3 : 1][4];
-        float zacc[NMT][2][4];
-#pragma unroll
-        for (int b = 0; b < (NMT == 2 ? 3 : 1); b++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
-#pragma unroll
-        for (int mt = 0; mt < NMT; mt++)
-#pragma unroll
-            for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-                for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
-
-        auto finish = [&](int it) {
-            if ((it % nChunk) == nChunk - 1) {
-                store_acc<LT>(sm, gacc, zacc, it / nChunk, g, c);
-#pragma unroll
-                for (int b = 0; b < (NMT == 2 ? 3 : 1); b++)
-#pragma unroll
-                    for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
-#pragma unroll
-                for (int mt = 0; mt < NMT; mt++)
-#pragma unroll
-                    for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-                        for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
-            }
-        };
-        Frag<NMT> fa, fb;
-        if (nItems > 0) load_chunk<NMT>(fa, cl, sc0, 0, nK, g, c);
-        for (int it = 0; it < nItems; it += 2) {
-            if (it + 1 < nItems) load_chunk<NMT>(fb, cl, sc0 + (it + 1) / nChunk, (it + 1) % nChunk, nK, g, c);
-            mma_chunk<LT, P>(fa, gacc, zacc, it % nChunk, nK, z2);
-            finish(it);
-            if (it + 2 < nItems) load_chunk<NMT>(fa, cl, sc0 + (it + 2) / nChunk, (it + 2) % nChunk, nK, g, c);
-            if (it + 1 < nItems) {
-                mma_chunk<LT, P>(fb, gacc, zacc, (it + 1) % nChunk, nK, z2);
-                finish(it + 1);
-            }
-        }
-    }
-    __syncwarp();
-
     // ---- solve phase: lane = (q, i), LT lanes per subcarrier ----
     // Cholesky G = Lc Lc^H and Linv = Lc^-1 with rows in registers and the
     // column / row broadcasts done by width-LT shuffles (no branches, no
@@ -523,30 +484,205 @@ __device__ __noinline__ void process_group(const FusedCell& cref, long grp, int 
     __syncwarp();   // shared memory is reused by the next group
 }
 
+// Per-warp shared memory of a launch: the epilogue region (largest footprint
+// of the layer tiles present) followed by NST operand stages.
+inline int stage_bytes_of(const FusedParams& p) {
+    int b = 0;
+    for (int ci = 0; ci < p.nCells; ci++) {
+        const int v = CHUNK * hrs_of(p.cell[ci].L) + 128 * p.cell[ci].nSym;
+        b = v > b ? v : b;
+    }
+    return (b + 15) & ~15;
+}
+inline int epi_bytes_of(const FusedParams& p) {
+    int b = 0;
+    for (int ci = 0; ci < p.nCells; ci++) {
+        const int v = warp_smem_bytes(p.cell[ci].LT);
+        b = v > b ? v : b;
+    }
+    return (b + 15) & ~15;
+}
+
+// Stage the copies of one item (subcarrier base pointers hs / ys, chunk ch)
+// of cell cl into the stage at shared address st.  Subcarriers of a group
+// are contiguous, so the producer only advances pointers between items.
+__device__ __forceinline__ void stage_item(const FusedCell& cl, const float2* hs, const float2* ys, int ch,
+                                           uint32_t st, int lane) {
+    const int L = cl.L, A = cl.A, nSym = cl.nSym, hrs = cl.hrs;
+    const int nRows = min(CHUNK, A - CHUNK * ch);
+    const float2* hsrc = hs + CHUNK * ch * L;
+    if (cl.vecH) {                      // L even: 16-byte pieces, L/2 per row
+        const int half = L >> 1;
+        const int n = nRows * half;
+        if (cl.lgHalfL >= 0) {
+            const int sh = cl.lgHalfL;
+            for (int e = lane; e < n; e += 32) cp_async16(st + (e >> sh) * hrs + (e & (half - 1)) * 16, hsrc + 2 * e);
+        } else {
+            for (int e = lane; e < n; e += 32) {
+                const int row = e / half;
+                cp_async16(st + row * hrs + (e - row * half) * 16, hsrc + 2 * e);
+            }
+        }
+    } else {                            // 8-byte pieces
+        const int n = nRows * L;
+        for (int e = lane; e < n; e += 32) {
+            const int row = e / L;
+            cp_async8(st + row * hrs + (e - row * L) * 8, hsrc + e);
+        }
+    }
+    const uint32_t yst = st + CHUNK * hrs;
+    const float2* ysrc = ys + CHUNK * ch;
+    for (int e = lane; e < nSym * 8; e += 32) {
+        const int s = e >> 3, k = e & 7;
+        const int a = 2 * k;
+        if (a < nRows) {
+            const uint32_t d = yst + s * 128 + ((k ^ ((s & 1) << 2)) << 4);
+            const float2* src = ysrc + (long)s * A + a;
+            if (cl.vecY && a + 1 < nRows) {
+                cp_async16(d, src);
+            } else {
+                cp_async8(d, src);
+                if (a + 1 < nRows) cp_async8(d + 8, src + 1);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ int group_valid(const FusedCell& cl, long grp) {
+    return (int)min((long)cl.GS, (long)cl.nSC - (grp - cl.group0) * cl.GS);
+}
+
 template <int P>
 __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant__ FusedParams p) {
+    extern __shared__ float4 smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int warpsPerCta = blockDim.x >> 5;
-    // per-warp shared memory: the largest footprint of the layer tiles present
-    int warpBytes = 0;
-    for (int ci = 0; ci < p.nCells; ci++) warpBytes = max(warpBytes, warp_smem_bytes(p.cell[ci].LT));
+    const int g = lane >> 2, c = lane & 3;
+    const int warpBytes = p.epiBytes + NST * p.stageBytes;
     const int smemOff = wib * (warpBytes / 8);
+    float2* sm = reinterpret_cast<float2*>(smem_raw) + smemOff;
+    const uint32_t stBase =
+        (uint32_t)__cvta_generic_to_shared(reinterpret_cast<char*>(smem_raw) + (long)wib * warpBytes + p.epiBytes);
     const long gw = (long)blockIdx.x * warpsPerCta + wib;
     const long nw = (long)gridDim.x * warpsPerCta;
-    int ci = 0;
-    for (long grp = gw; grp < p.totalGroups; grp += nw) {
-        while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
-        const FusedCell& cl = p.cell[ci];
-        const long lg = grp - cl.group0;
-        switch (cl.LT) {
-            case 1: process_group<1, P>(cl, lg, smemOff, lane); break;
-            case 2: process_group<2, P>(cl, lg, smemOff, lane); break;
-            case 4: process_group<4, P>(cl, lg, smemOff, lane); break;
-            case 8: process_group<8, P>(cl, lg, smemOff, lane); break;
-            default: process_group<16, P>(cl, lg, smemOff, lane); break;
-        }
+    const long total = p.totalGroups;
+    if (gw >= total) return;
+
+    // ---- producer cursor (registers): group, cell, subcarrier, chunk ----
+    long pg = gw;
+    int pci = 0;
+    while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
+    int pq = 0, pch = 0, pValid = group_valid(p.cell[pci], pg), pslot = 0;
+    const float2* phs;
+    const float2* pys;
+    {
+        const FusedCell& cl = p.cell[pci];
+        const long sc = (pg - cl.group0) * cl.GS;
+        phs = cl.H + sc * cl.A * cl.L;
+        pys = cl.Y + sc * cl.nSym * cl.A;
     }
+    auto produce = [&]() {
+        if (pg < total) {
+            const FusedCell& cl = p.cell[pci];
+            stage_item(cl, phs, pys, pch, stBase + pslot * p.stageBytes, lane);
+            if (++pch == cl.nChunk) {
+                pch = 0;
+                if (++pq < pValid) {
+                    phs += (long)cl.A * cl.L;
+                    pys += (long)cl.nSym * cl.A;
+                } else {
+                    pq = 0;
+                    pg += nw;
+                    if (pg < total) {
+                        while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
+                        const FusedCell& cn = p.cell[pci];
+                        pValid = group_valid(cn, pg);
+                        const long sc = (pg - cn.group0) * cn.GS;
+                        phs = cn.H + sc * cn.A * cn.L;
+                        pys = cn.Y + sc * cn.nSym * cn.A;
+                    }
+                }
+            }
+        }
+        cp_async_commit();
+        pslot = pslot == NST - 1 ? 0 : pslot + 1;
+    };
+#pragma unroll
+    for (int k = 0; k < NST - 1; k++) produce();
+
+    // ---- consumer ----
+    long grp = gw;
+    int ci = 0;
+    while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+    int q = 0, ch = 0, nValid = group_valid(p.cell[ci], grp), cslot = 0;
+    float gacc[3][4], zacc[2][2][4];
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
+
+    while (true) {
+        __syncwarp();                              // every lane is done with the slot refilled now
+        produce();
+        cp_async_wait<NST - 1>();                  // this item's copies (own lane) have landed
+        __syncwarp();                              // ... and every lane's
+        const FusedCell& cl = p.cell[ci];
+        const int LT = cl.LT;
+        const uint32_t st = stBase + cslot * p.stageBytes;
+        cslot = cslot == NST - 1 ? 0 : cslot + 1;
+        const int nRows = min(CHUNK, cl.A - CHUNK * ch);
+        const bool z2 = cl.nSym > 8;
+        switch (LT) {
+            case 1: mma_stage<1, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+            case 2: mma_stage<2, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+            case 4: mma_stage<4, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+            case 8: mma_stage<8, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+            default: mma_stage<16, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+        }
+        if (++ch < cl.nChunk) continue;
+        ch = 0;
+        switch (LT) {
+            case 1: store_acc<1>(sm, gacc, zacc, q, g, c); break;
+            case 2: store_acc<2>(sm, gacc, zacc, q, g, c); break;
+            case 4: store_acc<4>(sm, gacc, zacc, q, g, c); break;
+            case 8: store_acc<8>(sm, gacc, zacc, q, g, c); break;
+            default: store_acc<16>(sm, gacc, zacc, q, g, c); break;
+        }
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
+        if (++q < nValid) continue;
+        __syncwarp();
+        const CellView v = view_of(cl);
+        const long sc0 = (grp - cl.group0) * cl.GS;
+        switch (LT) {
+            case 1: solve_group<1, P>(v, sc0, nValid, smemOff, lane); break;
+            case 2: solve_group<2, P>(v, sc0, nValid, smemOff, lane); break;
+            case 4: solve_group<4, P>(v, sc0, nValid, smemOff, lane); break;
+            case 8: solve_group<8, P>(v, sc0, nValid, smemOff, lane); break;
+            default: solve_group<16, P>(v, sc0, nValid, smemOff, lane); break;
+        }
+        q = 0;
+        grp += nw;
+        if (grp >= total) break;
+        while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+        nValid = group_valid(p.cell[ci], grp);
+    }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -558,8 +694,9 @@ static int layer_tile(int L) {
     return t;
 }
 
-// warpBytes: the per-warp shared memory of the launch (largest footprint of
-// the layer tiles present; the footprint is not monotonic in the tile).
+// warpBytes: the per-warp shared memory of the launch (epilogue region of the
+// largest layer-tile footprint present, which is not monotonic in the tile,
+// plus NST operand stages).
 int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p, int& warpBytes) {
     if (!cells || nCells < 1 || nCells > kMaxCells) return AERIAL_ERR_INVALID_ARG;
     long g0 = 0;
@@ -586,15 +723,25 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
         f.nPam = c.nPamBits;
         f.LT = layer_tile(c.nLayers);
         f.vecY = ((c.nAnt % 2) == 0 && ((uintptr_t)c.Y_rx & 15) == 0) ? 1 : 0;
+        f.vecH = ((c.nLayers % 2) == 0 && ((uintptr_t)c.H & 15) == 0) ? 1 : 0;
+        {
+            const int half = c.nLayers / 2;
+            f.lgHalfL = (half > 0 && (half & (half - 1)) == 0) ? __builtin_ctz(half) : -1;
+        }
         f.lut = pam_lut(c.nPamBits);
         f.group0 = g0;
+        f.GS = 32 / f.LT;
+        f.nChunk = (c.nAnt + CHUNK - 1) / CHUNK;
+        f.hrs = hrs_of(c.nLayers);
         // LLR rows of 2*nPam floats are written as float4 for nPam 2/4: need 16 B alignment
         if ((c.nPamBits == 2 || c.nPamBits == 4) && ((uintptr_t)c.llr & 15)) return AERIAL_ERR_INVALID_ARG;
         g0 += (nSC + (32 / f.LT) - 1) / (32 / f.LT);
-        if (warp_smem_bytes(f.LT) > warpBytes) warpBytes = warp_smem_bytes(f.LT);
     }
     p.nCells = nCells;
     p.totalGroups = g0;
+    p.epiBytes = epi_bytes_of(p);
+    p.stageBytes = stage_bytes_of(p);
+    warpBytes = p.epiBytes + NST * p.stageBytes;
     return AERIAL_OK;
 }
 
@@ -613,7 +760,24 @@ struct LaunchShape {
     int warps, ctasPerSm;
 };
 
-static LaunchShape default_shape() { return {8, 2}; }
+// Launch shapes are limited by 16 resident warps per SM (128 registers per
+// thread) and by shared memory (operand ring + epilogue region per warp).
+constexpr int kSmemPerSm = 220 * 1024;
+constexpr int kWarpsPerSm = 16;
+
+static int max_ctas(int warps, int warpBytes) {
+    int k = kSmemPerSm / (warps * warpBytes);
+    if (k > kWarpsPerSm / warps) k = kWarpsPerSm / warps;
+    return k;
+}
+
+static LaunchShape default_shape(int warpBytes) {
+    for (int w : {4, 2, 1}) {
+        const int k = max_ctas(w, warpBytes);
+        if (k >= 1) return {w, k};
+    }
+    return {1, 1};
+}
 
 template <int P>
 static int launch_fused_p(const FusedParams& p, int warpBytes, LaunchShape sh, cudaStream_t st) {
@@ -634,7 +798,8 @@ static int launch_fused_p(const FusedParams& p, int warpBytes, LaunchShape sh, c
 
 int launch_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, cudaStream_t st) {
     if (sh.warps < 1 || sh.warps > 8 || sh.ctasPerSm < 1 || sh.ctasPerSm > 8) return AERIAL_ERR_INVALID_ARG;
-    if ((long)sh.warps * warpBytes * sh.ctasPerSm > 227 * 1024) return AERIAL_ERR_UNSUPPORTED;
+    if ((long)sh.warps * warpBytes * sh.ctasPerSm > 227 * 1024 || (long)sh.warps * warpBytes > 227 * 1024)
+        return AERIAL_ERR_UNSUPPORTED;
     switch (prec) {
         case AERIAL_PREC_FP16: return launch_fused_p<AERIAL_PREC_FP16>(p, warpBytes, sh, st);
         case AERIAL_PREC_BF16: return launch_fused_p<AERIAL_PREC_BF16>(p, warpBytes, sh, st);
@@ -653,7 +818,7 @@ extern "C" int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, 
     int warpBytes = 0;
     int s = build_fused_params(cells, nCells, p, warpBytes);
     if (s) return s;
-    LaunchShape sh = default_shape();
+    LaunchShape sh = default_shape(warpBytes);
     int prec = AERIAL_PREC_FP16;
     if (tuning) {
         prec = tuning->precision;
@@ -678,14 +843,20 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
     if (s) return s;
     cudaStream_t st = to_stream(stream);
     const int prec = best->precision;
-    static const LaunchShape cand[] = {{4, 2}, {4, 4}, {8, 1}, {8, 2}, {6, 2}, {2, 8}};
+    LaunchShape cand[16];
+    int nc = 0;
+    for (int w : {2, 3, 4, 6, 8}) {
+        const int k = max_ctas(w, warpBytes);
+        if (k >= 1) cand[nc++] = {w, k};
+        if (k >= 2) cand[nc++] = {w, k - 1};
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float bestT = 1e30f;
-    LaunchShape bestS = default_shape();
-    for (const LaunchShape& sh : cand) {
-        if ((long)sh.warps * warpBytes * sh.ctasPerSm > 220 * 1024) continue;
+    LaunchShape bestS = default_shape(warpBytes);
+    for (int ic = 0; ic < nc; ic++) {
+        const LaunchShape& sh = cand[ic];
         if ((s = launch_fused(p, warpBytes, prec, sh, st))) break;
         const int reps = 5;
         cudaEventRecord(e0, st);
