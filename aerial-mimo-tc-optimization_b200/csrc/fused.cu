@@ -207,7 +207,7 @@ __device__ __forceinline__ float4 lds128(uint32_t a) {
 // Gram blocks kept: (0,0) for LT <= 8; (0,0), (1,0), (1,1) for LT = 16.
 // Fragment reads of one staged chunk (two k-steps) and their MMAs.  Thread
 // (g, c) of k-step kk owns the antenna pair 8kk + 2c, +1 of the chunk.
-template <int LT, int P>
+template <int LT, int P, bool LEXACT>
 __device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L, int nSym, float (*gacc)[4],
                                           float (*zacc)[2][4], bool z2, int g, int c) {
     constexpr int NMT = LT > 8 ? 2 : 1;
@@ -221,7 +221,7 @@ __device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L
 #pragma unroll
         for (int mt = 0; mt < NMT; mt++) {
             const int l = g + 8 * mt;
-            const bool lv = l < L;
+            const bool lv = LEXACT || l < L;             // LEXACT: every lane's layer exists (L == LT)
             const int la = lv ? l : 0;                   // padded layers read row data they then discard
             const float2 h0 = lds64(st + a0 * hrs + la * 8);
             const float2 h1 = lds64(st + (a0 + 1) * hrs + la * 8);
@@ -339,13 +339,43 @@ __device__ __forceinline__ void write_llr(float* dst, const float* o) {
     }
 }
 
+// Max-log PAM demapper of the fused epilogue: the formula of llr_v1_baseline
+// (src/llr/aerial_llr_v3.cu:90-107) with the last square fused into the
+// subtraction (fma(-t, t, pMD)), the +-65504 clamp applied to the magnitude
+// and the soft bit's sign copied in with one bit operation.  It differs from
+// the reference's rounding by at most one FP32 ulp of each LLR (the plain
+// chain keeps the bit-exact form).
+template <int N>
+__device__ __forceinline__ void pam_llr_fast(float pI, float pQ, float noise, const PamLut& L, float* out) {
+    const float dist = L.d[N - 1];
+#pragma unroll
+    for (int iq = 0; iq < 2; iq++) {
+        float sb = iq ? pQ : pI;
+        float pm[N], sg[N];
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            const float a = fabsf(sb);
+            const float m = dist + a;
+            pm[i] = m * m;
+            sg[i] = sb;
+            if (i < N - 1) sb = L.d[i] - a;
+        }
+        const float t = fabsf(sb) - dist;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            const float v = fminf(fmaf(-t, t, pm[i]) * noise, 65504.f);
+            out[2 * i + iq] = __int_as_float(__float_as_int(v) ^ (__float_as_int(sg[i]) & 0x80000000));
+        }
+    }
+}
+
 template <int N>
 __device__ __forceinline__ void emit1(const CellView& cl, float* base, float2* ye, int s, float2 x, float invMu,
                                       float nInv) {
     const float2 v = make_float2(x.x * invMu, x.y * invMu);
     if (ye) __stcs(ye + s, v);
     float o[2 * N];
-    pam_llr<N>(v.x, v.y, nInv, cl.lut, o);
+    pam_llr_fast<N>(v.x, v.y, nInv, cl.lut, o);
     write_llr<N>(base + s * 2 * N, o);
 }
 
@@ -458,6 +488,7 @@ __device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid
         const float2 a = sG[m * W::RS + i];
 #pragma unroll
         for (int j = 0; j < LT; j += 2) {
+            if (j > m) break;                          // Linv[m][j] = 0 above the diagonal
             const float4 b = *reinterpret_cast<const float4*>(sG + m * W::RS + j);
             gi[j].x += a.x * b.x + a.y * b.y;
             gi[j].y += a.x * b.y - a.y * b.x;
@@ -548,11 +579,53 @@ __device__ __forceinline__ void stage_item(const FusedCell& cl, const float2* hs
     }
 }
 
+// stage_item for a launch whose cells all have L == LF (even): strides and
+// piece mapping are compile-time constants.
+template <int LF>
+__device__ __forceinline__ void stage_item_exact(const FusedCell& cl, const float2* hs, const float2* ys, int ch,
+                                                 uint32_t st, int lane) {
+    constexpr int HRS = hrs_of(LF);
+    constexpr int HALF = LF / 2;
+    const int A = cl.A, nSym = cl.nSym;
+    const int nRows = min(CHUNK, A - CHUNK * ch);
+    const float2* hsrc = hs + CHUNK * ch * LF;
+    const int n = nRows * HALF;
+#pragma unroll
+    for (int k = 0; k < (CHUNK * HALF + 31) / 32; k++) {
+        const int e = lane + 32 * k;
+        if (e < n) cp_async16(st + (e / HALF) * HRS + (e % HALF) * 16, hsrc + 2 * e);
+    }
+    const uint32_t yst = st + CHUNK * HRS;
+    const float2* ysrc = ys + CHUNK * ch;
+    if (nRows == CHUNK) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {                  // up to 16 rows x 8 pieces
+            const int e = lane + 32 * k;
+            const int s = e >> 3, kk = e & 7;
+            if (s < nSym) cp_async16(yst + s * 128 + ((kk ^ ((s & 1) << 2)) << 4), ysrc + (long)s * A + 2 * kk);
+        }
+    } else {
+        for (int e = lane; e < nSym * 8; e += 32) {
+            const int s = e >> 3, kk = e & 7;
+            const int a = 2 * kk;
+            if (a < nRows) {
+                const uint32_t d = yst + s * 128 + ((kk ^ ((s & 1) << 2)) << 4);
+                const float2* src = ysrc + (long)s * A + a;
+                if (a + 1 < nRows) cp_async16(d, src);
+                else cp_async8(d, src);
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ int group_valid(const FusedCell& cl, long grp) {
     return (int)min((long)cl.GS, (long)cl.nSC - (grp - cl.group0) * cl.GS);
 }
 
-template <int P>
+// LTF = 0: any mix of cells.  LTF in {2, 4, 8, 16}: every cell has
+// nLayers == LTF and 16-byte aligned H / Y_rx (the host checks), so the layer
+// tile, strides and masks are compile-time constants.
+template <int P, int LTF>
 __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant__ FusedParams p) {
     extern __shared__ float4 smem_raw[];
     const int lane = threadIdx.x & 31;
@@ -585,7 +658,10 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     auto produce = [&]() {
         if (pg < total) {
             const FusedCell& cl = p.cell[pci];
-            stage_item(cl, phs, pys, pch, stBase + pslot * p.stageBytes, lane);
+            if constexpr (LTF != 0)
+                stage_item_exact<LTF>(cl, phs, pys, pch, stBase + pslot * p.stageBytes, lane);
+            else
+                stage_item(cl, phs, pys, pch, stBase + pslot * p.stageBytes, lane);
             if (++pch == cl.nChunk) {
                 pch = 0;
                 if (++pq < pValid) {
@@ -634,26 +710,34 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
         cp_async_wait<NST - 1>();                  // this item's copies (own lane) have landed
         __syncwarp();                              // ... and every lane's
         const FusedCell& cl = p.cell[ci];
-        const int LT = cl.LT;
+        const int LT = LTF != 0 ? LTF : cl.LT;
         const uint32_t st = stBase + cslot * p.stageBytes;
         cslot = cslot == NST - 1 ? 0 : cslot + 1;
         const int nRows = min(CHUNK, cl.A - CHUNK * ch);
         const bool z2 = cl.nSym > 8;
-        switch (LT) {
-            case 1: mma_stage<1, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
-            case 2: mma_stage<2, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
-            case 4: mma_stage<4, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
-            case 8: mma_stage<8, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
-            default: mma_stage<16, P>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+        if constexpr (LTF != 0) {
+            mma_stage<LTF, P, true>(st, hrs_of(LTF), nRows, LTF, cl.nSym, gacc, zacc, z2, g, c);
+        } else {
+            switch (LT) {
+                case 1: mma_stage<1, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+                case 2: mma_stage<2, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+                case 4: mma_stage<4, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+                case 8: mma_stage<8, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+                default: mma_stage<16, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+            }
         }
         if (++ch < cl.nChunk) continue;
         ch = 0;
-        switch (LT) {
-            case 1: store_acc<1>(sm, gacc, zacc, q, g, c); break;
-            case 2: store_acc<2>(sm, gacc, zacc, q, g, c); break;
-            case 4: store_acc<4>(sm, gacc, zacc, q, g, c); break;
-            case 8: store_acc<8>(sm, gacc, zacc, q, g, c); break;
-            default: store_acc<16>(sm, gacc, zacc, q, g, c); break;
+        if constexpr (LTF != 0) {
+            store_acc<LTF>(sm, gacc, zacc, q, g, c);
+        } else {
+            switch (LT) {
+                case 1: store_acc<1>(sm, gacc, zacc, q, g, c); break;
+                case 2: store_acc<2>(sm, gacc, zacc, q, g, c); break;
+                case 4: store_acc<4>(sm, gacc, zacc, q, g, c); break;
+                case 8: store_acc<8>(sm, gacc, zacc, q, g, c); break;
+                default: store_acc<16>(sm, gacc, zacc, q, g, c); break;
+            }
         }
 #pragma unroll
         for (int b = 0; b < 3; b++)
@@ -669,12 +753,16 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
         __syncwarp();
         const CellView v = view_of(cl);
         const long sc0 = (grp - cl.group0) * cl.GS;
-        switch (LT) {
-            case 1: solve_group<1, P>(v, sc0, nValid, smemOff, lane); break;
-            case 2: solve_group<2, P>(v, sc0, nValid, smemOff, lane); break;
-            case 4: solve_group<4, P>(v, sc0, nValid, smemOff, lane); break;
-            case 8: solve_group<8, P>(v, sc0, nValid, smemOff, lane); break;
-            default: solve_group<16, P>(v, sc0, nValid, smemOff, lane); break;
+        if constexpr (LTF != 0) {
+            solve_group<LTF, P>(v, sc0, nValid, smemOff, lane);
+        } else {
+            switch (LT) {
+                case 1: solve_group<1, P>(v, sc0, nValid, smemOff, lane); break;
+                case 2: solve_group<2, P>(v, sc0, nValid, smemOff, lane); break;
+                case 4: solve_group<4, P>(v, sc0, nValid, smemOff, lane); break;
+                case 8: solve_group<8, P>(v, sc0, nValid, smemOff, lane); break;
+                default: solve_group<16, P>(v, sc0, nValid, smemOff, lane); break;
+            }
         }
         q = 0;
         grp += nw;
@@ -779,12 +867,13 @@ static LaunchShape default_shape(int warpBytes) {
     return {1, 1};
 }
 
-template <int P>
-static int launch_fused_p(const FusedParams& p, int warpBytes, LaunchShape sh, cudaStream_t st) {
+template <int P, int LTF>
+static int launch_fused_v(const FusedParams& p, int warpBytes, LaunchShape sh, cudaStream_t st) {
     const int bytes = sh.warps * warpBytes;
     static int configured = 0;
     if (bytes > 48 * 1024 && bytes > configured) {
-        cudaError_t e = cudaFuncSetAttribute(fused_eq_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaError_t e =
+            cudaFuncSetAttribute(fused_eq_kernel<P, LTF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         if (e != cudaSuccess) return (int)e;
         configured = bytes;
     }
@@ -792,8 +881,31 @@ static int launch_fused_p(const FusedParams& p, int warpBytes, LaunchShape sh, c
     long grid = (long)sm_count() * sh.ctasPerSm;
     if (grid > need) grid = need;
     if (grid < 1) grid = 1;
-    fused_eq_kernel<P><<<(unsigned)grid, sh.warps * 32, bytes, st>>>(p);
+    fused_eq_kernel<P, LTF><<<(unsigned)grid, sh.warps * 32, bytes, st>>>(p);
     return launch_status();
+}
+
+// The layer tile shared by every cell when each has nLayers == tile in
+// {2, 4, 8, 16} and 16-byte aligned H / Y_rx; 0 otherwise (generic kernel).
+static int exact_tile(const FusedParams& p) {
+    const int lt = p.cell[0].LT;
+    if (lt < 2) return 0;
+    for (int i = 0; i < p.nCells; i++) {
+        const FusedCell& c = p.cell[i];
+        if (c.LT != lt || c.L != lt || !c.vecH || !c.vecY) return 0;
+    }
+    return lt;
+}
+
+template <int P>
+static int launch_fused_p(const FusedParams& p, int warpBytes, LaunchShape sh, cudaStream_t st) {
+    switch (exact_tile(p)) {
+        case 2: return launch_fused_v<P, 2>(p, warpBytes, sh, st);
+        case 4: return launch_fused_v<P, 4>(p, warpBytes, sh, st);
+        case 8: return launch_fused_v<P, 8>(p, warpBytes, sh, st);
+        case 16: return launch_fused_v<P, 16>(p, warpBytes, sh, st);
+        default: return launch_fused_v<P, 0>(p, warpBytes, sh, st);
+    }
 }
 
 int launch_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, cudaStream_t st) {

@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--slots", type=int, default=16, help="cell-slots per step (per GPU)")
+    ap.add_argument("--slots", type=int, default=64, help="cell-slots per step (per GPU)")
     ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16", "bf16x3"])
     ap.add_argument("--soak", type=float, default=1.5, help="seconds of untimed load before timing (clock steady state)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
