@@ -86,6 +86,7 @@ SIGNATURES = {
     "aerial_pusch_eq_plain_workspace": (_Z, [ctypes.POINTER(CellDesc), _I]),
     "aerial_pusch_eq_plain": (_I, [ctypes.POINTER(CellDesc), _I, _P, _Z, _P]),
     "aerial_autotune": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), ctypes.POINTER(_F), _P]),
+    "aerial_pusch_eq_plain_static": (_I, [ctypes.POINTER(CellDesc), _I, _P]),
 }
 
 
@@ -231,6 +232,14 @@ def pusch_eq_plain(cells, workspace, stream=None):
     arr, n = _cells_array(cells)
     _check(lib().aerial_pusch_eq_plain(arr, n, _ptr(workspace), workspace.numel() * workspace.element_size(),
                                        _stream(stream)), "pusch_eq_plain")
+
+
+def pusch_eq_plain_static(cells, stream=None):
+    """The plain FP32 chain without a workspace argument, for callers that cannot
+    allocate device memory: intermediates live in the library's static 16 MiB
+    device array (shared by all calls; calls overlapping on the GPU race)."""
+    arr, n = _cells_array(cells)
+    _check(lib().aerial_pusch_eq_plain_static(arr, n, _stream(stream)), "pusch_eq_plain_static")
 
 
 def autotune(cells, precision=PREC_FP16, stream=None):

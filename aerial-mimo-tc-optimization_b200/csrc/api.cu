@@ -11,6 +11,7 @@ extern "C" const char* aerial_error_string(int status) {
         case AERIAL_ERR_QUEUE_FULL: return "submission queue full";
         case AERIAL_ERR_TIMEOUT: return "bounded wait ran out";
         case AERIAL_ERR_NOT_FOUND: return "unknown cell or request";
+        case AERIAL_ERR_SCRATCH_LIMIT: return "request needs more than the library's static scratch (16 MiB)";
         default:
             if (status > 0 && status < 1000) return cudaGetErrorString((cudaError_t)status);
             return "unknown status";

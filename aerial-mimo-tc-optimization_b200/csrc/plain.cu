@@ -318,3 +318,54 @@ extern "C" int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, 
     }
     return AERIAL_OK;
 }
+
+// ---------------------------------------------------------------------------
+// The plain chain for callers that must not allocate device memory.
+//
+// Some hosts cannot call cudaMalloc on the path that equalizes a slot: a
+// real-time receiver loop where an allocation may block or synchronize the
+// device and miss the slot deadline, or a plugin inside a framework that owns
+// all device memory and hands out none.  This entry point keeps the plain
+// chain's intermediates (G, C, noiseInv, Y_eq) in one file-scope device array
+// instead of a caller workspace.  The array is part of the module image, so
+// every GPU that loads this library holds it until the process exits.
+//
+// The array's host-side name is only a stand-in for the device symbol; the
+// device address comes from cudaGetSymbolAddress, done once per device with
+// that device current, on the first call made on it (which must therefore
+// happen before any stream capture).  All calls share the one array and it
+// keeps the last call's contents: every scratch byte a call reads is first
+// written by that same call, so nothing needs clearing, but calls that
+// overlap on the GPU (two streams, two threads) race on it.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+static __device__ __align__(256) unsigned char g_plain_static_scratch[AERIAL_STATIC_SCRATCH_BYTES];
+
+static int static_scratch_address(void** out) {
+    static std::mutex mu;
+    static void* addr[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    if (dev < 0 || dev >= 64) return AERIAL_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_plain_static_scratch);
+        if (e != cudaSuccess) return (int)e;
+        addr[dev] = p;
+    }
+    *out = addr[dev];
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_pusch_eq_plain_static(const aerial_cell_desc* cells, int nCells, void* stream) {
+    if (!cells || nCells < 1) return AERIAL_ERR_INVALID_ARG;
+    if (aerial_pusch_eq_plain_workspace(cells, nCells) > (size_t)AERIAL_STATIC_SCRATCH_BYTES)
+        return AERIAL_ERR_SCRATCH_LIMIT;
+    void* scratch = nullptr;
+    const int s = static_scratch_address(&scratch);
+    if (s != AERIAL_OK) return s;
+    return aerial_pusch_eq_plain(cells, nCells, scratch, (size_t)AERIAL_STATIC_SCRATCH_BYTES, stream);
+}

@@ -58,7 +58,8 @@ enum {
     AERIAL_ERR_BUDGET = 1004,        /* serving: request exceeds the memory budget */
     AERIAL_ERR_QUEUE_FULL = 1005,    /* serving: submission queue full */
     AERIAL_ERR_TIMEOUT = 1006,       /* a bounded wait ran out */
-    AERIAL_ERR_NOT_FOUND = 1007      /* serving: unknown cell or request */
+    AERIAL_ERR_NOT_FOUND = 1007,     /* serving: unknown cell or request */
+    AERIAL_ERR_SCRATCH_LIMIT = 1008  /* request needs more than the library's static scratch */
 };
 
 /* Supported envelope: 1 <= nLayers <= 16, 1 <= nSym <= 16, 1 <= nAnt <= 256,
@@ -179,6 +180,21 @@ int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, const aeria
 size_t aerial_pusch_eq_plain_workspace(const aerial_cell_desc* cells, int nCells);
 int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, void* workspace,
                           size_t workspaceBytes, void* stream);
+
+/* The plain chain for callers that cannot allocate device memory -- a
+ * real-time slot loop where cudaMalloc may block or synchronize the device,
+ * or a plugin whose host framework owns all device memory.  No counterpart in
+ * the reference.  Same cells and results as aerial_pusch_eq_plain, but the
+ * intermediates live in one static device array of
+ * AERIAL_STATIC_SCRATCH_BYTES (16 MiB) inside this library, held on every GPU
+ * that loads it until exit; a batch whose largest cell needs more (see
+ * aerial_pusch_eq_plain_workspace; e.g. a 273-PRB, 128-antenna, 16-layer
+ * cell) is rejected with AERIAL_ERR_SCRATCH_LIMIT before anything runs.
+ * The first call on each device looks up the array's device address (make
+ * that call before any stream capture).  Calls share the array, so calls
+ * that overlap on the GPU race; nothing is allocated or freed. */
+#define AERIAL_STATIC_SCRATCH_BYTES (16u << 20)
+int aerial_pusch_eq_plain_static(const aerial_cell_desc* cells, int nCells, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Autotuner                                                                  */
