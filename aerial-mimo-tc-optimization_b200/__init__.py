@@ -87,6 +87,10 @@ SIGNATURES = {
     "aerial_pusch_eq_plain": (_I, [ctypes.POINTER(CellDesc), _I, _P, _Z, _P]),
     "aerial_autotune": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), ctypes.POINTER(_F), _P]),
     "aerial_pusch_eq_plain_static": (_I, [ctypes.POINTER(CellDesc), _I, _P]),
+    "aerial_eq_graph_create": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), ctypes.POINTER(_P)]),
+    "aerial_eq_graph_update": (_I, [_P, ctypes.POINTER(CellDesc), _I]),
+    "aerial_eq_graph_launch": (_I, [_P, _P]),
+    "aerial_eq_graph_destroy": (_I, [_P]),
 }
 
 
@@ -249,3 +253,35 @@ def autotune(cells, precision=PREC_FP16, stream=None):
     us = ctypes.c_float(0.0)
     _check(lib().aerial_autotune(arr, n, ctypes.pointer(t), ctypes.pointer(us), _stream(stream)), "autotune")
     return t, float(us.value)
+
+
+class FusedGraph:
+    """The fused launch for a fixed set of cell shapes as an executable CUDA graph.
+
+    ``update(cells)`` re-points it at new buffers (same shapes); ``launch()``
+    replays it.  Call ``close()`` (or use as a context manager) to free it."""
+
+    def __init__(self, cells, tuning: Tuning | None = None):
+        arr, n = _cells_array(cells)
+        h = ctypes.c_void_p()
+        tp = ctypes.pointer(tuning) if tuning is not None else None
+        _check(lib().aerial_eq_graph_create(arr, n, tp, ctypes.byref(h)), "eq_graph_create")
+        self._h = h
+
+    def update(self, cells):
+        arr, n = _cells_array(cells)
+        _check(lib().aerial_eq_graph_update(self._h, arr, n), "eq_graph_update")
+
+    def launch(self, stream=None):
+        _check(lib().aerial_eq_graph_launch(self._h, _stream(stream)), "eq_graph_launch")
+
+    def close(self):
+        if self._h:
+            _check(lib().aerial_eq_graph_destroy(self._h), "eq_graph_destroy")
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -867,8 +867,16 @@ static LaunchShape default_shape(int warpBytes) {
     return {1, 1};
 }
 
+// A resolved launch: kernel instantiation, grid, block and dynamic shared
+// memory.  Resolving also raises the kernel's shared-memory limit once.
+struct LaunchPlan {
+    const void* func;
+    dim3 grid, block;
+    int smem;
+};
+
 template <int P, int LTF>
-static int launch_fused_v(const FusedParams& p, int warpBytes, LaunchShape sh, cudaStream_t st) {
+static int plan_v(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
     const int bytes = sh.warps * warpBytes;
     static int configured = 0;
     if (bytes > 48 * 1024 && bytes > configured) {
@@ -881,8 +889,11 @@ static int launch_fused_v(const FusedParams& p, int warpBytes, LaunchShape sh, c
     long grid = (long)sm_count() * sh.ctasPerSm;
     if (grid > need) grid = need;
     if (grid < 1) grid = 1;
-    fused_eq_kernel<P, LTF><<<(unsigned)grid, sh.warps * 32, bytes, st>>>(p);
-    return launch_status();
+    out.func = reinterpret_cast<const void*>(fused_eq_kernel<P, LTF>);
+    out.grid = dim3((unsigned)grid);
+    out.block = dim3(sh.warps * 32);
+    out.smem = bytes;
+    return AERIAL_OK;
 }
 
 // The layer tile shared by every cell when each has nLayers == tile in
@@ -898,25 +909,45 @@ static int exact_tile(const FusedParams& p) {
 }
 
 template <int P>
-static int launch_fused_p(const FusedParams& p, int warpBytes, LaunchShape sh, cudaStream_t st) {
+static int plan_p(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
     switch (exact_tile(p)) {
-        case 2: return launch_fused_v<P, 2>(p, warpBytes, sh, st);
-        case 4: return launch_fused_v<P, 4>(p, warpBytes, sh, st);
-        case 8: return launch_fused_v<P, 8>(p, warpBytes, sh, st);
-        case 16: return launch_fused_v<P, 16>(p, warpBytes, sh, st);
-        default: return launch_fused_v<P, 0>(p, warpBytes, sh, st);
+        case 2: return plan_v<P, 2>(p, warpBytes, sh, out);
+        case 4: return plan_v<P, 4>(p, warpBytes, sh, out);
+        case 8: return plan_v<P, 8>(p, warpBytes, sh, out);
+        case 16: return plan_v<P, 16>(p, warpBytes, sh, out);
+        default: return plan_v<P, 0>(p, warpBytes, sh, out);
     }
 }
 
-int launch_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, cudaStream_t st) {
+int plan_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, LaunchPlan& out) {
     if (sh.warps < 1 || sh.warps > 8 || sh.ctasPerSm < 1 || sh.ctasPerSm > 8) return AERIAL_ERR_INVALID_ARG;
     if ((long)sh.warps * warpBytes * sh.ctasPerSm > 227 * 1024 || (long)sh.warps * warpBytes > 227 * 1024)
         return AERIAL_ERR_UNSUPPORTED;
     switch (prec) {
-        case AERIAL_PREC_FP16: return launch_fused_p<AERIAL_PREC_FP16>(p, warpBytes, sh, st);
-        case AERIAL_PREC_BF16: return launch_fused_p<AERIAL_PREC_BF16>(p, warpBytes, sh, st);
-        case AERIAL_PREC_BF16X3: return launch_fused_p<AERIAL_PREC_BF16X3>(p, warpBytes, sh, st);
+        case AERIAL_PREC_FP16: return plan_p<AERIAL_PREC_FP16>(p, warpBytes, sh, out);
+        case AERIAL_PREC_BF16: return plan_p<AERIAL_PREC_BF16>(p, warpBytes, sh, out);
+        case AERIAL_PREC_BF16X3: return plan_p<AERIAL_PREC_BF16X3>(p, warpBytes, sh, out);
         default: return AERIAL_ERR_UNSUPPORTED;
+    }
+}
+
+int launch_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, cudaStream_t st) {
+    LaunchPlan pl;
+    int s = plan_fused(p, warpBytes, prec, sh, pl);
+    if (s) return s;
+    void* args[] = {const_cast<FusedParams*>(&p)};
+    cudaError_t e = cudaLaunchKernel(pl.func, pl.grid, pl.block, args, (size_t)pl.smem, st);
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
+// Resolve precision and launch shape from an optional tuning struct.
+static void resolve_tuning(const aerial_tuning* tuning, int warpBytes, int& prec, LaunchShape& sh) {
+    sh = default_shape(warpBytes);
+    prec = AERIAL_PREC_FP16;
+    if (tuning) {
+        prec = tuning->precision;
+        if (tuning->warps_per_cta) sh.warps = tuning->warps_per_cta;
+        if (tuning->ctas_per_sm) sh.ctasPerSm = tuning->ctas_per_sm;
     }
 }
 
@@ -930,13 +961,9 @@ extern "C" int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, 
     int warpBytes = 0;
     int s = build_fused_params(cells, nCells, p, warpBytes);
     if (s) return s;
-    LaunchShape sh = default_shape(warpBytes);
-    int prec = AERIAL_PREC_FP16;
-    if (tuning) {
-        prec = tuning->precision;
-        if (tuning->warps_per_cta) sh.warps = tuning->warps_per_cta;
-        if (tuning->ctas_per_sm) sh.ctasPerSm = tuning->ctas_per_sm;
-    }
+    LaunchShape sh;
+    int prec;
+    resolve_tuning(tuning, warpBytes, prec, sh);
     return launch_fused(p, warpBytes, prec, sh, to_stream(stream));
 }
 
@@ -990,4 +1017,95 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
     best->sc_per_group = 0;
     if (bestUs) *bestUs = bestT * 1000.f;
     return AERIAL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CUDA graph of the persistent launch.  The graph holds one kernel node built
+// directly (no stream capture); aerial_eq_graph_update re-points it at new
+// slot buffers / noise levels of the same cell shapes with
+// cudaGraphExecKernelNodeSetParams, so a slot loop replays one executable
+// graph per slot without re-instantiation.
+// ---------------------------------------------------------------------------
+struct aerial_eq_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNode_t node = nullptr;
+    FusedParams params;
+    LaunchPlan plan;
+};
+
+static cudaKernelNodeParams node_params(aerial_eq_graph* g, void** args) {
+    cudaKernelNodeParams kp{};
+    kp.func = const_cast<void*>(g->plan.func);
+    kp.gridDim = g->plan.grid;
+    kp.blockDim = g->plan.block;
+    kp.sharedMemBytes = (unsigned)g->plan.smem;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    return kp;
+}
+
+extern "C" int aerial_eq_graph_create(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
+                                      aerial_eq_graph** out) {
+    if (!out) return AERIAL_ERR_INVALID_ARG;
+    *out = nullptr;
+    aerial_eq_graph* g = new aerial_eq_graph();
+    int warpBytes = 0;
+    int s = build_fused_params(cells, nCells, g->params, warpBytes);
+    if (!s) {
+        LaunchShape sh;
+        int prec;
+        resolve_tuning(tuning, warpBytes, prec, sh);
+        s = plan_fused(g->params, warpBytes, prec, sh, g->plan);
+    }
+    cudaError_t e = cudaSuccess;
+    if (!s) e = cudaGraphCreate(&g->graph, 0);
+    if (!s && e == cudaSuccess) {
+        void* args[] = {&g->params};
+        cudaKernelNodeParams kp = node_params(g, args);
+        e = cudaGraphAddKernelNode(&g->node, g->graph, nullptr, 0, &kp);
+    }
+    if (!s && e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (!s && e != cudaSuccess) s = (int)e;
+    if (s) {
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        if (g->graph) cudaGraphDestroy(g->graph);
+        delete g;
+        return s;
+    }
+    *out = g;
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_eq_graph_update(aerial_eq_graph* g, const aerial_cell_desc* cells, int nCells) {
+    if (!g || !cells || nCells != g->params.nCells) return AERIAL_ERR_INVALID_ARG;
+    FusedParams np;
+    int warpBytes = 0;
+    int s = build_fused_params(cells, nCells, np, warpBytes);
+    if (s) return s;
+    for (int i = 0; i < nCells; i++) {
+        const FusedCell &a = np.cell[i], &b = g->params.cell[i];
+        if (a.nSC != b.nSC || a.A != b.A || a.L != b.L || a.nSym != b.nSym || a.nPam != b.nPam ||
+            a.vecH != b.vecH || a.vecY != b.vecY)
+            return AERIAL_ERR_UNSUPPORTED;      // a new shape needs a new graph
+    }
+    g->params = np;
+    void* args[] = {&g->params};
+    cudaKernelNodeParams kp = node_params(g, args);
+    cudaError_t e = cudaGraphExecKernelNodeSetParams(g->exec, g->node, &kp);
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
+extern "C" int aerial_eq_graph_launch(aerial_eq_graph* g, void* stream) {
+    if (!g) return AERIAL_ERR_INVALID_ARG;
+    cudaError_t e = cudaGraphLaunch(g->exec, to_stream(stream));
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
+extern "C" int aerial_eq_graph_destroy(aerial_eq_graph* g) {
+    if (!g) return AERIAL_ERR_INVALID_ARG;
+    cudaError_t e1 = g->exec ? cudaGraphExecDestroy(g->exec) : cudaSuccess;
+    cudaError_t e2 = g->graph ? cudaGraphDestroy(g->graph) : cudaSuccess;
+    delete g;
+    return e1 != cudaSuccess ? (int)e1 : (e2 != cudaSuccess ? (int)e2 : AERIAL_OK);
 }

@@ -126,6 +126,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(values, world: int, device=None):
+    """Element-wise max of per-rank timings (ms) across the process group.
+
+    Every rank calls it at the same point with the same number of values.
+    With world == 1 it returns the values unchanged."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def whole_job_rate(units_per_rank_per_step: int, steps: int, world: int, max_elapsed_ms: float) -> float:
+    """Whole-job throughput: all ranks' units over the slowest rank's time (weak scaling)."""
+    return world * units_per_rank_per_step * steps / (max_elapsed_ms / 1e3)
+
+
 def cpu_chain_rate(orc, cell, seconds: float):
     """REs/s of the scalar FP32 chain on the host cores over a bounded sample."""
     H, Y = cell.H.numpy(), cell.Y.numpy()
@@ -261,12 +280,8 @@ def main():
     clocks = sampler.stop()
     elapsed_ms = e0.elapsed_time(e1)
     launch_ms = [s.elapsed_time(e) for s, e in ev]
-    t = torch.tensor([elapsed_ms, statistics.mean(launch_ms)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_ms, launch_avg_ms = float(t[0]), float(t[1])
-
-    value = world * res_per_step * a.steps / (elapsed_ms / 1e3)
+    elapsed_ms, launch_avg_ms = max_over_ranks([elapsed_ms, statistics.mean(launch_ms)], world, dev)
+    value = whole_job_rate(res_per_step, a.steps, world, elapsed_ms)
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_step / (launch_avg_ms / 1e3) / 1e9
     tr = ncu_traffic_per_slot()
@@ -305,10 +320,8 @@ def main():
             e2e_step()
         s1.record(stream)
         torch.cuda.synchronize()
-        t2 = torch.tensor([s0.elapsed_time(s1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * res_per_step * k2 / (float(t2[0]) / 1e3), "unit": UNIT,
+        e2e_ms, = max_over_ranks([s0.elapsed_time(s1)], world, dev)
+        e2e = {"value": whole_job_rate(res_per_step, k2, world, e2e_ms), "unit": UNIT,
                "h2d_bytes_per_step": in_bytes_per_step, "d2h_bytes_per_step": out_bytes_per_step,
                "steps": k2, "path": "pinned host H, Y_rx -> aerial_pusch_eq_fused -> pinned host LLR, one stream"}
         # parity of the end-to-end output against the resident run

@@ -196,6 +196,18 @@ int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, void* works
 #define AERIAL_STATIC_SCRATCH_BYTES (16u << 20)
 int aerial_pusch_eq_plain_static(const aerial_cell_desc* cells, int nCells, void* stream);
 
+/* The same fused launch as an executable CUDA graph (one kernel node, built
+ * without stream capture).  aerial_eq_graph_update re-points the node at new
+ * buffers / sigma2 of cells with the same shapes (AERIAL_ERR_UNSUPPORTED if a
+ * shape changes); launching replays the graph on `stream`.  No counterpart in
+ * the reference (it has no graphs). */
+typedef struct aerial_eq_graph aerial_eq_graph;
+int aerial_eq_graph_create(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
+                           aerial_eq_graph** out);
+int aerial_eq_graph_update(aerial_eq_graph* graph, const aerial_cell_desc* cells, int nCells);
+int aerial_eq_graph_launch(aerial_eq_graph* graph, void* stream);
+int aerial_eq_graph_destroy(aerial_eq_graph* graph);
+
 /* ------------------------------------------------------------------------ */
 /* Autotuner                                                                  */
 /* ------------------------------------------------------------------------ */
