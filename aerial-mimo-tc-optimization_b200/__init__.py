@@ -67,6 +67,45 @@ class Tuning(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    """``aerial_server_config``."""
+
+    _fields_ = [
+        ("memory_budget_bytes", ctypes.c_int64),
+        ("streams", ctypes.c_int),
+        ("max_batch", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("mode", ctypes.c_int),
+        ("queue_capacity", ctypes.c_int),
+        ("start_paused", ctypes.c_int),
+        ("deadline_us", ctypes.c_float),
+    ]
+
+
+class ServerCompletion(ctypes.Structure):
+    _fields_ = [("request_id", ctypes.c_uint64), ("cell_id", ctypes.c_int), ("status", ctypes.c_int),
+                ("latency_us", ctypes.c_float)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("slots_done", ctypes.c_long),
+        ("p50_us", ctypes.c_float), ("p99_us", ctypes.c_float), ("max_us", ctypes.c_float),
+        ("mean_us", ctypes.c_float),
+        ("deadline_misses", ctypes.c_long),
+        ("res_done", ctypes.c_long),
+        ("span_s", ctypes.c_double),
+        ("res_per_s", ctypes.c_double),
+        ("batches", ctypes.c_long),
+        ("mean_batch", ctypes.c_float),
+        ("srs_updates", ctypes.c_long),
+        ("budget_used_bytes", ctypes.c_int64),
+        ("pending", ctypes.c_long),
+    ]
+
+
+SERVER_FUSED, SERVER_PLAIN = 0, 1
+
 _LIB = None
 
 # exported symbol -> (restype, argtypes)
@@ -91,6 +130,17 @@ SIGNATURES = {
     "aerial_eq_graph_update": (_I, [_P, ctypes.POINTER(CellDesc), _I]),
     "aerial_eq_graph_launch": (_I, [_P, _P]),
     "aerial_eq_graph_destroy": (_I, [_P]),
+    "aerial_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
+    "aerial_server_destroy": (_I, [_P]),
+    "aerial_server_add_cell": (_I, [_P, _I, _I, _I, _I, _I, _F, ctypes.POINTER(_I)]),
+    "aerial_server_set_channel": (_I, [_P, _I, _P, _F]),
+    "aerial_server_srs_update": (_I, [_P, _I, _P, _P, _P, _I, _I, ctypes.POINTER(ctypes.c_uint64)]),
+    "aerial_server_submit": (_I, [_P, _I, _P, _P, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64)]),
+    "aerial_server_poll": (_I, [_P, ctypes.POINTER(ServerCompletion), _I, ctypes.POINTER(_I)]),
+    "aerial_server_wait": (_I, [_P, ctypes.c_uint64, _I]),
+    "aerial_server_drain": (_I, [_P, _I]),
+    "aerial_server_pause": (_I, [_P, _I]),
+    "aerial_server_stats": (_I, [_P, ctypes.POINTER(ServerStats)]),
 }
 
 
@@ -278,6 +328,83 @@ class FusedGraph:
     def close(self):
         if self._h:
             _check(lib().aerial_eq_graph_destroy(self._h), "eq_graph_destroy")
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Server:
+    """The slot-serving loop (continuous batching into fused launches).
+
+    Cells are registered with ``add_cell`` and keep their channel resident;
+    ``submit`` queues one slot (device tensors in / out) and returns its id;
+    completions come back through ``poll`` / ``wait`` / ``drain``; ``stats``
+    reports p50/p99 latency, deadline misses and REs/s."""
+
+    def __init__(self, memory_budget_bytes=16 << 30, streams=3, max_batch=64, precision=PREC_FP16,
+                 mode=SERVER_FUSED, queue_capacity=0, start_paused=False, deadline_us=500.0):
+        if isinstance(precision, str):
+            precision = PREC_NAMES[precision]
+        cfg = ServerConfig(int(memory_budget_bytes), int(streams), int(max_batch), int(precision), int(mode),
+                           int(queue_capacity), int(bool(start_paused)), float(deadline_us))
+        h = ctypes.c_void_p()
+        _check(lib().aerial_server_create(ctypes.byref(cfg), ctypes.byref(h)), "server_create")
+        self._h = h
+
+    def add_cell(self, nPRB, nAnt, nLayers, nSym, nPamBits, sigma2) -> int:
+        cid = ctypes.c_int()
+        _check(lib().aerial_server_add_cell(self._h, nPRB, nAnt, nLayers, nSym, nPamBits, float(sigma2),
+                                            ctypes.byref(cid)), "server_add_cell")
+        return cid.value
+
+    def set_channel(self, cell, H, sigma2):
+        _check(lib().aerial_server_set_channel(self._h, cell, ctypes.c_void_p(H.data_ptr()), float(sigma2)),
+               "server_set_channel")
+
+    def srs_update(self, cell, SRS, W, FOCC, K, foccLen) -> int:
+        rid = ctypes.c_uint64()
+        _check(lib().aerial_server_srs_update(self._h, cell, _ptr(SRS), _ptr(W), _ptr(FOCC), K, foccLen,
+                                              ctypes.byref(rid)), "server_srs_update")
+        return rid.value
+
+    def submit(self, cell, Y, llr_out, arrival_ns=0) -> int:
+        rid = ctypes.c_uint64()
+        _check(lib().aerial_server_submit(self._h, cell, _ptr(Y), _ptr(llr_out), int(arrival_ns),
+                                          ctypes.byref(rid)), "server_submit")
+        return rid.value
+
+    def submit_status(self, cell, Y, llr_out, arrival_ns=0) -> int:
+        """submit() returning the raw status instead of raising."""
+        rid = ctypes.c_uint64()
+        return lib().aerial_server_submit(self._h, cell, _ptr(Y), _ptr(llr_out), int(arrival_ns), ctypes.byref(rid))
+
+    def poll(self, max_out=4096):
+        buf = (ServerCompletion * max_out)()
+        n = ctypes.c_int()
+        _check(lib().aerial_server_poll(self._h, buf, max_out, ctypes.byref(n)), "server_poll")
+        return [(buf[i].request_id, buf[i].cell_id, buf[i].status, buf[i].latency_us) for i in range(n.value)]
+
+    def wait(self, request_id, timeout_ms=10000) -> int:
+        return lib().aerial_server_wait(self._h, request_id, int(timeout_ms))
+
+    def drain(self, timeout_ms=60000):
+        _check(lib().aerial_server_drain(self._h, int(timeout_ms)), "server_drain")
+
+    def pause(self, paused=True):
+        _check(lib().aerial_server_pause(self._h, int(bool(paused))), "server_pause")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().aerial_server_stats(self._h, ctypes.byref(st)), "server_stats")
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self):
+        if self._h:
+            _check(lib().aerial_server_destroy(self._h), "server_destroy")
             self._h = None
 
     def __enter__(self):

@@ -1,0 +1,489 @@
+// server.cu -- slot-serving loop: continuous batching of per-cell slot
+// requests into fused equalization launches.
+//
+// Cells are registered once; their channel estimates (H) and noise level stay
+// resident in device memory owned by the server and are refreshed in place by
+// SRS filter-multiply updates.  Slot requests reference the slot's received
+// samples and LLR output in device memory (fronthaul data lands in GPU memory)
+// and are admitted against a device-memory budget that covers the resident
+// channels plus the buffers of every admitted request; a request that does not
+// fit waits, in arrival order, until completions free memory.  A dispatcher
+// thread takes whatever is admitted and pending as soon as one of the server's
+// streams is free and launches it as ONE fused kernel, so batches overlap on
+// the device; completion is observed by polling CUDA events.  Per-subcarrier
+// results do not depend on batch composition (the fused kernel's guarantee),
+// so a slot's LLRs are the same alone and in any mix.
+//
+// The reference has no serving layer: its multi-cell study
+// (src/multicell_contention.cu:167-235) launches one kernel per cell on its
+// own stream and measures the contention; this loop replaces that pattern.
+#include "common.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace aeq {
+
+static int64_t now_ns() {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct SrvCell {
+    aerial_cell_desc shape{};   // H points at the resident channel; Y_rx/llr unused
+    aerial_cf32* H = nullptr;
+    size_t hBytes = 0;
+    int inflight = 0;           // requests of this cell inside launched batches
+    bool srsBusy = false;       // an SRS update of the resident channel is running
+    int64_t reqBytes = 0;       // Y_rx + LLR bytes of one slot
+    long res = 0;               // REs per slot (subcarriers x symbols)
+};
+
+struct SrvReq {
+    uint64_t id = 0;
+    int kind = 0;               // 0 slot, 1 SRS update
+    int cell = 0;
+    const aerial_cf32* Y = nullptr;
+    float* llr = nullptr;
+    // SRS update operands
+    const aerial_ch2 *srs = nullptr, *W = nullptr, *focc = nullptr;
+    int K = 0, P = 0, F = 0;
+    int64_t arrival = 0, launched = 0, done = 0;
+    int status = AERIAL_OK;
+    bool admitted = false, finished = false;
+};
+
+struct SrvBatch {
+    cudaEvent_t ev = nullptr;
+    std::vector<SrvReq*> reqs;
+    bool busy = false;
+};
+
+}  // namespace aeq
+
+using namespace aeq;
+
+struct aerial_server {
+    aerial_server_config cfg{};
+    int device = 0;
+    std::mutex mu;
+    std::condition_variable cv;        // wakes the dispatcher
+    std::condition_variable doneCv;    // wakes waiters
+    std::vector<SrvCell> cells;
+    std::deque<SrvReq*> pending;
+    std::unordered_map<uint64_t, SrvReq*> byId;
+    std::deque<SrvReq*> completed;     // not yet returned by poll
+    std::vector<cudaStream_t> streams;
+    std::vector<SrvBatch> batches;     // one per stream
+    std::vector<void*> plainWs;        // per-stream workspace of the plain-chain mode
+    size_t plainWsBytes = 0;
+    int64_t used = 0;                  // budget in use (resident H + admitted requests)
+    uint64_t nextId = 1;
+    bool stop = false, paused = false;
+    std::thread th;
+    // statistics
+    std::vector<int64_t> lat;          // completion - arrival (ns) of finished slots
+    int64_t firstArrival = 0, lastDone = 0;
+    long resDone = 0, batchesLaunched = 0, slotsLaunched = 0, srsDone = 0, misses = 0;
+    int launchError = 0;
+};
+
+static void finish_batch(aerial_server* s, SrvBatch& b, int status) {
+    const int64_t t = now_ns();
+    for (SrvReq* r : b.reqs) {
+        r->done = t;
+        r->finished = true;
+        if (status) r->status = status;
+        SrvCell& c = s->cells[r->cell];
+        c.inflight--;
+        if (r->kind == 0) {
+            s->used -= c.reqBytes;
+            const int64_t l = r->done - r->arrival;
+            s->lat.push_back(l);
+            if (l > (int64_t)(s->cfg.deadline_us * 1000.0)) s->misses++;
+            s->resDone += c.res;
+            s->lastDone = std::max(s->lastDone, t);
+        } else {
+            s->srsDone++;
+            c.srsBusy = false;
+        }
+        s->completed.push_back(r);
+    }
+    b.reqs.clear();
+    b.busy = false;
+}
+
+// Launch one batch from the head of the pending queue on stream i.  Called
+// with the lock held.  Returns true if something was launched.
+static bool launch_batch(aerial_server* s, int i) {
+    SrvBatch& b = s->batches[i];
+    cudaStream_t st = s->streams[i];
+    // an SRS update at the head runs alone, once its cell has nothing in flight
+    if (!s->pending.empty() && s->pending.front()->kind == 1) {
+        SrvReq* r = s->pending.front();
+        SrvCell& c = s->cells[r->cell];
+        if (c.inflight) return false;
+        s->pending.pop_front();
+        const int nBlocks = c.shape.nPRB * 12 / r->K;
+        r->launched = now_ns();
+        int st1 = aerial_srs_to_channel(c.H, r->srs, r->W, r->focc, c.shape.nAnt, nBlocks, r->K, r->P, r->F, st);
+        c.inflight++;
+        c.srsBusy = true;
+        b.reqs.push_back(r);
+        b.busy = true;
+        if (st1) { finish_batch(s, b, st1); return true; }
+        cudaEventRecord(b.ev, st);
+        return true;
+    }
+    aerial_cell_desc descs[AERIAL_MAX_CELLS];
+    int n = 0;
+    const int cap = std::min(std::max(1, s->cfg.max_batch), (int)AERIAL_MAX_CELLS);
+    while (!s->pending.empty() && n < cap) {
+        SrvReq* r = s->pending.front();
+        if (r->kind != 0) break;                       // SRS update: next batch
+        SrvCell& c = s->cells[r->cell];
+        if (c.srsBusy) break;                          // its channel is being rewritten: wait, in order
+        if (!r->admitted) {
+            if (s->used + c.reqBytes > s->cfg.memory_budget_bytes) break;   // waits, in order
+            s->used += c.reqBytes;
+            r->admitted = true;
+        }
+        s->pending.pop_front();
+        aerial_cell_desc d = c.shape;
+        d.Y_rx = r->Y;
+        d.llr = r->llr;
+        d.Y_eq = nullptr;
+        descs[n++] = d;
+        c.inflight++;
+        r->launched = now_ns();
+        b.reqs.push_back(r);
+    }
+    if (!n) return false;
+    int status;
+    if (s->cfg.mode == AERIAL_SERVER_PLAIN) {
+        // the plain FP32 chain, request by request (comparison mode)
+        status = AERIAL_OK;
+        for (int k = 0; k < n && !status; k++)
+            status = aerial_pusch_eq_plain(&descs[k], 1, s->plainWs[i], s->plainWsBytes, st);
+    } else {
+        aerial_tuning t{s->cfg.precision, 0, 0, 0};
+        status = aerial_pusch_eq_fused(descs, n, &t, st);
+    }
+    b.busy = true;
+    s->batchesLaunched++;
+    s->slotsLaunched += n;
+    if (status) {
+        s->launchError = status;
+        finish_batch(s, b, status);
+        return true;
+    }
+    cudaEventRecord(b.ev, st);
+    return true;
+}
+
+static void dispatcher(aerial_server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        bool progress = false;
+        // completions
+        for (SrvBatch& b : s->batches) {
+            if (!b.busy) continue;
+            cudaError_t e = cudaEventQuery(b.ev);
+            if (e == cudaSuccess) {
+                finish_batch(s, b, AERIAL_OK);
+                progress = true;
+            } else if (e != cudaErrorNotReady) {
+                finish_batch(s, b, (int)e);
+                progress = true;
+            }
+        }
+        if (progress) s->doneCv.notify_all();
+        // launches
+        if (!s->paused) {
+            for (size_t i = 0; i < s->batches.size(); i++)
+                if (!s->batches[i].busy && !s->pending.empty()) progress |= launch_batch(s, (int)i);
+        }
+        bool anyBusy = false;
+        for (SrvBatch& b : s->batches) anyBusy |= b.busy;
+        if (anyBusy) {
+            // poll the in-flight events without sleeping: completion times are
+            // taken when the event is seen, so the loop stays tight
+            lk.unlock();
+            std::this_thread::yield();
+            lk.lock();
+        } else if (!progress) {
+            s->cv.wait_for(lk, std::chrono::milliseconds(2));
+        }
+    }
+}
+
+extern "C" int aerial_server_create(const aerial_server_config* cfg, aerial_server** out) {
+    if (!cfg || !out || cfg->memory_budget_bytes <= 0 || cfg->streams < 1 || cfg->streams > 16 ||
+        cfg->max_batch < 1 || cfg->deadline_us <= 0.f)
+        return AERIAL_ERR_INVALID_ARG;
+    *out = nullptr;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return AERIAL_ERR_NO_DEVICE;
+    aerial_server* s = new aerial_server();
+    s->cfg = *cfg;
+    s->device = dev;
+    s->paused = cfg->start_paused != 0;
+    s->streams.resize(cfg->streams);
+    s->batches.resize(cfg->streams);
+    for (int i = 0; i < cfg->streams; i++) {
+        e = cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->batches[i].ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            for (int k = 0; k <= i; k++) {
+                if (s->streams[k]) cudaStreamDestroy(s->streams[k]);
+                if (s->batches[k].ev) cudaEventDestroy(s->batches[k].ev);
+            }
+            delete s;
+            return (int)e;
+        }
+    }
+    s->th = std::thread(dispatcher, s);
+    *out = s;
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_destroy(aerial_server* s) {
+    if (!s) return AERIAL_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    s->th.join();
+    for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
+    for (size_t i = 0; i < s->streams.size(); i++) {
+        cudaEventDestroy(s->batches[i].ev);
+        cudaStreamDestroy(s->streams[i]);
+    }
+    for (SrvCell& c : s->cells) cudaFree(c.H);
+    for (void* w : s->plainWs) cudaFree(w);
+    for (auto& kv : s->byId) delete kv.second;
+    delete s;
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_add_cell(aerial_server* s, int nPRB, int nAnt, int nLayers, int nSym, int nPamBits,
+                                      float sigma2, int* cellId) {
+    if (!s || !cellId || nPRB < 1 || nAnt < 1 || nAnt > AERIAL_MAX_ANTS || nLayers < 1 ||
+        nLayers > AERIAL_MAX_LAYERS || nSym < 1 || nSym > AERIAL_MAX_SYMS || nPamBits < 1 || nPamBits > 4 ||
+        !(sigma2 >= 0.f))
+        return AERIAL_ERR_INVALID_ARG;
+    SrvCell c;
+    const long nSC = 12L * nPRB;
+    c.hBytes = sizeof(aerial_cf32) * nSC * nAnt * nLayers;
+    c.reqBytes = (int64_t)(sizeof(aerial_cf32) * nSC * nSym * nAnt + sizeof(float) * nSC * nLayers * nSym * 2 * nPamBits);
+    c.res = nSC * nSym;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->used + (int64_t)c.hBytes + c.reqBytes > s->cfg.memory_budget_bytes) return AERIAL_ERR_BUDGET;
+    cudaError_t e = cudaMalloc(&c.H, c.hBytes);
+    if (e != cudaSuccess) return (int)e;
+    cudaMemset(c.H, 0, c.hBytes);
+    c.shape.H = c.H;
+    c.shape.sigma2 = sigma2;
+    c.shape.nPRB = nPRB;
+    c.shape.nAnt = nAnt;
+    c.shape.nLayers = nLayers;
+    c.shape.nSym = nSym;
+    c.shape.nPamBits = nPamBits;
+    s->used += (int64_t)c.hBytes;
+    if (s->cfg.mode == AERIAL_SERVER_PLAIN) {
+        // the plain chain's intermediates, one workspace per stream, sized for the largest cell
+        const size_t need = aerial_pusch_eq_plain_workspace(&c.shape, 1);
+        if (need > s->plainWsBytes) {
+            const int64_t extra = (int64_t)(need - s->plainWsBytes) * (int64_t)s->streams.size();
+            if (s->used + extra + c.reqBytes > s->cfg.memory_budget_bytes) {
+                s->used -= (int64_t)c.hBytes;
+                cudaFree(c.H);
+                return AERIAL_ERR_BUDGET;
+            }
+            s->plainWs.resize(s->streams.size(), nullptr);
+            for (void*& w : s->plainWs) {
+                cudaFree(w);
+                w = nullptr;
+                e = cudaMalloc(&w, need);
+                if (e != cudaSuccess) return (int)e;
+            }
+            s->used += extra;
+            s->plainWsBytes = need;
+        }
+    }
+    s->cells.push_back(c);
+    *cellId = (int)s->cells.size() - 1;
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_set_channel(aerial_server* s, int cellId, const aerial_cf32* H, float sigma2) {
+    if (!s || !H || !(sigma2 >= 0.f)) return AERIAL_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (cellId < 0 || cellId >= (int)s->cells.size()) return AERIAL_ERR_NOT_FOUND;
+    SrvCell& c = s->cells[cellId];
+    // wait (bounded) until no launched batch reads the resident channel
+    const auto limit = std::chrono::steady_clock::now() + std::chrono::seconds(5);
+    while (c.inflight) {
+        if (s->doneCv.wait_until(lk, limit) == std::cv_status::timeout && c.inflight) return AERIAL_ERR_TIMEOUT;
+    }
+    cudaError_t e = cudaMemcpy(c.H, H, c.hBytes, cudaMemcpyDefault);
+    c.shape.sigma2 = sigma2;
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
+extern "C" int aerial_server_submit(aerial_server* s, int cellId, const aerial_cf32* Y_rx, float* llr,
+                                    int64_t arrival_ns, uint64_t* requestId) {
+    if (!s || !Y_rx || !llr) return AERIAL_ERR_INVALID_ARG;
+    SrvReq* r = new SrvReq();
+    r->Y = Y_rx;
+    r->llr = llr;
+    r->arrival = arrival_ns > 0 ? arrival_ns : now_ns();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (cellId < 0 || cellId >= (int)s->cells.size()) { delete r; return AERIAL_ERR_NOT_FOUND; }
+        if (s->cells[cellId].reqBytes + (int64_t)s->cells[cellId].hBytes > s->cfg.memory_budget_bytes) {
+            delete r;
+            return AERIAL_ERR_BUDGET;
+        }
+        if ((int)s->pending.size() >= (s->cfg.queue_capacity > 0 ? s->cfg.queue_capacity : 1 << 20)) {
+            delete r;
+            return AERIAL_ERR_QUEUE_FULL;
+        }
+        r->cell = cellId;
+        r->id = s->nextId++;
+        if (!s->firstArrival || r->arrival < s->firstArrival) s->firstArrival = r->arrival;
+        s->byId[r->id] = r;
+        s->pending.push_back(r);
+        if (requestId) *requestId = r->id;
+    }
+    s->cv.notify_one();
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_srs_update(aerial_server* s, int cellId, const aerial_ch2* SRS, const aerial_ch2* W,
+                                        const aerial_ch2* FOCC, int K, int foccLen, uint64_t* requestId) {
+    if (!s || !SRS || !W || !FOCC || K < 1 || foccLen < 1) return AERIAL_ERR_INVALID_ARG;
+    SrvReq* r = new SrvReq();
+    r->kind = 1;
+    r->srs = SRS;
+    r->W = W;
+    r->focc = FOCC;
+    r->K = K;
+    r->F = foccLen;
+    r->arrival = now_ns();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (cellId < 0 || cellId >= (int)s->cells.size()) { delete r; return AERIAL_ERR_NOT_FOUND; }
+        const SrvCell& c = s->cells[cellId];
+        if ((c.shape.nPRB * 12) % K) { delete r; return AERIAL_ERR_INVALID_ARG; }
+        r->P = c.shape.nLayers;           // one SRS port per layer
+        r->cell = cellId;
+        r->id = s->nextId++;
+        s->byId[r->id] = r;
+        s->pending.push_back(r);
+        if (requestId) *requestId = r->id;
+    }
+    s->cv.notify_one();
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_poll(aerial_server* s, aerial_server_completion* out, int maxOut, int* nOut) {
+    if (!s || !nOut || (maxOut > 0 && !out)) return AERIAL_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    int n = 0;
+    while (n < maxOut && !s->completed.empty()) {
+        SrvReq* r = s->completed.front();
+        s->completed.pop_front();
+        out[n].request_id = r->id;
+        out[n].cell_id = r->cell;
+        out[n].status = r->status;
+        out[n].latency_us = (float)((r->done - r->arrival) * 1e-3);
+        n++;
+        s->byId.erase(r->id);
+        delete r;
+    }
+    *nOut = n;
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_wait(aerial_server* s, uint64_t requestId, int timeout_ms) {
+    if (!s) return AERIAL_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->byId.find(requestId);
+    if (it == s->byId.end()) return AERIAL_ERR_NOT_FOUND;
+    SrvReq* r = it->second;
+    const auto limit = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms);
+    while (!r->finished) {
+        if (s->doneCv.wait_until(lk, limit) == std::cv_status::timeout && !r->finished) return AERIAL_ERR_TIMEOUT;
+    }
+    return r->status;
+}
+
+extern "C" int aerial_server_drain(aerial_server* s, int timeout_ms) {
+    if (!s) return AERIAL_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    const auto limit = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms);
+    auto busy = [&] {
+        if (!s->pending.empty()) return true;
+        for (SrvBatch& b : s->batches)
+            if (b.busy) return true;
+        return false;
+    };
+    while (busy()) {
+        if (s->doneCv.wait_until(lk, limit) == std::cv_status::timeout && busy()) return AERIAL_ERR_TIMEOUT;
+    }
+    return s->launchError;
+}
+
+extern "C" int aerial_server_pause(aerial_server* s, int paused) {
+    if (!s) return AERIAL_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->paused = paused != 0;
+    }
+    s->cv.notify_one();
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_stats(aerial_server* s, aerial_server_statistics* out) {
+    if (!s || !out) return AERIAL_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    aerial_server_statistics st{};
+    std::vector<int64_t> l = s->lat;
+    st.slots_done = (long)l.size();
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double p) {
+            size_t i = (size_t)std::ceil(p / 100.0 * l.size());
+            if (i < 1) i = 1;
+            return l[std::min(l.size(), i) - 1] * 1e-3;
+        };
+        st.p50_us = (float)pct(50);
+        st.p99_us = (float)pct(99);
+        st.max_us = (float)(l.back() * 1e-3);
+        double sum = 0;
+        for (int64_t v : l) sum += v;
+        st.mean_us = (float)(sum / l.size() * 1e-3);
+    }
+    st.deadline_misses = s->misses;
+    st.res_done = s->resDone;
+    st.span_s = (s->lastDone > s->firstArrival) ? (double)(s->lastDone - s->firstArrival) * 1e-9 : 0.0;
+    st.res_per_s = st.span_s > 0 ? st.res_done / st.span_s : 0.0;
+    st.batches = s->batchesLaunched;
+    st.mean_batch = s->batchesLaunched ? (float)s->slotsLaunched / s->batchesLaunched : 0.f;
+    st.srs_updates = s->srsDone;
+    st.budget_used_bytes = s->used;
+    st.pending = (long)s->pending.size();
+    *out = st;
+    return AERIAL_OK;
+}

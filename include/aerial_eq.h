@@ -209,6 +209,79 @@ int aerial_eq_graph_launch(aerial_eq_graph* graph, void* stream);
 int aerial_eq_graph_destroy(aerial_eq_graph* graph);
 
 /* ------------------------------------------------------------------------ */
+/* Slot-serving loop                                                          */
+/*                                                                            */
+/* Cells are registered once; their channel estimate H and noise variance     */
+/* stay resident in device memory owned by the server (refreshed by           */
+/* aerial_server_set_channel or, on the device, by an SRS filter-multiply     */
+/* update).  A slot request names the slot's received samples and LLR output  */
+/* in device memory.  Requests are admitted against a device-memory budget   */
+/* (resident channels + the buffers of every admitted request); one that does */
+/* not fit waits, in arrival order.  A dispatcher thread launches whatever is */
+/* admitted and pending as one fused kernel whenever one of the server's      */
+/* streams is free, so batches overlap on the device; results per subcarrier  */
+/* are independent of the batch.  No counterpart in the reference, whose     */
+/* multi-cell study runs one kernel per cell on its own stream                */
+/* (src/multicell_contention.cu:167-235).                                     */
+/* ------------------------------------------------------------------------ */
+enum { AERIAL_SERVER_FUSED = 0, AERIAL_SERVER_PLAIN = 1 };
+
+typedef struct {
+    int64_t memory_budget_bytes;  /* device-memory admission budget */
+    int streams;                  /* batches in flight at once (1..16) */
+    int max_batch;                /* cell-slots per launch (1..AERIAL_MAX_CELLS) */
+    int precision;                /* AERIAL_PREC_* of the fused kernel */
+    int mode;                     /* AERIAL_SERVER_FUSED, or AERIAL_SERVER_PLAIN: the plain FP32
+                                     chain request by request (comparison) */
+    int queue_capacity;           /* pending requests accepted (0 = unbounded) */
+    int start_paused;             /* 1: queue without dispatching until aerial_server_pause(s, 0) */
+    float deadline_us;            /* slot deadline counted by the statistics */
+} aerial_server_config;
+
+typedef struct {
+    uint64_t request_id;
+    int cell_id;
+    int status;                   /* 0 or the launch's status */
+    float latency_us;             /* completion - arrival */
+} aerial_server_completion;
+
+typedef struct {
+    long slots_done;
+    float p50_us, p99_us, max_us, mean_us;   /* slot latency: completion - arrival */
+    long deadline_misses;
+    long res_done;                /* equalized REs (subcarrier x symbol) */
+    double span_s;                /* first arrival -> last completion */
+    double res_per_s;
+    long batches;
+    float mean_batch;             /* cell-slots per launch */
+    long srs_updates;
+    int64_t budget_used_bytes;
+    long pending;
+} aerial_server_statistics;
+
+typedef struct aerial_server aerial_server;
+
+int aerial_server_create(const aerial_server_config* cfg, aerial_server** out);
+int aerial_server_destroy(aerial_server* server);
+int aerial_server_add_cell(aerial_server* server, int nPRB, int nAnt, int nLayers, int nSym, int nPamBits,
+                           float sigma2, int* cellId);
+/* Copy a channel estimate (host or device memory) into the cell's resident H. */
+int aerial_server_set_channel(aerial_server* server, int cellId, const aerial_cf32* H, float sigma2);
+/* Queue an SRS update: filter multiply into the cell's resident H (one SRS
+ * port per layer, K subcarriers per block); slots queued after it see it. */
+int aerial_server_srs_update(aerial_server* server, int cellId, const aerial_ch2* SRS, const aerial_ch2* W,
+                             const aerial_ch2* FOCC, int K, int foccLen, uint64_t* requestId);
+/* Queue one slot: Y_rx [nSC][nSym][nAnt] in, LLRs out (device memory).
+ * arrival_ns: steady-clock arrival time in ns (0 = now). */
+int aerial_server_submit(aerial_server* server, int cellId, const aerial_cf32* Y_rx, float* llr,
+                         int64_t arrival_ns, uint64_t* requestId);
+int aerial_server_poll(aerial_server* server, aerial_server_completion* out, int maxOut, int* nOut);
+int aerial_server_wait(aerial_server* server, uint64_t requestId, int timeout_ms);
+int aerial_server_drain(aerial_server* server, int timeout_ms);
+int aerial_server_pause(aerial_server* server, int paused);
+int aerial_server_stats(aerial_server* server, aerial_server_statistics* out);
+
+/* ------------------------------------------------------------------------ */
 /* Autotuner                                                                  */
 /* ------------------------------------------------------------------------ */
 

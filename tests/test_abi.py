@@ -58,3 +58,18 @@ def test_invalid_arguments_rejected_before_any_launch():
     assert lib.aerial_pusch_eq_fused(cells, 1, None, None) == 1001     # null buffers
     assert lib.aerial_pusch_eq_fused(cells, 0, None, None) == 1001
     assert lib.aerial_pusch_eq_fused(cells, 65, None, None) == 1001
+
+
+def test_server_rejects_bad_config_without_gpu():
+    """Host-side argument checks of the serving loop (no device needed)."""
+    pkg = load_pkg()
+    lib = pkg.lib()
+    h = ctypes.c_void_p()
+    assert lib.aerial_server_create(None, ctypes.byref(h)) == 1001
+    cfg = pkg.ServerConfig(0, 2, 64, 0, 0, 0, 0, 500.0)          # zero budget
+    assert lib.aerial_server_create(ctypes.byref(cfg), ctypes.byref(h)) == 1001
+    cfg = pkg.ServerConfig(1 << 30, 0, 64, 0, 0, 0, 0, 500.0)    # no stream
+    assert lib.aerial_server_create(ctypes.byref(cfg), ctypes.byref(h)) == 1001
+    assert lib.aerial_server_destroy(None) == 1001
+    n = ctypes.c_int()
+    assert lib.aerial_server_poll(None, None, 0, ctypes.byref(n)) == 1001

@@ -1,0 +1,136 @@
+"""The slot-serving loop: continuous batching into fused launches.
+
+Each slot's LLRs must be bit-identical to the same slot equalized alone by a
+single fused launch, whatever else shares its batch; admission holds requests
+that do not fit the memory budget until completions free it; a bounded wait
+on a paused server returns a timeout status (host-side failure injection, no
+GPU fault); SRS updates rewrite the resident channel before later slots."""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+TIMEOUT = 1006
+
+
+def _alone(aeq, c, H, Y, cuda, plain=False):
+    llr = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+    d = aeq.cell_desc(H, Y, llr, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+    if plain:
+        ws = torch.empty(aeq.pusch_eq_plain_workspace([d]), dtype=torch.uint8, device=cuda)
+        aeq.pusch_eq_plain([d], ws)
+    else:
+        aeq.pusch_eq_fused([d])
+    torch.cuda.synchronize()
+    return llr.cpu().numpy()
+
+
+def _cells(wl, n, seed):
+    shapes = wl.multicell_shapes(n, seed=seed)
+    return [wl.make_cell(min(p, 51), a, l, 11, q, snr, "iid", seed=seed + 7 * i)
+            for i, (p, a, l, q, snr) in enumerate(shapes)]
+
+
+@pytest.mark.parametrize("mode", ["fused", "plain"])
+def test_server_results_same_alone_and_in_mix(aeq, wl, cuda, mode):
+    cells = _cells(wl, 6, 101)
+    slots = 3
+    with aeq.Server(streams=3, mode=aeq.SERVER_PLAIN if mode == "plain" else aeq.SERVER_FUSED) as srv:
+        ids, outs, Ys = [], [], []
+        cid = []
+        for c in cells:
+            k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
+            srv.set_channel(k, c.H.to(cuda), c.sigma2)
+            cid.append(k)
+        gens = [[wl.make_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, 4 ** c.nPamBits, c.snr_db, seed=900 + 31 * i + s)
+                 for s in range(slots)] for i, c in enumerate(cells)]
+        for s in range(slots):                       # interleave the cells' slots
+            for i, c in enumerate(cells):
+                Y = gens[i][s].Y.to(cuda)
+                out = torch.full((c.llr_numel,), float("nan"), dtype=torch.float32, device=cuda)
+                ids.append(srv.submit(cid[i], Y, out))
+                outs.append((i, s, out))
+                Ys.append(Y)
+        srv.drain()
+        done = srv.poll()
+        assert len(done) == len(ids) and all(st == 0 for _, _, st, _ in done)
+        stats = srv.stats()
+        assert stats["slots_done"] == len(ids) and stats["p99_us"] >= stats["p50_us"] > 0
+    torch.cuda.synchronize()
+    for (i, s, out), Y in zip(outs, Ys):
+        c = cells[i]
+        ref = _alone(aeq, c, c.H.to(cuda), Y, cuda, plain=(mode == "plain"))
+        np.testing.assert_array_equal(out.cpu().numpy(), ref)
+
+
+def test_server_budget_admission_serializes(aeq, wl, cuda):
+    c = wl.make_cell(24, 32, 4, 11, 16, 20.0, seed=111)
+    h_bytes = 8 * c.nSC * c.nAnt * c.nLayers
+    req_bytes = 8 * c.nSC * c.nSym * c.nAnt + 4 * c.llr_numel
+    with aeq.Server(memory_budget_bytes=h_bytes + req_bytes, streams=3) as srv:
+        k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
+        srv.set_channel(k, c.H.to(cuda), c.sigma2)
+        Y = c.Y.to(cuda)
+        outs = [torch.empty(c.llr_numel, dtype=torch.float32, device=cuda) for _ in range(8)]
+        for o in outs:
+            srv.submit(k, Y, o)
+        srv.drain()
+        st = srv.stats()
+        assert st["slots_done"] == 8
+        assert st["mean_batch"] == 1.0                 # one admitted request at a time
+        assert st["budget_used_bytes"] == h_bytes       # every request released its share
+    ref = _alone(aeq, c, c.H.to(cuda), Y, cuda)
+    for o in outs:
+        np.testing.assert_array_equal(o.cpu().numpy(), ref)
+
+
+def test_server_rejects_cell_beyond_budget(aeq, cuda):
+    with aeq.Server(memory_budget_bytes=1 << 20, streams=1) as srv:
+        with pytest.raises(aeq.AerialError):
+            srv.add_cell(132, 64, 8, 11, 4, 0.01)     # 6.5 MB of channel alone
+
+
+def test_server_bounded_wait_times_out_while_paused(aeq, wl, cuda):
+    c = wl.make_cell(4, 16, 2, 11, 4, 15.0, seed=121)
+    with aeq.Server(streams=1, start_paused=True) as srv:
+        k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
+        srv.set_channel(k, c.H.to(cuda), c.sigma2)
+        out = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+        rid = srv.submit(k, c.Y.to(cuda), out)
+        t0 = time.monotonic()
+        assert srv.wait(rid, timeout_ms=50) == TIMEOUT
+        assert time.monotonic() - t0 < 5.0
+        assert srv.stats()["pending"] == 1
+        srv.pause(False)
+        assert srv.wait(rid, timeout_ms=10000) == 0
+        assert srv.wait(10 ** 9, timeout_ms=10) == 1007   # unknown request
+
+
+def test_server_srs_update_rewrites_resident_channel(aeq, orc, wl, cuda):
+    K, F = 12, 12
+    c = wl.make_cell(2, 32, 4, 11, 16, 20.0, seed=131)
+    nBlk = c.nSC // K
+    s, w, f = orc.ref_srs_inputs(5, nBlk * c.nAnt * K, K * K, c.nLayers * F)
+    dS = torch.from_numpy(s.view(np.int16)).to(cuda)
+    dW = torch.from_numpy(w.view(np.int16)).to(cuda)
+    dF = torch.from_numpy(f.view(np.int16)).to(cuda)
+    Hsrs = torch.empty(c.nSC, c.nAnt, c.nLayers, dtype=torch.complex64, device=cuda)
+    aeq.srs_to_channel(Hsrs, dS, dW, dF, c.nAnt, nBlk, K, c.nLayers, F)
+    Y = c.Y.to(cuda)
+    with aeq.Server(streams=2) as srv:
+        k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
+        srv.set_channel(k, c.H.to(cuda), c.sigma2)
+        before = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+        after = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+        srv.submit(k, Y, before)
+        srv.srs_update(k, dS, dW, dF, K, F)
+        srv.submit(k, Y, after)
+        srv.drain()
+        assert srv.stats()["srs_updates"] == 1
+    np.testing.assert_array_equal(before.cpu().numpy(), _alone(aeq, c, c.H.to(cuda), Y, cuda))
+    np.testing.assert_array_equal(after.cpu().numpy(), _alone(aeq, c, Hsrs, Y, cuda))
