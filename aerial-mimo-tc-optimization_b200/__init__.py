@@ -79,6 +79,8 @@ class ServerConfig(ctypes.Structure):
         ("queue_capacity", ctypes.c_int),
         ("start_paused", ctypes.c_int),
         ("deadline_us", ctypes.c_float),
+        ("batch_window_us", ctypes.c_float),
+        ("min_batch", ctypes.c_int),
     ]
 
 
@@ -92,6 +94,8 @@ class ServerStats(ctypes.Structure):
         ("slots_done", ctypes.c_long),
         ("p50_us", ctypes.c_float), ("p99_us", ctypes.c_float), ("max_us", ctypes.c_float),
         ("mean_us", ctypes.c_float),
+        ("queue_p99_us", ctypes.c_float),
+        ("service_p99_us", ctypes.c_float),
         ("deadline_misses", ctypes.c_long),
         ("res_done", ctypes.c_long),
         ("span_s", ctypes.c_double),
@@ -113,6 +117,7 @@ _P, _I, _F, _Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_size_t
 SIGNATURES = {
     "aerial_error_string": (ctypes.c_char_p, [_I]),
     "aerial_version": (_I, []),
+    "aerial_prepare": (_I, []),
     "aerial_coef_apply": (_I, [_P, _P, _P, _I, _I, _I, _I, _P]),
     "aerial_coef_apply_tc": (_I, [_P, _P, _P, _I, _I, _I, _I, _P]),
     "aerial_gram": (_I, [_P, _F, _P, _I, _I, _I, _P]),
@@ -141,6 +146,7 @@ SIGNATURES = {
     "aerial_server_drain": (_I, [_P, _I]),
     "aerial_server_pause": (_I, [_P, _I]),
     "aerial_server_stats": (_I, [_P, ctypes.POINTER(ServerStats)]),
+    "aerial_server_reset_stats": (_I, [_P]),
 }
 
 
@@ -163,6 +169,11 @@ def _lib_handle():
 def lib():
     """The loaded ``libaerial_eq.so`` (ctypes handle)."""
     return _lib_handle()
+
+
+def prepare():
+    """Load every kernel of the library on the current device (avoids first-launch stalls)."""
+    _check(lib().aerial_prepare(), "prepare")
 
 
 def _check(status: int, where: str) -> None:
@@ -346,11 +357,13 @@ class Server:
     reports p50/p99 latency, deadline misses and REs/s."""
 
     def __init__(self, memory_budget_bytes=16 << 30, streams=3, max_batch=64, precision=PREC_FP16,
-                 mode=SERVER_FUSED, queue_capacity=0, start_paused=False, deadline_us=500.0):
+                 mode=SERVER_FUSED, queue_capacity=0, start_paused=False, deadline_us=500.0,
+                 batch_window_us=0.0, min_batch=0):
         if isinstance(precision, str):
             precision = PREC_NAMES[precision]
         cfg = ServerConfig(int(memory_budget_bytes), int(streams), int(max_batch), int(precision), int(mode),
-                           int(queue_capacity), int(bool(start_paused)), float(deadline_us))
+                           int(queue_capacity), int(bool(start_paused)), float(deadline_us),
+                           float(batch_window_us), int(min_batch))
         h = ctypes.c_void_p()
         _check(lib().aerial_server_create(ctypes.byref(cfg), ctypes.byref(h)), "server_create")
         self._h = h
@@ -401,6 +414,9 @@ class Server:
         st = ServerStats()
         _check(lib().aerial_server_stats(self._h, ctypes.byref(st)), "server_stats")
         return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def reset_stats(self):
+        _check(lib().aerial_server_reset_stats(self._h), "server_reset_stats")
 
     def close(self):
         if self._h:

@@ -19,3 +19,14 @@ extern "C" const char* aerial_error_string(int status) {
 }
 
 extern "C" int aerial_version(void) { return 10000; /* 1.0.0 */ }
+
+namespace aeq {
+int prepare_fused_kernels();
+}
+
+// Load the library's kernels on the current device (see the header).
+extern "C" int aerial_prepare(void) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return AERIAL_ERR_NO_DEVICE;
+    return aeq::prepare_fused_kernels();
+}

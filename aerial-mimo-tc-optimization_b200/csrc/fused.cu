@@ -1109,3 +1109,38 @@ extern "C" int aerial_eq_graph_destroy(aerial_eq_graph* g) {
     delete g;
     return e1 != cudaSuccess ? (int)e1 : (e2 != cudaSuccess ? (int)e2 : AERIAL_OK);
 }
+
+namespace aeq {
+
+// ---------------------------------------------------------------------------
+// Load every fused-kernel instantiation on the current device and raise its
+// shared-memory limit, so the first launch of a variant inside a latency-
+// critical loop does not pay module loading.
+// ---------------------------------------------------------------------------
+template <int P, int LTF>
+static int prepare_v() {
+    cudaFuncAttributes at;
+    cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel<P, LTF>);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fused_eq_kernel<P, LTF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
+template <int P>
+static int prepare_p() {
+    int s = prepare_v<P, 0>();
+    if (!s) s = prepare_v<P, 2>();
+    if (!s) s = prepare_v<P, 4>();
+    if (!s) s = prepare_v<P, 8>();
+    if (!s) s = prepare_v<P, 16>();
+    return s;
+}
+
+int prepare_fused_kernels() {
+    int s = prepare_p<AERIAL_PREC_FP16>();
+    if (!s) s = prepare_p<AERIAL_PREC_BF16>();
+    if (!s) s = prepare_p<AERIAL_PREC_BF16X3>();
+    return s;
+}
+
+}  // namespace aeq

@@ -83,6 +83,7 @@ struct aerial_server {
     std::vector<cudaStream_t> streams;
     std::vector<SrvBatch> batches;     // one per stream
     std::vector<void*> plainWs;        // per-stream workspace of the plain-chain mode
+    std::vector<char> blocked;         // per-cell scratch of form_batch
     size_t plainWsBytes = 0;
     int64_t used = 0;                  // budget in use (resident H + admitted requests)
     uint64_t nextId = 1;
@@ -90,9 +91,11 @@ struct aerial_server {
     std::thread th;
     // statistics
     std::vector<int64_t> lat;          // completion - arrival (ns) of finished slots
+    std::vector<int64_t> qlat, slat;   // arrival -> launch, launch -> completion
     int64_t firstArrival = 0, lastDone = 0;
     long resDone = 0, batchesLaunched = 0, slotsLaunched = 0, srsDone = 0, misses = 0;
     int launchError = 0;
+    int inflightBatches = 0;           // batches launched and not finished (under mu)
 };
 
 static void finish_batch(aerial_server* s, SrvBatch& b, int status) {
@@ -107,6 +110,8 @@ static void finish_batch(aerial_server* s, SrvBatch& b, int status) {
             s->used -= c.reqBytes;
             const int64_t l = r->done - r->arrival;
             s->lat.push_back(l);
+            s->qlat.push_back(r->launched - r->arrival);
+            s->slat.push_back(r->done - r->launched);
             if (l > (int64_t)(s->cfg.deadline_us * 1000.0)) s->misses++;
             s->resDone += c.res;
             s->lastDone = std::max(s->lastDone, t);
@@ -120,108 +125,170 @@ static void finish_batch(aerial_server* s, SrvBatch& b, int status) {
     b.busy = false;
 }
 
-// Launch one batch from the head of the pending queue on stream i.  Called
-// with the lock held.  Returns true if something was launched.
-static bool launch_batch(aerial_server* s, int i) {
-    SrvBatch& b = s->batches[i];
-    cudaStream_t st = s->streams[i];
-    // an SRS update at the head runs alone, once its cell has nothing in flight
-    if (!s->pending.empty() && s->pending.front()->kind == 1) {
-        SrvReq* r = s->pending.front();
-        SrvCell& c = s->cells[r->cell];
-        if (c.inflight) return false;
-        s->pending.pop_front();
-        const int nBlocks = c.shape.nPRB * 12 / r->K;
-        r->launched = now_ns();
-        int st1 = aerial_srs_to_channel(c.H, r->srs, r->W, r->focc, c.shape.nAnt, nBlocks, r->K, r->P, r->F, st);
-        c.inflight++;
-        c.srsBusy = true;
-        b.reqs.push_back(r);
-        b.busy = true;
-        if (st1) { finish_batch(s, b, st1); return true; }
-        cudaEventRecord(b.ev, st);
-        return true;
-    }
+// A batch formed under the lock and launched outside it.
+struct Formed {
+    int n = 0;                          // slot requests (0: none)
     aerial_cell_desc descs[AERIAL_MAX_CELLS];
-    int n = 0;
+    bool srs = false;                   // an SRS update instead
+    aerial_cf32* H = nullptr;
+    const aerial_ch2 *S = nullptr, *W = nullptr, *F = nullptr;
+    int nAnt = 0, nBlocks = 0, K = 0, P = 0, foccLen = 0;
+};
+
+// Form one batch for stream i from the pending queue; lock held.
+//
+// Order is kept per cell, not globally: a cell's slots never overtake its
+// queued SRS update (which waits until none of that cell's slots is in
+// flight, then runs alone), but other cells' slots pass it.  Admission is in
+// arrival order: the first slot that does not fit the budget stops the scan.
+static void form_batch(aerial_server* s, int i, Formed& f) {
+    SrvBatch& b = s->batches[i];
     const int cap = std::min(std::max(1, s->cfg.max_batch), (int)AERIAL_MAX_CELLS);
-    while (!s->pending.empty() && n < cap) {
-        SrvReq* r = s->pending.front();
-        if (r->kind != 0) break;                       // SRS update: next batch
+    std::vector<char>& blocked = s->blocked;
+    blocked.assign(s->cells.size(), 0);
+    int scanned = 0;
+    for (size_t k = 0; k < s->pending.size() && f.n < cap && scanned < 1024; scanned++) {
+        SrvReq* r = s->pending[k];
         SrvCell& c = s->cells[r->cell];
-        if (c.srsBusy) break;                          // its channel is being rewritten: wait, in order
+        if (r->kind == 1) {
+            if (!blocked[r->cell] && !c.inflight && !c.srsBusy && f.n == 0) {
+                s->pending.erase(s->pending.begin() + k);
+                r->launched = now_ns();
+                c.inflight++;
+                c.srsBusy = true;
+                b.reqs.push_back(r);
+                f.srs = true;
+                f.H = c.H;
+                f.S = r->srs;
+                f.W = r->W;
+                f.F = r->focc;
+                f.nAnt = c.shape.nAnt;
+                f.nBlocks = c.shape.nPRB * 12 / r->K;
+                f.K = r->K;
+                f.P = r->P;
+                f.foccLen = r->F;
+                return;
+            }
+            blocked[r->cell] = 1;       // the cell's later slots wait behind its update
+            k++;
+            continue;
+        }
+        if (blocked[r->cell] || c.srsBusy) {
+            blocked[r->cell] = 1;
+            k++;
+            continue;
+        }
         if (!r->admitted) {
-            if (s->used + c.reqBytes > s->cfg.memory_budget_bytes) break;   // waits, in order
+            if (s->used + c.reqBytes > s->cfg.memory_budget_bytes) break;   // waits, in arrival order
             s->used += c.reqBytes;
             r->admitted = true;
         }
-        s->pending.pop_front();
+        s->pending.erase(s->pending.begin() + k);
         aerial_cell_desc d = c.shape;
         d.Y_rx = r->Y;
         d.llr = r->llr;
         d.Y_eq = nullptr;
-        descs[n++] = d;
+        f.descs[f.n++] = d;
         c.inflight++;
         r->launched = now_ns();
         b.reqs.push_back(r);
     }
-    if (!n) return false;
-    int status;
-    if (s->cfg.mode == AERIAL_SERVER_PLAIN) {
-        // the plain FP32 chain, request by request (comparison mode)
-        status = AERIAL_OK;
-        for (int k = 0; k < n && !status; k++)
-            status = aerial_pusch_eq_plain(&descs[k], 1, s->plainWs[i], s->plainWsBytes, st);
-    } else {
-        aerial_tuning t{s->cfg.precision, 0, 0, 0};
-        status = aerial_pusch_eq_fused(descs, n, &t, st);
-    }
-    b.busy = true;
-    s->batchesLaunched++;
-    s->slotsLaunched += n;
-    if (status) {
-        s->launchError = status;
-        finish_batch(s, b, status);
-        return true;
-    }
-    cudaEventRecord(b.ev, st);
-    return true;
 }
 
+// Batching window: launch fewer than min_batch pending slots only once the
+// oldest has waited batch_window_us; lock held.
+static bool batch_ready(aerial_server* s) {
+    if (s->cfg.min_batch <= 1 || s->cfg.batch_window_us <= 0.f) return true;
+    if ((int)s->pending.size() >= s->cfg.min_batch) return true;
+    return now_ns() - s->pending.front()->arrival >= (int64_t)(s->cfg.batch_window_us * 1000.0);
+}
+
+// Launch a formed batch on stream i; no lock held.  Returns the status.
+static int launch_formed(aerial_server* s, int i, const Formed& f) {
+    cudaStream_t st = s->streams[i];
+    int status = AERIAL_OK;
+    if (f.srs) {
+        status = aerial_srs_to_channel(f.H, f.S, f.W, f.F, f.nAnt, f.nBlocks, f.K, f.P, f.foccLen, st);
+    } else if (s->cfg.mode == AERIAL_SERVER_PLAIN) {
+        // the plain FP32 chain, request by request (comparison mode)
+        for (int k = 0; k < f.n && !status; k++)
+            status = aerial_pusch_eq_plain(&f.descs[k], 1, s->plainWs[i], s->plainWsBytes, st);
+    } else {
+        aerial_tuning t{s->cfg.precision, 0, 0, 0};
+        status = aerial_pusch_eq_fused(f.descs, f.n, &t, st);
+    }
+    if (!status) {
+        cudaError_t e = cudaEventRecord(s->batches[i].ev, st);
+        if (e != cudaSuccess) status = (int)e;
+    }
+    return status;
+}
+
+// The dispatcher: CUDA calls (launches, event queries) happen outside the
+// lock, so submissions are never held up by a launch in progress.
 static void dispatcher(aerial_server* s) {
     cudaSetDevice(s->device);
-    std::unique_lock<std::mutex> lk(s->mu);
-    while (!s->stop) {
+    Formed f;
+    std::unique_lock<std::mutex> lk(s->mu, std::defer_lock);
+    while (true) {
         bool progress = false;
-        // completions
+        // completions (the busy flags and events are the dispatcher's own)
         for (SrvBatch& b : s->batches) {
             if (!b.busy) continue;
-            cudaError_t e = cudaEventQuery(b.ev);
-            if (e == cudaSuccess) {
-                finish_batch(s, b, AERIAL_OK);
-                progress = true;
-            } else if (e != cudaErrorNotReady) {
-                finish_batch(s, b, (int)e);
-                progress = true;
-            }
+            const cudaError_t e = cudaEventQuery(b.ev);
+            if (e == cudaErrorNotReady) continue;
+            lk.lock();
+            finish_batch(s, b, e == cudaSuccess ? AERIAL_OK : (int)e);
+            s->inflightBatches--;
+            lk.unlock();
+            s->doneCv.notify_all();
+            progress = true;
         }
-        if (progress) s->doneCv.notify_all();
         // launches
-        if (!s->paused) {
-            for (size_t i = 0; i < s->batches.size(); i++)
-                if (!s->batches[i].busy && !s->pending.empty()) progress |= launch_batch(s, (int)i);
+        for (size_t i = 0; i < s->batches.size(); i++) {
+            SrvBatch& b = s->batches[i];
+            if (b.busy) continue;
+            lk.lock();
+            if (s->stop) {
+                lk.unlock();
+                return;
+            }
+            f.n = 0;
+            f.srs = false;
+            if (!s->paused && !s->pending.empty() && batch_ready(s)) form_batch(s, (int)i, f);
+            const bool formed = f.n > 0 || f.srs;
+            if (formed) {
+                b.busy = true;
+                s->inflightBatches++;
+                if (!f.srs) {
+                    s->batchesLaunched++;
+                    s->slotsLaunched += f.n;
+                }
+            }
+            lk.unlock();
+            if (!formed) continue;
+            progress = true;
+            const int status = launch_formed(s, (int)i, f);
+            if (status) {
+                lk.lock();
+                s->launchError = status;
+                finish_batch(s, b, status);
+                s->inflightBatches--;
+                lk.unlock();
+                s->doneCv.notify_all();
+            }
         }
         bool anyBusy = false;
         for (SrvBatch& b : s->batches) anyBusy |= b.busy;
-        if (anyBusy) {
-            // poll the in-flight events without sleeping: completion times are
-            // taken when the event is seen, so the loop stays tight
+        lk.lock();
+        if (s->stop) {
             lk.unlock();
-            std::this_thread::yield();
-            lk.lock();
-        } else if (!progress) {
-            s->cv.wait_for(lk, std::chrono::milliseconds(2));
+            return;
         }
+        const bool waiting = !s->pending.empty() && !s->paused;   // e.g. inside a batching window
+        if (!anyBusy && !progress && !waiting) s->cv.wait_for(lk, std::chrono::milliseconds(2));
+        lk.unlock();
+        if (anyBusy || waiting) std::this_thread::yield();
     }
 }
 
@@ -233,6 +300,8 @@ extern "C" int aerial_server_create(const aerial_server_config* cfg, aerial_serv
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return AERIAL_ERR_NO_DEVICE;
+    const int prep = aerial_prepare();
+    if (prep != AERIAL_OK) return prep;
     aerial_server* s = new aerial_server();
     s->cfg = *cfg;
     s->device = dev;
@@ -433,12 +502,7 @@ extern "C" int aerial_server_drain(aerial_server* s, int timeout_ms) {
     if (!s) return AERIAL_ERR_INVALID_ARG;
     std::unique_lock<std::mutex> lk(s->mu);
     const auto limit = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms);
-    auto busy = [&] {
-        if (!s->pending.empty()) return true;
-        for (SrvBatch& b : s->batches)
-            if (b.busy) return true;
-        return false;
-    };
+    auto busy = [&] { return !s->pending.empty() || s->inflightBatches > 0; };
     while (busy()) {
         if (s->doneCv.wait_until(lk, limit) == std::cv_status::timeout && busy()) return AERIAL_ERR_TIMEOUT;
     }
@@ -474,6 +538,14 @@ extern "C" int aerial_server_stats(aerial_server* s, aerial_server_statistics* o
         double sum = 0;
         for (int64_t v : l) sum += v;
         st.mean_us = (float)(sum / l.size() * 1e-3);
+        auto p99 = [](std::vector<int64_t> v) {
+            std::sort(v.begin(), v.end());
+            size_t i = (size_t)std::ceil(0.99 * v.size());
+            if (i < 1) i = 1;
+            return (float)(v[std::min(v.size(), i) - 1] * 1e-3);
+        };
+        st.queue_p99_us = p99(s->qlat);
+        st.service_p99_us = p99(s->slat);
     }
     st.deadline_misses = s->misses;
     st.res_done = s->resDone;
@@ -485,5 +557,16 @@ extern "C" int aerial_server_stats(aerial_server* s, aerial_server_statistics* o
     st.budget_used_bytes = s->used;
     st.pending = (long)s->pending.size();
     *out = st;
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_reset_stats(aerial_server* s) {
+    if (!s) return AERIAL_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->lat.clear();
+    s->qlat.clear();
+    s->slat.clear();
+    s->firstArrival = s->lastDone = 0;
+    s->resDone = s->batchesLaunched = s->slotsLaunched = s->srsDone = s->misses = 0;
     return AERIAL_OK;
 }

@@ -22,6 +22,7 @@ the same workload.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import importlib
 import json
 import os
@@ -39,6 +40,18 @@ UNIT = "REs/s"
 WORKLOAD = ("PUSCH equalization, 132 PRB = 1584 subcarriers x 64 Rx antennas x 8 layers x 11 data symbols, "
             "256-QAM, SNR 25 dB, per-PRB CN(0,1/64) channel + per-subcarrier perturbation; "
             "Gram -> FP32 Cholesky MMSE -> apply -> max-log LLR (float32)")
+WORKLOADS = {
+    1: ("plain-chain cell: 24 PRB = 288 subcarriers x 32 Rx antennas x 4 layers x 11 data symbols, 16-QAM, "
+        "SNR 20 dB, i.i.d. CN(0,1/32) channel"),
+    2: WORKLOAD,
+    3: ("precision stress: 273 PRB = 3276 subcarriers x 128 Rx antennas x 16 layers x 11 data symbols, 256-QAM, "
+        "SNR 30 dB, exponentially correlated (rho = 0.7) receive antennas"),
+    4: ("uneven 16-cell batch in one persistent launch: PRB in {24,51,106,132,273}, antennas in {16,32,64}, "
+        "layers in {2,4,8}, QPSK..256-QAM, SNR U(10,30) dB, from a seed"),
+}
+DEFAULT_SLOTS = {1: 960, 2: 64, 3: 12, 4: 16}
+DEFAULT_PRECISION = {1: "fp16", 2: "fp16", 3: "bf16x3", 4: "fp16", 5: "fp16"}
+L2_BYTES = 126 * 1024 * 1024
 
 
 def parse():
@@ -47,8 +60,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--slots", type=int, default=64, help="cell-slots per step (per GPU)")
-    ap.add_argument("--precision", default="fp16", choices=["fp16", "bf16", "bf16x3"])
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
+                    help="benchmark configuration (2 = the headline 100 MHz cell)")
+    ap.add_argument("--slots", type=int, default=0, help="cell-slots per step per GPU (0 = the config's default)")
+    ap.add_argument("--precision", default="", choices=["", "fp16", "bf16", "bf16x3"])
+    ap.add_argument("--duration", type=float, default=1.0, help="serving run length in seconds (config 5)")
+    ap.add_argument("--window-us", type=float, default=0.0, help="serving batching window (config 5; 0 = launch at once)")
+    ap.add_argument("--min-batch", type=int, default=0, help="serving minimum batch before the window ends")
     ap.add_argument("--soak", type=float, default=1.5, help="seconds of untimed load before timing (clock steady state)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -126,6 +144,31 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def host_cell(wl, cfg: int):
+    """One host-resident slot of a configuration for the CPU baseline."""
+    if cfg in (1, 2, 3):
+        return wl.config_cell(cfg, seed=42)
+    return wl.multicell(16, seed=42)[0]
+
+
+def build_cells(wl, cfg: int, slots: int, rank: int, dev):
+    """The step's cell-slots.  Slots of one configuration share sigma2, so for
+    the small configuration 1 consecutive slots are laid out contiguously and
+    described as one cell of slots x 24 PRBs (at most 64 descriptors a launch)."""
+    if cfg == 2:
+        return [wl.config_cell(2, seed=1000 * rank + 17 * i + 1, device=dev) for i in range(slots)]
+    if cfg == 3:
+        return [wl.config_cell(3, seed=1000 * rank + 17 * i + 1, device=dev) for i in range(slots)]
+    if cfg == 1:
+        per = -(-slots // 64)
+        n = -(-slots // per)
+        return [wl.make_cell(24 * per, 32, 4, 11, 16, 20.0, "iid", seed=1000 * rank + 17 * i + 1, device=dev)
+                for i in range(n)]
+    if cfg == 4:
+        return wl.multicell(slots, seed=42 + 1000 * rank, device=dev)
+    raise ValueError(cfg)
+
+
 def max_over_ranks(values, world: int, device=None):
     """Element-wise max of per-rank timings (ms) across the process group.
 
@@ -173,7 +216,7 @@ def run_reference(a, rank):
     wl = importlib.import_module("aerial-mimo-tc-optimization_b200.workload")
     cores = os.cpu_count() or 1
     orc.set_threads(cores)
-    cell = wl.config_cell(2, seed=42)
+    cell = host_cell(wl, a.config if a.config in (1, 2, 3, 4) else 2)
     H, Y = cell.H.numpy(), cell.Y.numpy()
     # calibrate one slot, then size each step so the whole run stays within ~2 minutes
     t0 = time.perf_counter()
@@ -191,12 +234,12 @@ def run_reference(a, rank):
         orc.chain_f32(Hs, Ys, *args)
     el = time.perf_counter() - t0
     v = a.steps * nsc * cell.nSym / el
-    sample = f"{nprb} of 132 PRB ({nsc} subcarriers) of one slot per step, OpenMP over subcarriers"
+    sample = f"{nprb} of {cell.nPRB} PRB ({nsc} subcarriers) of one slot per step, OpenMP over subcarriers"
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * el / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "sample": sample},
+        "config": {"workload": WORKLOADS.get(a.config, WORKLOAD), "benchmark_config": a.config, "sample": sample},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "notes": "scalar FP32 chain of the reference (gram_scalar, Cholesky solve, coef_apply_v1_scalar, "
@@ -211,6 +254,10 @@ def run_reference(a, rank):
 
 def main():
     a = parse()
+    if not a.precision:
+        a.precision = DEFAULT_PRECISION[a.config]
+    if not a.slots:
+        a.slots = DEFAULT_SLOTS.get(a.config, 64)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -234,8 +281,11 @@ def main():
         if world > 1:
             dist.barrier()
 
+    if a.config == 5:
+        run_serving(a, aeq, wl, dev)
+        return
     S = a.slots
-    cells = [wl.config_cell(2, seed=1000 * rank + 17 * i + 1, device=dev) for i in range(S)]
+    cells = build_cells(wl, a.config, S, rank, dev)
     llrs = [torch.empty(c.llr_numel, dtype=torch.float32, device=dev) for c in cells]
     descs = [aeq.cell_desc(c.H, c.Y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
              for c, l in zip(cells, llrs)]
@@ -251,6 +301,10 @@ def main():
     def step():
         aeq.pusch_eq_fused(descs, tun, stream)
 
+    flush = None
+    if bytes_per_step < 2 * L2_BYTES:
+        # the step fits (or nearly fits) in L2: flush it before every timed launch
+        flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     for _ in range(a.warmup):
         step()
     torch.cuda.synchronize()
@@ -270,6 +324,8 @@ def main():
     torch.cuda.nvtx.range_push("timed")          # ncu --nvtx --nvtx-include "timed/" lists these launches
     e0.record(stream)
     for i in range(a.steps):
+        if flush is not None:
+            flush.fill_(float(i))
         ev[i][0].record(stream)
         step()
         ev[i][1].record(stream)
@@ -278,8 +334,9 @@ def main():
     torch.cuda.nvtx.range_pop()
     barrier()
     clocks = sampler.stop()
-    elapsed_ms = e0.elapsed_time(e1)
     launch_ms = [s.elapsed_time(e) for s, e in ev]
+    # with L2 flushes between launches only the launches are timed
+    elapsed_ms = e0.elapsed_time(e1) if flush is None else sum(launch_ms)
     elapsed_ms, launch_avg_ms = max_over_ranks([elapsed_ms, statistics.mean(launch_ms)], world, dev)
     value = whole_job_rate(res_per_step, a.steps, world, elapsed_ms)
     peak, peak_kind = measured_peaks()
@@ -302,11 +359,11 @@ def main():
               for c, h, y, l in zip(cells, dH, dY, dL)]
 
         def e2e_step():
-            for i in range(S):
+            for i in range(len(cells)):
                 dH[i].copy_(hH[i], non_blocking=True)
                 dY[i].copy_(hY[i], non_blocking=True)
             aeq.pusch_eq_fused(d2, tun, stream)
-            for i in range(S):
+            for i in range(len(cells)):
                 hL[i].copy_(dL[i], non_blocking=True)
 
         k2 = max(3, min(a.steps, 20))
@@ -331,15 +388,17 @@ def main():
     cpu_base = None
     if rank == 0 and world == 1 and not a.no_extras:
         extras = bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a)
+        if a.config == 4:
+            extras["tiles"] = compare_tiles(aeq, descs, tun, stream, a, flush)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         from oracle import oracle as orc
 
         cores = os.cpu_count() or 1
         orc.set_threads(cores)
-        hc = wl.config_cell(2, seed=42)
+        hc = host_cell(wl, a.config)
         v, runs, el = cpu_chain_rate(orc, hc, a.cpu_seconds)
         cpu_base = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                    "sample": f"{runs} full slot(s) (1584 subcarriers) in {el:.1f} s, OpenMP over subcarriers"}
+                    "sample": f"{runs} full slot(s) ({hc.nSC} subcarriers) in {el:.1f} s, OpenMP over subcarriers"}
 
     if world > 1:
         dist.barrier()
@@ -350,8 +409,11 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": a.precision + " operands / fp32 accumulate and solve", "data": "synthetic (seeded, generated on device)",
-        "config": {"workload": WORKLOAD, "slots_per_step_per_gpu": S, "res_per_step_per_gpu": res_per_step,
-                   "l2": f"inputs larger than L2 ({bytes_per_step / 1e6:.0f} MB touched per step per GPU)",
+        "config": {"workload": WORKLOADS[a.config], "benchmark_config": a.config, "cells_per_step": len(cells),
+                   "slots_per_step_per_gpu": S, "res_per_step_per_gpu": res_per_step,
+                   "l2": (f"inputs larger than L2 ({bytes_per_step / 1e6:.0f} MB touched per step per GPU)"
+                          if flush is None else
+                          f"L2 flushed before each timed launch ({bytes_per_step / 1e6:.0f} MB per step)"),
                    "precision": a.precision, "tuning": {"warps_per_cta": tun.warps_per_cta,
                                                          "ctas_per_sm": tun.ctas_per_sm},
                    "parallelism": f"independent cell-slots per GPU x{world}"},
@@ -363,6 +425,125 @@ def main():
     }
     line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+def run_serving(a, aeq, wl, dev):
+    """Configuration 5: 40 cells submit slots as Poisson arrivals (mean one
+    slot per 500 us per cell) to the serving loop; every 20th slot of a cell
+    is preceded by an SRS channel update (filter multiply, K = 12, one port per
+    layer).  The same arrival trace is served by the fused batched loop and by
+    the plain FP32 chain run request by request."""
+    import numpy as np
+    import torch
+
+    n_cells, per_slot_s, srs_every = 40, 500e-6, 20
+    shapes = wl.multicell_shapes(n_cells, seed=5)
+    cells, Ys, rings, srs_ops = [], [], [], []
+    for i, (p, A, L, q, snr) in enumerate(shapes):
+        c = wl.make_cell(p, A, L, 11, q, snr, "iid", seed=5000 + i, device=dev)
+        extra = wl.make_cell(p, A, L, 11, q, snr, "iid", seed=7000 + i, device=dev)
+        cells.append(c)
+        Ys.append([c.Y, extra.Y])
+        rings.append([torch.empty(c.llr_numel, dtype=torch.float32, device=dev) for _ in range(16)])
+        g = torch.Generator(device=dev)
+        g.manual_seed(9000 + i)
+        nblk = c.nSC // 12
+        srs_ops.append([(torch.randn(n, generator=g, device=dev) * 0.5).half().view(torch.int16).contiguous()
+                        for n in (2 * nblk * A * 12, 2 * 12 * 12, 2 * L * 12)])
+    rng = np.random.default_rng(11)
+    arrivals = []
+    for ci in range(n_cells):
+        t = rng.exponential(per_slot_s)
+        while t < a.duration:
+            arrivals.append((t, ci))
+            t += rng.exponential(per_slot_s)
+    arrivals.sort()
+    lib = aeq.lib()
+
+    def serve(mode, window_us, min_batch):
+        srv = aeq.Server(memory_budget_bytes=16 << 30, streams=3, max_batch=64, precision=a.precision,
+                         mode=mode, deadline_us=500.0, batch_window_us=window_us, min_batch=min_batch)
+        ids = []
+        for c in cells:
+            k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
+            srv.set_channel(k, c.H, c.sigma2)
+            ids.append(k)
+        # one untimed slot per cell (first launch of every shape), then reset the statistics by
+        # draining and polling before the trace starts
+        for ci, k in enumerate(ids):
+            srv.submit(k, Ys[ci][0], rings[ci][0])
+        srv.drain(60000)
+        srv.poll(max_out=4096)
+        srv.reset_stats()
+        yp = [[ctypes.c_void_p(y.data_ptr()) for y in ys] for ys in Ys]
+        rp = [[ctypes.c_void_p(r.data_ptr()) for r in ring] for ring in rings]
+        sp = [[ctypes.c_void_p(t.data_ptr()) for t in ops] for ops in srs_ops]
+        count = [0] * n_cells
+        handle = srv._h
+        torch.cuda.synchronize()
+        t0 = time.monotonic_ns() + 20_000_000
+        errors = 0
+        lag = []
+        for t, ci in arrivals:
+            target = t0 + int(t * 1e9)
+            now = time.monotonic_ns()
+            while now < target:
+                now = time.monotonic_ns()
+            lag.append(now - target)
+            k = count[ci]
+            count[ci] += 1
+            if k and k % srs_every == 0:
+                errors += lib.aerial_server_srs_update(handle, ids[ci], sp[ci][0], sp[ci][1], sp[ci][2], 12, 12,
+                                                       None) != 0
+            errors += lib.aerial_server_submit(handle, ids[ci], yp[ci][k % 2], rp[ci][k % 16], target, None) != 0
+        srv.drain(600000)
+        st = srv.stats()
+        srv.close()
+        st["submit_errors"] = int(errors)
+        lag.sort()
+        st["client_submit_lag_p99_us"] = lag[int(0.99 * (len(lag) - 1))] * 1e-3 if lag else 0.0
+        st["miss_rate"] = st["deadline_misses"] / max(1, st["slots_done"])
+        return st
+
+    fused = serve(aeq.SERVER_FUSED, a.window_us, a.min_batch)
+    plain = serve(aeq.SERVER_PLAIN, 0.0, 0)
+    keep = ("slots_done", "p50_us", "p99_us", "max_us", "mean_us", "queue_p99_us", "service_p99_us",
+            "deadline_misses", "miss_rate", "res_per_s", "batches", "mean_batch", "srs_updates", "submit_errors",
+            "client_submit_lag_p99_us")
+    line = {
+        "metric": "serving: equalized REs/s with p99 slot latency (deadline 500 us)", "value": fused["res_per_s"],
+        "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "benchmark_config": 5,
+        "config": {"workload": (f"{n_cells} cells, Poisson slot arrivals (mean one per 500 us per cell) for "
+                                f"{a.duration:.1f} s, shapes drawn as the 16-cell batch, SRS update every "
+                                f"{srs_every} slots, 16 GB admission budget, 3 streams, up to 64 slots a launch"),
+                   "slots_offered": len(arrivals), "precision": a.precision},
+        "fused_batched": dict({k: fused[k] for k in keep}, batch_window_us=a.window_us, min_batch=a.min_batch),
+        "plain_fp32_per_request": {k: plain[k] for k in keep},
+        "p99_ratio_plain_over_fused": plain["p99_us"] / max(fused["p99_us"], 1e-9),
+        "data": "synthetic (seeded, generated on device)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def compare_tiles(aeq, descs, tuned, stream, a, flush):
+    """Configuration 4: autotuned launch shape against the fixed default shape."""
+    import torch
+
+    def timed(t, k=20):
+        e = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        for i in range(k):
+            if flush is not None:
+                flush.fill_(float(i))
+            e[i][0].record(stream)
+            aeq.pusch_eq_fused(descs, t, stream)
+            e[i][1].record(stream)
+        torch.cuda.synchronize()
+        ms = sorted(x.elapsed_time(y) for x, y in e)
+        return 1e3 * ms[len(ms) // 2]
+
+    fixed = aeq.make_tuning(a.precision)
+    return {"autotuned_us": timed(tuned), "fixed_default_us": timed(fixed),
+            "autotuned_shape": {"warps_per_cta": tuned.warps_per_cta, "ctas_per_sm": tuned.ctas_per_sm}}
 
 
 def bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a):
@@ -398,7 +579,7 @@ def bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a):
             lat.append(s0.elapsed_time(s1) * 1e3)
     lat.sort()
     out["single_slot_latency_us"] = {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-                                     "note": "one 1584-SC cell per launch, L2 flushed before each"}
+                                     "note": f"one {cells[0].nSC}-SC cell per launch, L2 flushed before each"}
     # accuracy of slot 0 vs the FP64 model
     try:
         from oracle import oracle as orc

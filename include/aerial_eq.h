@@ -72,6 +72,12 @@ enum {
 const char* aerial_error_string(int status);
 int aerial_version(void);
 
+/* Load every kernel of the library on the current device and set its launch
+ * attributes.  Optional: without it the first launch of each kernel variant
+ * pays the driver's lazy module loading (milliseconds), which a latency-
+ * critical slot loop should do before it starts.  aerial_server_create calls it. */
+int aerial_prepare(void);
+
 /* ------------------------------------------------------------------------ */
 /* Per-stage entry points (the plain FP32 chain; bit-exact restatements of   */
 /* the reference's scalar kernels where the reference has the stage).        */
@@ -236,6 +242,9 @@ typedef struct {
     int queue_capacity;           /* pending requests accepted (0 = unbounded) */
     int start_paused;             /* 1: queue without dispatching until aerial_server_pause(s, 0) */
     float deadline_us;            /* slot deadline counted by the statistics */
+    float batch_window_us;        /* launch a batch smaller than min_batch only once its oldest
+                                     slot has waited this long (0 = launch at once) */
+    int min_batch;                /* see batch_window_us (0 or 1 = no minimum) */
 } aerial_server_config;
 
 typedef struct {
@@ -248,6 +257,8 @@ typedef struct {
 typedef struct {
     long slots_done;
     float p50_us, p99_us, max_us, mean_us;   /* slot latency: completion - arrival */
+    float queue_p99_us;           /* arrival -> launch */
+    float service_p99_us;         /* launch -> completion observed */
     long deadline_misses;
     long res_done;                /* equalized REs (subcarrier x symbol) */
     double span_s;                /* first arrival -> last completion */
@@ -280,6 +291,8 @@ int aerial_server_wait(aerial_server* server, uint64_t requestId, int timeout_ms
 int aerial_server_drain(aerial_server* server, int timeout_ms);
 int aerial_server_pause(aerial_server* server, int paused);
 int aerial_server_stats(aerial_server* server, aerial_server_statistics* out);
+/* Forget the latency samples and counters gathered so far (e.g. after warm-up). */
+int aerial_server_reset_stats(aerial_server* server);
 
 /* ------------------------------------------------------------------------ */
 /* Autotuner                                                                  */

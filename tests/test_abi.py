@@ -66,9 +66,9 @@ def test_server_rejects_bad_config_without_gpu():
     lib = pkg.lib()
     h = ctypes.c_void_p()
     assert lib.aerial_server_create(None, ctypes.byref(h)) == 1001
-    cfg = pkg.ServerConfig(0, 2, 64, 0, 0, 0, 0, 500.0)          # zero budget
+    cfg = pkg.ServerConfig(0, 2, 64, 0, 0, 0, 0, 500.0, 0.0, 0)   # zero budget
     assert lib.aerial_server_create(ctypes.byref(cfg), ctypes.byref(h)) == 1001
-    cfg = pkg.ServerConfig(1 << 30, 0, 64, 0, 0, 0, 0, 500.0)    # no stream
+    cfg = pkg.ServerConfig(1 << 30, 0, 64, 0, 0, 0, 0, 500.0, 0.0, 0)   # no stream
     assert lib.aerial_server_create(ctypes.byref(cfg), ctypes.byref(h)) == 1001
     assert lib.aerial_server_destroy(None) == 1001
     n = ctypes.c_int()
