@@ -174,7 +174,10 @@ __device__ __forceinline__ CellView view_of(const FusedCell& c) {
 // 16 received rows Y[s][a0..a0+15] of 128 bytes whose 16-byte pieces are
 // XOR-swizzled by (s & 1) * 4 (conflict-free 16-byte fragment reads).
 // ---------------------------------------------------------------------------
-constexpr int NST = 3;          // stages per warp
+#ifndef AEQ_FUSED_STAGES
+#define AEQ_FUSED_STAGES 3
+#endif
+constexpr int NST = AEQ_FUSED_STAGES;   // stages per warp
 constexpr int CHUNK = 16;       // antennas per stage (two k-steps)
 
 __host__ __device__ constexpr int hrs_of(int L) {
@@ -207,7 +210,11 @@ __device__ __forceinline__ float4 lds128(uint32_t a) {
 // Gram blocks kept: (0,0) for LT <= 8; (0,0), (1,0), (1,1) for LT = 16.
 // Fragment reads of one staged chunk (two k-steps) and their MMAs.  Thread
 // (g, c) of k-step kk owns the antenna pair 8kk + 2c, +1 of the chunk.
-template <int LT, int P, bool LEXACT>
+//
+// FULL: all 16 antennas of the chunk exist, so no antenna mask is applied.
+// Rows of symbols past nSym are never masked: each received row only feeds
+// its own Z column, and columns past nSym are never read.
+template <int LT, int P, bool LEXACT, bool FULL>
 __device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L, int nSym, float (*gacc)[4],
                                           float (*zacc)[2][4], bool z2, int g, int c) {
     constexpr int NMT = LT > 8 ? 2 : 1;
@@ -215,8 +222,8 @@ __device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L
 #pragma unroll
     for (int kk = 0; kk < 2; kk++) {
         const int a0 = 8 * kk + 2 * c;
-        if (8 * kk >= nRows) break;                      // uniform: tail chunk of 8 antennas
-        const bool v0 = a0 < nRows, v1 = a0 + 1 < nRows;
+        if (!FULL && 8 * kk >= nRows) break;             // uniform: tail chunk of 8 antennas
+        const bool v0 = FULL || a0 < nRows, v1 = FULL || a0 + 1 < nRows;
         float4 hv[NMT];
 #pragma unroll
         for (int mt = 0; mt < NMT; mt++) {
@@ -232,11 +239,9 @@ __device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L
 #pragma unroll
         for (int nt = 0; nt < 2; nt++) {
             const int s = 8 * nt + g;
-            const bool sv = s < nSym;
-            const int sa = sv ? s : 0;                   // rows past nSym are not staged: read row 0, discard
+            const int sa = s < nSym ? s : 0;             // rows past nSym are not staged: read row 0 instead
             const float4 y = lds128(ys + sa * 128 + (((a0 >> 1) ^ ((sa & 1) << 2)) << 4));
-            yv[nt] = make_float4((sv && v0) ? y.x : 0.f, (sv && v0) ? y.y : 0.f, (sv && v1) ? y.z : 0.f,
-                                 (sv && v1) ? y.w : 0.f);
+            yv[nt] = FULL ? y : make_float4(v0 ? y.x : 0.f, v0 ? y.y : 0.f, v1 ? y.z : 0.f, v1 ? y.w : 0.f);
         }
         if constexpr (P == AERIAL_PREC_BF16X3) {
             uint32_t ah[NMT][2], al[NMT][2];
@@ -618,6 +623,27 @@ __device__ __forceinline__ void stage_item_exact(const FusedCell& cl, const floa
     }
 }
 
+// A full 16-antenna chunk of a launch whose cells all have L == LF: the
+// channel rows are 16 * LF / 2 pieces of 16 bytes (lane e -> row e / (LF/2),
+// piece e % (LF/2)), the received rows 8 pieces each (lane -> row lane / 8 + 4k,
+// piece lane % 8).  hLaneS / yLaneS are the lane's stage offsets of its first
+// pieces, ys points at the lane's first received piece, yStep = 4 rows, and
+// nYk is the lane's count of received rows below nSym.
+template <int LF>
+__device__ __forceinline__ void stage_full(uint32_t st, uint32_t hLaneS, uint32_t yLaneS, const float2* hsrc,
+                                           const float2* ys, int yStep, int nYk, int lane) {
+    constexpr int HRS = hrs_of(LF);
+    constexpr int HALF = LF / 2;
+    constexpr int NP = CHUNK * HALF;                    // channel pieces per chunk
+    constexpr int RPK = 32 / HALF;                      // channel rows per 32 pieces
+#pragma unroll
+    for (int k = 0; k < (NP + 31) / 32; k++)
+        if (NP >= 32 * (k + 1) || lane < NP - 32 * k) cp_async16(st + hLaneS + k * RPK * HRS, hsrc + 2 * lane + 64 * k);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (k < nYk) cp_async16(st + yLaneS + 512 * k, ys + k * yStep);
+}
+
 __device__ __forceinline__ int group_valid(const FusedCell& cl, long grp) {
     return (int)min((long)cl.GS, (long)cl.nSC - (grp - cl.group0) * cl.GS);
 }
@@ -643,40 +669,61 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     if (gw >= total) return;
 
     // ---- producer cursor (registers): group, cell, subcarrier, chunk ----
+    // Per-lane staging offsets are fixed for the whole launch (exact tile) or
+    // for a cell (received-row pieces), so a full chunk costs a few adds and
+    // its cp.async instructions.
+    uint32_t hLaneS = 0, yLaneS = 0;
+    if constexpr (LTF != 0) {
+        constexpr int HALF = LTF / 2;
+        hLaneS = (lane / HALF) * hrs_of(LTF) + (lane % HALF) * 16;
+        yLaneS = CHUNK * hrs_of(LTF) + (lane >> 3) * 128 + (((lane & 7) ^ (((lane >> 3) & 1) << 2)) << 4);
+    }
     long pg = gw;
     int pci = 0;
     while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
-    int pq = 0, pch = 0, pValid = group_valid(p.cell[pci], pg), pslot = 0;
+    int pq = 0, pch = 0, pslot = 0, pValid, pNChunk, pNFull, pYStep, pYLane, pYk;
+    long pHsc, pYsc;
     const float2* phs;
     const float2* pys;
-    {
+    auto load_pcell = [&]() {
         const FusedCell& cl = p.cell[pci];
+        const int A = cl.A, nSym = cl.nSym;
+        pNChunk = cl.nChunk;
+        pNFull = A / CHUNK;
+        pHsc = (long)A * (LTF != 0 ? LTF : cl.L);
+        pYsc = (long)nSym * A;
+        pValid = group_valid(cl, pg);
         const long sc = (pg - cl.group0) * cl.GS;
-        phs = cl.H + sc * cl.A * cl.L;
-        pys = cl.Y + sc * cl.nSym * cl.A;
-    }
+        phs = cl.H + sc * pHsc;
+        pys = cl.Y + sc * pYsc;
+        pYStep = 4 * A;                                   // received rows s and s + 4
+        pYLane = (lane >> 3) * A + 2 * (lane & 7);        // this lane's first piece
+        pYk = min(4, max(0, (nSym - (lane >> 3) + 3) >> 2));
+    };
+    load_pcell();
     auto produce = [&]() {
         if (pg < total) {
-            const FusedCell& cl = p.cell[pci];
-            if constexpr (LTF != 0)
-                stage_item_exact<LTF>(cl, phs, pys, pch, stBase + pslot * p.stageBytes, lane);
-            else
-                stage_item(cl, phs, pys, pch, stBase + pslot * p.stageBytes, lane);
-            if (++pch == cl.nChunk) {
+            const uint32_t st = stBase + pslot * p.stageBytes;
+            if constexpr (LTF != 0) {
+                if (pch < pNFull)
+                    stage_full<LTF>(st, hLaneS, yLaneS, phs + CHUNK * pch * LTF, pys + CHUNK * pch + pYLane, pYStep,
+                                    pYk, lane);
+                else
+                    stage_item_exact<LTF>(p.cell[pci], phs, pys, pch, st, lane);
+            } else {
+                stage_item(p.cell[pci], phs, pys, pch, st, lane);
+            }
+            if (++pch == pNChunk) {
                 pch = 0;
                 if (++pq < pValid) {
-                    phs += (long)cl.A * cl.L;
-                    pys += (long)cl.nSym * cl.A;
+                    phs += pHsc;
+                    pys += pYsc;
                 } else {
                     pq = 0;
                     pg += nw;
                     if (pg < total) {
                         while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
-                        const FusedCell& cn = p.cell[pci];
-                        pValid = group_valid(cn, pg);
-                        const long sc = (pg - cn.group0) * cn.GS;
-                        phs = cn.H + sc * cn.A * cn.L;
-                        pys = cn.Y + sc * cn.nSym * cn.A;
+                        load_pcell();
                     }
                 }
             }
@@ -687,11 +734,25 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
 #pragma unroll
     for (int k = 0; k < NST - 1; k++) produce();
 
-    // ---- consumer ----
+    // ---- consumer: cell constants in registers, reloaded per group ----
     long grp = gw;
     int ci = 0;
     while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
-    int q = 0, ch = 0, nValid = group_valid(p.cell[ci], grp), cslot = 0;
+    int q = 0, ch = 0, cslot = 0, nValid, cNChunk, cNFull, cA, cNSym, cL, cLT, cHrs;
+    bool z2;
+    auto load_ccell = [&]() {
+        const FusedCell& cl = p.cell[ci];
+        nValid = group_valid(cl, grp);
+        cA = cl.A;
+        cNSym = cl.nSym;
+        cNChunk = cl.nChunk;
+        cNFull = cl.A / CHUNK;
+        cL = cl.L;
+        cLT = LTF != 0 ? LTF : cl.LT;
+        cHrs = cl.hrs;
+        z2 = cl.nSym > 8;
+    };
+    load_ccell();
     float gacc[3][4], zacc[2][2][4];
 #pragma unroll
     for (int b = 0; b < 3; b++)
@@ -709,29 +770,29 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
         produce();
         cp_async_wait<NST - 1>();                  // this item's copies (own lane) have landed
         __syncwarp();                              // ... and every lane's
-        const FusedCell& cl = p.cell[ci];
-        const int LT = LTF != 0 ? LTF : cl.LT;
         const uint32_t st = stBase + cslot * p.stageBytes;
         cslot = cslot == NST - 1 ? 0 : cslot + 1;
-        const int nRows = min(CHUNK, cl.A - CHUNK * ch);
-        const bool z2 = cl.nSym > 8;
         if constexpr (LTF != 0) {
-            mma_stage<LTF, P, true>(st, hrs_of(LTF), nRows, LTF, cl.nSym, gacc, zacc, z2, g, c);
+            if (ch < cNFull)
+                mma_stage<LTF, P, true, true>(st, hrs_of(LTF), CHUNK, LTF, cNSym, gacc, zacc, z2, g, c);
+            else
+                mma_stage<LTF, P, true, false>(st, hrs_of(LTF), cA - CHUNK * ch, LTF, cNSym, gacc, zacc, z2, g, c);
         } else {
-            switch (LT) {
-                case 1: mma_stage<1, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
-                case 2: mma_stage<2, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
-                case 4: mma_stage<4, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
-                case 8: mma_stage<8, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
-                default: mma_stage<16, P, false>(st, cl.hrs, nRows, cl.L, cl.nSym, gacc, zacc, z2, g, c); break;
+            const int nRows = min(CHUNK, cA - CHUNK * ch);
+            switch (cLT) {
+                case 1: mma_stage<1, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
+                case 2: mma_stage<2, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
+                case 4: mma_stage<4, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
+                case 8: mma_stage<8, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
+                default: mma_stage<16, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
             }
         }
-        if (++ch < cl.nChunk) continue;
+        if (++ch < cNChunk) continue;
         ch = 0;
         if constexpr (LTF != 0) {
             store_acc<LTF>(sm, gacc, zacc, q, g, c);
         } else {
-            switch (LT) {
+            switch (cLT) {
                 case 1: store_acc<1>(sm, gacc, zacc, q, g, c); break;
                 case 2: store_acc<2>(sm, gacc, zacc, q, g, c); break;
                 case 4: store_acc<4>(sm, gacc, zacc, q, g, c); break;
@@ -751,24 +812,27 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
                 for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
         if (++q < nValid) continue;
         __syncwarp();
-        const CellView v = view_of(cl);
-        const long sc0 = (grp - cl.group0) * cl.GS;
-        if constexpr (LTF != 0) {
-            solve_group<LTF, P>(v, sc0, nValid, smemOff, lane);
-        } else {
-            switch (LT) {
-                case 1: solve_group<1, P>(v, sc0, nValid, smemOff, lane); break;
-                case 2: solve_group<2, P>(v, sc0, nValid, smemOff, lane); break;
-                case 4: solve_group<4, P>(v, sc0, nValid, smemOff, lane); break;
-                case 8: solve_group<8, P>(v, sc0, nValid, smemOff, lane); break;
-                default: solve_group<16, P>(v, sc0, nValid, smemOff, lane); break;
+        {
+            const FusedCell& cl = p.cell[ci];
+            const CellView v = view_of(cl);
+            const long sc0 = (grp - cl.group0) * cl.GS;
+            if constexpr (LTF != 0) {
+                solve_group<LTF, P>(v, sc0, nValid, smemOff, lane);
+            } else {
+                switch (cLT) {
+                    case 1: solve_group<1, P>(v, sc0, nValid, smemOff, lane); break;
+                    case 2: solve_group<2, P>(v, sc0, nValid, smemOff, lane); break;
+                    case 4: solve_group<4, P>(v, sc0, nValid, smemOff, lane); break;
+                    case 8: solve_group<8, P>(v, sc0, nValid, smemOff, lane); break;
+                    default: solve_group<16, P>(v, sc0, nValid, smemOff, lane); break;
+                }
             }
         }
         q = 0;
         grp += nw;
         if (grp >= total) break;
         while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
-        nValid = group_valid(p.cell[ci], grp);
+        load_ccell();
     }
     cp_async_wait<0>();
 }
