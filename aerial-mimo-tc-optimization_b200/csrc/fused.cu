@@ -345,14 +345,16 @@ __device__ __forceinline__ void write_llr(float* dst, const float* o) {
 }
 
 // Max-log PAM demapper of the fused epilogue: the formula of llr_v1_baseline
-// (src/llr/aerial_llr_v3.cu:90-107) with the last square fused into the
-// subtraction (fma(-t, t, pMD)), the +-65504 clamp applied to the magnitude
-// and the soft bit's sign copied in with one bit operation.  It differs from
-// the reference's rounding by at most one FP32 ulp of each LLR (the plain
-// chain keeps the bit-exact form).
+// (src/llr/aerial_llr_v3.cu:90-107) evaluated on a scaled axis.  With
+// r = sqrt(noiseInv), the soft estimate and the distances D_i scaled by r,
+//   (pm_i - t^2) * noiseInv = (r m_i)^2 - (r t)^2,
+// so each LLR is one fma(-t', t', m'^2) with no noise multiply.  The +-65504
+// clamp is applied to the magnitude and the soft bit's sign copied in with
+// one bit operation.  It differs from the reference's rounding by a few FP32
+// ulps of each LLR (the plain chain keeps the bit-exact form).
 template <int N>
-__device__ __forceinline__ void pam_llr_fast(float pI, float pQ, float noise, const PamLut& L, float* out) {
-    const float dist = L.d[N - 1];
+__device__ __forceinline__ void pam_llr_scaled(float pI, float pQ, const float* d, float* out) {
+    const float dist = d[N - 1];
 #pragma unroll
     for (int iq = 0; iq < 2; iq++) {
         float sb = iq ? pQ : pI;
@@ -363,52 +365,60 @@ __device__ __forceinline__ void pam_llr_fast(float pI, float pQ, float noise, co
             const float m = dist + a;
             pm[i] = m * m;
             sg[i] = sb;
-            if (i < N - 1) sb = L.d[i] - a;
+            if (i < N - 1) sb = d[i] - a;
         }
         const float t = fabsf(sb) - dist;
 #pragma unroll
         for (int i = 0; i < N; i++) {
-            const float v = fminf(fmaf(-t, t, pm[i]) * noise, 65504.f);
+            const float v = fminf(fmaf(-t, t, pm[i]), 65504.f);
             out[2 * i + iq] = __int_as_float(__float_as_int(v) ^ (__float_as_int(sg[i]) & 0x80000000));
         }
     }
 }
 
+// Symbol s of layer row i: Y_eq = x / mu (optional output), LLRs of x * r / mu.
 template <int N>
-__device__ __forceinline__ void emit1(const CellView& cl, float* base, float2* ye, int s, float2 x, float invMu,
-                                      float nInv) {
-    const float2 v = make_float2(x.x * invMu, x.y * invMu);
-    if (ye) __stcs(ye + s, v);
+__device__ __forceinline__ void emit1(float* base, float2* ye, int s, float2 x, float invMu, float scl,
+                                      const float* d) {
+    if (ye) __stcs(ye + s, make_float2(x.x * invMu, x.y * invMu));
     float o[2 * N];
-    pam_llr_fast<N>(v.x, v.y, nInv, cl.lut, o);
+    pam_llr_scaled<N>(x.x * scl, x.y * scl, d, o);
     write_llr<N>(base + s * 2 * N, o);
 }
 
-// X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs, then unbias and demap.
+// X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs (FP32 fma chains), then
+// unbias and demap.  Lanes without an output row return at once.
 template <int LT, int N>
 __device__ __forceinline__ void solve_emit(const CellView& cl, const float2* sZ, const float2* gi, long sc, int i,
                                            bool out, float invMu, float nInv) {
     using W = WarpSmem<LT>;
+    if (!out) return;
     float* base = cl.llr + ((sc * cl.L + i) * (long)cl.nSym) * (2 * N);
     float2* ye = cl.yeq ? cl.yeq + (sc * cl.L + i) * (long)cl.nSym : nullptr;
+    const float r = sqrtf(nInv);
+    const float scl = invMu * r;
+    float d[N];
 #pragma unroll
-    for (int s = 0; s < 16; s += 2) {
-        if (s < cl.nSym) {
-            float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
+    for (int k = 0; k < N; k++) d[k] = cl.lut.d[k] * r;
+    const int nSym = cl.nSym;
+#pragma unroll 1
+    for (int s = 0; s < nSym; s += 2) {
+        float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int m = 0; m < LT; m++) {
-                const float2 a = gi[m];
-                const float4 z = *reinterpret_cast<const float4*>(sZ + m * W::ZS + s);
-                x0.x += a.x * z.x - a.y * z.y;
-                x0.y += a.x * z.y + a.y * z.x;
-                x1.x += a.x * z.z - a.y * z.w;
-                x1.y += a.x * z.w + a.y * z.z;
-            }
-            if (out) {
-                emit1<N>(cl, base, ye, s, x0, invMu, nInv);
-                if (s + 1 < cl.nSym) emit1<N>(cl, base, ye, s + 1, x1, invMu, nInv);
-            }
+        for (int m = 0; m < LT; m++) {
+            const float2 a = gi[m];
+            const float4 z = *reinterpret_cast<const float4*>(sZ + m * W::ZS + s);
+            x0.x = fmaf(a.x, z.x, x0.x);
+            x0.x = fmaf(-a.y, z.y, x0.x);
+            x0.y = fmaf(a.x, z.y, x0.y);
+            x0.y = fmaf(a.y, z.x, x0.y);
+            x1.x = fmaf(a.x, z.z, x1.x);
+            x1.x = fmaf(-a.y, z.w, x1.x);
+            x1.y = fmaf(a.x, z.w, x1.y);
+            x1.y = fmaf(a.y, z.z, x1.y);
         }
+        emit1<N>(base, ye, s, x0, invMu, scl, d);
+        if (s + 1 < nSym) emit1<N>(base, ye, s + 1, x1, invMu, scl, d);
     }
 }
 
@@ -495,11 +505,11 @@ __device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid
         for (int j = 0; j < LT; j += 2) {
             if (j > m) break;                          // Linv[m][j] = 0 above the diagonal
             const float4 b = *reinterpret_cast<const float4*>(sG + m * W::RS + j);
-            gi[j].x += a.x * b.x + a.y * b.y;
-            gi[j].y += a.x * b.y - a.y * b.x;
+            gi[j].x = fmaf(a.y, b.y, fmaf(a.x, b.x, gi[j].x));
+            gi[j].y = fmaf(-a.y, b.x, fmaf(a.x, b.y, gi[j].y));
             if (j + 1 < LT) {
-                gi[j + 1].x += a.x * b.z + a.y * b.w;
-                gi[j + 1].y += a.x * b.w - a.y * b.z;
+                gi[j + 1].x = fmaf(a.y, b.w, fmaf(a.x, b.z, gi[j + 1].x));
+                gi[j + 1].y = fmaf(-a.y, b.z, fmaf(a.x, b.w, gi[j + 1].y));
             }
         }
     }
@@ -920,15 +930,22 @@ constexpr int kWarpsPerSm = 16;
 static int max_ctas(int warps, int warpBytes) {
     int k = kSmemPerSm / (warps * warpBytes);
     if (k > kWarpsPerSm / warps) k = kWarpsPerSm / warps;
+    if (k > 8) k = 8;
     return k;
 }
 
+// The shape with the most resident warps per SM; ties go to the larger CTA.
 static LaunchShape default_shape(int warpBytes) {
-    for (int w : {4, 2, 1}) {
+    LaunchShape best{1, max_ctas(1, warpBytes) > 0 ? max_ctas(1, warpBytes) : 1};
+    int bestWarps = 0;
+    for (int w : {4, 3, 2}) {
         const int k = max_ctas(w, warpBytes);
-        if (k >= 1) return {w, k};
+        if (k >= 1 && w * k > bestWarps) {
+            best = {w, k};
+            bestWarps = w * k;
+        }
     }
-    return {1, 1};
+    return best;
 }
 
 // A resolved launch: kernel instantiation, grid, block and dynamic shared
