@@ -51,6 +51,8 @@ struct FusedParams {
     int nCells;
     int epiBytes;    // per-warp epilogue region (bytes)
     int stageBytes;  // per operand stage (bytes)
+    int exactTile;   // shared exact layer tile (2, 4, 8, 16) or 0: selects the kernel
+    int nStages;     // operand stages per warp of that kernel
     long totalGroups;
 };
 
@@ -164,7 +166,7 @@ __device__ __forceinline__ CellView view_of(const FusedCell& c) {
 
 // ---------------------------------------------------------------------------
 // Operand staging.  Each warp streams its (subcarrier, 16-antenna chunk)
-// items through a ring of NST shared-memory stages with cp.async (16-byte
+// items through a ring of shared-memory stages with cp.async (16-byte
 // global -> shared copies that need no registers).  The ring runs ahead
 // across group boundaries, so while a warp does the FP32 solve and the LLR
 // epilogue of one group, the first chunks of its next group are in flight.
@@ -174,10 +176,10 @@ __device__ __forceinline__ CellView view_of(const FusedCell& c) {
 // 16 received rows Y[s][a0..a0+15] of 128 bytes whose 16-byte pieces are
 // XOR-swizzled by (s & 1) * 4 (conflict-free 16-byte fragment reads).
 // ---------------------------------------------------------------------------
-#ifndef AEQ_FUSED_STAGES
-#define AEQ_FUSED_STAGES 3
-#endif
-constexpr int NST = AEQ_FUSED_STAGES;   // stages per warp
+// Stages per warp: four where the epilogue region is small (exact tiles up to
+// 8 layers), three for the 16-layer tile and the generic kernel, whose larger
+// shared-memory footprint would otherwise cost resident warps.
+__host__ __device__ constexpr int stages_of(int exactTile) { return exactTile == 0 || exactTile == 16 ? 3 : 4; }
 constexpr int CHUNK = 16;       // antennas per stage (two k-steps)
 
 __host__ __device__ constexpr int hrs_of(int L) {
@@ -214,11 +216,13 @@ __device__ __forceinline__ float4 lds128(uint32_t a) {
 // FULL: all 16 antennas of the chunk exist, so no antenna mask is applied.
 // Rows of symbols past nSym are never masked: each received row only feeds
 // its own Z column, and columns past nSym are never read.
+// yo[kk][nt]: the lane's received-row fragment offsets in a stage (row
+// 8 nt + g, clamped to row 0 past nSym, antenna pair 8 kk + 2 c, swizzled),
+// fixed per cell.
 template <int LT, int P, bool LEXACT, bool FULL>
-__device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L, int nSym, float (*gacc)[4],
-                                          float (*zacc)[2][4], bool z2, int g, int c) {
+__device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L, const uint32_t (&yo)[2][2],
+                                          float (*gacc)[4], float (*zacc)[2][4], bool z2, int g, int c) {
     constexpr int NMT = LT > 8 ? 2 : 1;
-    const uint32_t ys = st + CHUNK * hrs;
 #pragma unroll
     for (int kk = 0; kk < 2; kk++) {
         const int a0 = 8 * kk + 2 * c;
@@ -238,9 +242,7 @@ __device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L
         float4 yv[2];
 #pragma unroll
         for (int nt = 0; nt < 2; nt++) {
-            const int s = 8 * nt + g;
-            const int sa = s < nSym ? s : 0;             // rows past nSym are not staged: read row 0 instead
-            const float4 y = lds128(ys + sa * 128 + (((a0 >> 1) ^ ((sa & 1) << 2)) << 4));
+            const float4 y = lds128(st + yo[kk][nt]);
             yv[nt] = FULL ? y : make_float4(v0 ? y.x : 0.f, v0 ? y.y : 0.f, v1 ? y.z : 0.f, v1 ? y.w : 0.f);
         }
         if constexpr (P == AERIAL_PREC_BF16X3) {
@@ -376,31 +378,21 @@ __device__ __forceinline__ void pam_llr_scaled(float pI, float pQ, const float* 
     }
 }
 
-// Symbol s of layer row i: Y_eq = x / mu (optional output), LLRs of x * r / mu.
-template <int N>
-__device__ __forceinline__ void emit1(float* base, float2* ye, int s, float2 x, float invMu, float scl,
-                                      const float* d) {
-    if (ye) __stcs(ye + s, make_float2(x.x * invMu, x.y * invMu));
+// One symbol of a layer row: Y_eq = x / mu (when YE), LLRs of x * r / mu at lp.
+template <int N, bool YE>
+__device__ __forceinline__ void emit1(float* lp, float2* ye, float2 x, float invMu, float scl, const float* d) {
+    if constexpr (YE) __stcs(ye, make_float2(x.x * invMu, x.y * invMu));
     float o[2 * N];
     pam_llr_scaled<N>(x.x * scl, x.y * scl, d, o);
-    write_llr<N>(base + s * 2 * N, o);
+    write_llr<N>(lp, o);
 }
 
 // X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs (FP32 fma chains), then
-// unbias and demap.  Lanes without an output row return at once.
-template <int LT, int N>
-__device__ __forceinline__ void solve_emit(const CellView& cl, const float2* sZ, const float2* gi, long sc, int i,
-                                           bool out, float invMu, float nInv) {
+// unbias and demap; lp / ye walk the row's LLRs and equalized symbols.
+template <int LT, int N, bool YE>
+__device__ __forceinline__ void emit_row(const float2* sZ, const float2* gi, float* lp, float2* ye, int nSym,
+                                         float invMu, float scl, const float* d) {
     using W = WarpSmem<LT>;
-    if (!out) return;
-    float* base = cl.llr + ((sc * cl.L + i) * (long)cl.nSym) * (2 * N);
-    float2* ye = cl.yeq ? cl.yeq + (sc * cl.L + i) * (long)cl.nSym : nullptr;
-    const float r = sqrtf(nInv);
-    const float scl = invMu * r;
-    float d[N];
-#pragma unroll
-    for (int k = 0; k < N; k++) d[k] = cl.lut.d[k] * r;
-    const int nSym = cl.nSym;
 #pragma unroll 1
     for (int s = 0; s < nSym; s += 2) {
         float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
@@ -417,9 +409,30 @@ __device__ __forceinline__ void solve_emit(const CellView& cl, const float2* sZ,
             x1.y = fmaf(a.x, z.w, x1.y);
             x1.y = fmaf(a.y, z.z, x1.y);
         }
-        emit1<N>(base, ye, s, x0, invMu, scl, d);
-        if (s + 1 < nSym) emit1<N>(base, ye, s + 1, x1, invMu, scl, d);
+        emit1<N, YE>(lp, ye, x0, invMu, scl, d);
+        if (s + 1 < nSym) emit1<N, YE>(lp + 2 * N, ye + 1, x1, invMu, scl, d);
+        lp += 4 * N;
+        if constexpr (YE) ye += 2;
     }
+}
+
+// Lane (sc, i): layer row i of subcarrier sc.  Lanes without an output row
+// return at once.
+template <int LT, int N>
+__device__ __forceinline__ void solve_emit(const CellView& cl, const float2* sZ, const float2* gi, long sc, int i,
+                                           bool out, float invMu, float nInv) {
+    if (!out) return;
+    const long row = sc * cl.L + i;
+    float* lp = cl.llr + row * cl.nSym * (2 * N);
+    const float r = sqrtf(nInv);
+    const float scl = invMu * r;
+    float d[N];
+#pragma unroll
+    for (int k = 0; k < N; k++) d[k] = cl.lut.d[k] * r;
+    if (cl.yeq)
+        emit_row<LT, N, true>(sZ, gi, lp, cl.yeq + row * cl.nSym, cl.nSym, invMu, scl, d);
+    else
+        emit_row<LT, N, false>(sZ, gi, lp, nullptr, cl.nSym, invMu, scl, d);
 }
 
 __device__ __forceinline__ float shfl_f(float v, int src, int width) {
@@ -531,7 +544,7 @@ __device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid
 }
 
 // Per-warp shared memory of a launch: the epilogue region (largest footprint
-// of the layer tiles present) followed by NST operand stages.
+// of the layer tiles present) followed by the operand stages.
 inline int stage_bytes_of(const FusedParams& p) {
     int b = 0;
     for (int ci = 0; ci < p.nCells; ci++) {
@@ -668,6 +681,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     const int wib = threadIdx.x >> 5;
     const int warpsPerCta = blockDim.x >> 5;
     const int g = lane >> 2, c = lane & 3;
+    constexpr int NST = stages_of(LTF);
     const int warpBytes = p.epiBytes + NST * p.stageBytes;
     const int smemOff = wib * (warpBytes / 8);
     float2* sm = reinterpret_cast<float2*>(smem_raw) + smemOff;
@@ -748,19 +762,28 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     long grp = gw;
     int ci = 0;
     while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
-    int q = 0, ch = 0, cslot = 0, nValid, cNChunk, cNFull, cA, cNSym, cL, cLT, cHrs;
+    int q = 0, ch = 0, cslot = 0, nValid, cNChunk, cNFull, cA, cL, cLT, cHrs;
     bool z2;
+    uint32_t yo[2][2];
     auto load_ccell = [&]() {
         const FusedCell& cl = p.cell[ci];
         nValid = group_valid(cl, grp);
         cA = cl.A;
-        cNSym = cl.nSym;
         cNChunk = cl.nChunk;
         cNFull = cl.A / CHUNK;
         cL = cl.L;
         cLT = LTF != 0 ? LTF : cl.LT;
         cHrs = cl.hrs;
         z2 = cl.nSym > 8;
+        const uint32_t ys = CHUNK * (LTF != 0 ? hrs_of(LTF) : cl.hrs);
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) {
+                const int r = 8 * nt + g;
+                const int ra = r < cl.nSym ? r : 0;      // rows past nSym are not staged: read row 0 instead
+                yo[kk][nt] = ys + ra * 128 + (((4 * kk + c) ^ ((ra & 1) << 2)) << 4);
+            }
     };
     load_ccell();
     float gacc[3][4], zacc[2][2][4];
@@ -784,17 +807,17 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
         cslot = cslot == NST - 1 ? 0 : cslot + 1;
         if constexpr (LTF != 0) {
             if (ch < cNFull)
-                mma_stage<LTF, P, true, true>(st, hrs_of(LTF), CHUNK, LTF, cNSym, gacc, zacc, z2, g, c);
+                mma_stage<LTF, P, true, true>(st, hrs_of(LTF), CHUNK, LTF, yo, gacc, zacc, z2, g, c);
             else
-                mma_stage<LTF, P, true, false>(st, hrs_of(LTF), cA - CHUNK * ch, LTF, cNSym, gacc, zacc, z2, g, c);
+                mma_stage<LTF, P, true, false>(st, hrs_of(LTF), cA - CHUNK * ch, LTF, yo, gacc, zacc, z2, g, c);
         } else {
             const int nRows = min(CHUNK, cA - CHUNK * ch);
             switch (cLT) {
-                case 1: mma_stage<1, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
-                case 2: mma_stage<2, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
-                case 4: mma_stage<4, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
-                case 8: mma_stage<8, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
-                default: mma_stage<16, P, false, false>(st, cHrs, nRows, cL, cNSym, gacc, zacc, z2, g, c); break;
+                case 1: mma_stage<1, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
+                case 2: mma_stage<2, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
+                case 4: mma_stage<4, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
+                case 8: mma_stage<8, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
+                default: mma_stage<16, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
             }
         }
         if (++ch < cNChunk) continue;
@@ -856,9 +879,21 @@ static int layer_tile(int L) {
     return t;
 }
 
+// The layer tile shared by every cell when each has nLayers == tile in
+// {2, 4, 8, 16} and 16-byte aligned H / Y_rx; 0 otherwise (generic kernel).
+static int exact_tile(const FusedParams& p) {
+    const int lt = p.cell[0].LT;
+    if (lt < 2) return 0;
+    for (int i = 0; i < p.nCells; i++) {
+        const FusedCell& c = p.cell[i];
+        if (c.LT != lt || c.L != lt || !c.vecH || !c.vecY) return 0;
+    }
+    return lt;
+}
+
 // warpBytes: the per-warp shared memory of the launch (epilogue region of the
 // largest layer-tile footprint present, which is not monotonic in the tile,
-// plus NST operand stages).
+// plus the kernel's operand stages).
 int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p, int& warpBytes) {
     if (!cells || nCells < 1 || nCells > kMaxCells) return AERIAL_ERR_INVALID_ARG;
     long g0 = 0;
@@ -903,7 +938,9 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
     p.totalGroups = g0;
     p.epiBytes = epi_bytes_of(p);
     p.stageBytes = stage_bytes_of(p);
-    warpBytes = p.epiBytes + NST * p.stageBytes;
+    p.exactTile = exact_tile(p);
+    p.nStages = stages_of(p.exactTile);
+    warpBytes = p.epiBytes + p.nStages * p.stageBytes;
     return AERIAL_OK;
 }
 
@@ -977,21 +1014,9 @@ static int plan_v(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPla
     return AERIAL_OK;
 }
 
-// The layer tile shared by every cell when each has nLayers == tile in
-// {2, 4, 8, 16} and 16-byte aligned H / Y_rx; 0 otherwise (generic kernel).
-static int exact_tile(const FusedParams& p) {
-    const int lt = p.cell[0].LT;
-    if (lt < 2) return 0;
-    for (int i = 0; i < p.nCells; i++) {
-        const FusedCell& c = p.cell[i];
-        if (c.LT != lt || c.L != lt || !c.vecH || !c.vecY) return 0;
-    }
-    return lt;
-}
-
 template <int P>
 static int plan_p(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
-    switch (exact_tile(p)) {
+    switch (p.exactTile) {
         case 2: return plan_v<P, 2>(p, warpBytes, sh, out);
         case 4: return plan_v<P, 4>(p, warpBytes, sh, out);
         case 8: return plan_v<P, 8>(p, warpBytes, sh, out);
