@@ -131,6 +131,8 @@ SIGNATURES = {
     "aerial_pusch_eq_plain": (_I, [ctypes.POINTER(CellDesc), _I, _P, _Z, _P]),
     "aerial_autotune": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), ctypes.POINTER(_F), _P]),
     "aerial_pusch_eq_plain_static": (_I, [ctypes.POINTER(CellDesc), _I, _P]),
+    "aerial_pusch_eq_host_workspace": (_I, [ctypes.POINTER(CellDesc), _I, _I, ctypes.POINTER(_Z)]),
+    "aerial_pusch_eq_host": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), _I, _P, _Z, _P]),
     "aerial_eq_graph_create": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), ctypes.POINTER(_P)]),
     "aerial_eq_graph_update": (_I, [_P, ctypes.POINTER(CellDesc), _I]),
     "aerial_eq_graph_launch": (_I, [_P, _P]),
@@ -305,6 +307,48 @@ def pusch_eq_plain_static(cells, stream=None):
     device array (shared by all calls; calls overlapping on the GPU race)."""
     arr, n = _cells_array(cells)
     _check(lib().aerial_pusch_eq_plain_static(arr, n, _stream(stream)), "pusch_eq_plain_static")
+
+
+def _host_ptr(t):
+    if t is None:
+        return None
+    if t.is_cuda:
+        raise ValueError("expected a host tensor (pinned for overlapped copies)")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def host_cell_desc(H, Y_rx, llr_out, sigma2, nPRB, nAnt, nLayers, nSym, nPamBits, Y_eq=None) -> CellDesc:
+    """A cell whose buffers are host tensors, for pusch_eq_host."""
+    d = CellDesc()
+    d.H = _host_ptr(H).value
+    d.Y_rx = _host_ptr(Y_rx).value
+    d.llr = _host_ptr(llr_out).value
+    d.Y_eq = _host_ptr(Y_eq).value if Y_eq is not None else None
+    d.sigma2 = float(sigma2)
+    d.nPRB, d.nAnt, d.nLayers, d.nSym, d.nPamBits = int(nPRB), int(nAnt), int(nLayers), int(nSym), int(nPamBits)
+    return d
+
+
+def pusch_eq_host_workspace(cells, cells_per_batch=0) -> int:
+    """Device bytes that pusch_eq_host needs to stage these host cells."""
+    arr = (CellDesc * len(cells))(*cells)
+    b = _Z(0)
+    _check(lib().aerial_pusch_eq_host_workspace(arr, len(cells), int(cells_per_batch), ctypes.byref(b)),
+           "pusch_eq_host_workspace")
+    return int(b.value)
+
+
+def pusch_eq_host(cells, workspace, tuning: Tuning | None = None, cells_per_batch=0, stream=None):
+    """The fused chain on host buffers (host_cell_desc cells): copies in,
+    equalizes and copies the LLRs back, batches overlapped over three streams.
+    Asynchronous on `stream`: synchronize it before reading the outputs."""
+    arr = (CellDesc * len(cells))(*cells)
+    tp = ctypes.pointer(tuning) if tuning is not None else None
+    _check(lib().aerial_pusch_eq_host(arr, len(cells), tp, int(cells_per_batch), _ptr(workspace),
+                                      workspace.numel() * workspace.element_size(), _stream(stream)),
+           "pusch_eq_host")
 
 
 def autotune(cells, precision=PREC_FP16, stream=None):

@@ -179,6 +179,23 @@ typedef struct {
 int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
                           void* stream);
 
+/* The fused chain on HOST buffers: each cell's H, Y_rx, llr (and optional
+ * Y_eq) are host pointers (page-locked for the copies to overlap).  Cells
+ * run in batches of cellsPerBatch (0 = automatic: batches of at least 4 MiB
+ * of input) through three internal streams, so host-to-device copies, fused
+ * launches and device-to-host copies of successive batches overlap.  The
+ * caller's device workspace (256-byte aligned, size from
+ * aerial_pusch_eq_host_workspace) stages the batches.  Everything is
+ * enqueued asynchronously behind the work already on `stream`, and `stream`
+ * waits for all of it: synchronize `stream` before reading the outputs.  Any
+ * number of cells; the first call on a device creates the internal streams.
+ * Replaces the reference's blocking cudaMemcpy staging around its launches
+ * (src/aerial_coef_wmma.cu:396-397, :414-416). */
+int aerial_pusch_eq_host_workspace(const aerial_cell_desc* cells, int nCells, int cellsPerBatch,
+                                   size_t* bytes);
+int aerial_pusch_eq_host(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
+                         int cellsPerBatch, void* workspace, size_t workspaceBytes, void* stream);
+
 /* The plain FP32 chain for the same cells: aerial_gram, aerial_mmse_coef,
  * aerial_coef_apply and aerial_llr_f32 per cell, intermediates in the
  * caller's workspace (size from aerial_pusch_eq_plain_workspace).  This is

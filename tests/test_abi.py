@@ -73,3 +73,35 @@ def test_server_rejects_bad_config_without_gpu():
     assert lib.aerial_server_destroy(None) == 1001
     n = ctypes.c_int()
     assert lib.aerial_server_poll(None, None, 0, ctypes.byref(n)) == 1001
+
+
+def test_host_pipeline_workspace_and_checks_without_gpu():
+    """Workspace sizing and argument checks of aerial_pusch_eq_host run on the
+    host: three slots of the largest batch, every buffer 256-byte aligned."""
+    pkg = load_pkg()
+    lib = pkg.lib()
+    fake = 0x100000
+    def desc(nPRB, nAnt, nLayers, nSym, nPam, yeq=False):
+        return pkg.CellDesc(fake, fake, fake, fake if yeq else None, 0.1, nPRB, nAnt, nLayers, nSym, nPam)
+    al = lambda v: (v + 255) // 256 * 256
+    def foot(p, a, l, s, n, yeq=False):
+        sc = 12 * p
+        return al(sc * a * l * 8) + al(sc * s * a * 8) + al(sc * l * s * 2 * n * 4) + (al(sc * l * s * 8) if yeq else 0)
+    cells = [desc(132, 64, 8, 11, 4), desc(24, 32, 4, 11, 2, True), desc(273, 128, 16, 11, 4),
+             desc(51, 16, 2, 14, 1), desc(106, 64, 4, 11, 3)]
+    arr = (pkg.CellDesc * 5)(*cells)
+    b = ctypes.c_size_t(0)
+    assert lib.aerial_pusch_eq_host_workspace(arr, 5, 2, ctypes.byref(b)) == 0
+    f = [foot(132, 64, 8, 11, 4), foot(24, 32, 4, 11, 2, True), foot(273, 128, 16, 11, 4), foot(51, 16, 2, 14, 1),
+         foot(106, 64, 4, 11, 3)]
+    assert b.value == 3 * max(f[0] + f[1], f[2] + f[3], f[4])
+    assert lib.aerial_pusch_eq_host_workspace(arr, 1, 0, ctypes.byref(b)) == 0
+    assert b.value == f[0]                      # one batch, one slot
+    assert lib.aerial_pusch_eq_host_workspace(arr, 5, -1, ctypes.byref(b)) == 1001
+    assert lib.aerial_pusch_eq_host_workspace(None, 5, 0, ctypes.byref(b)) == 1001
+    bad = (pkg.CellDesc * 1)(desc(132, 64, 17, 11, 4))
+    assert lib.aerial_pusch_eq_host_workspace(bad, 1, 0, ctypes.byref(b)) == 1001
+    ws = ctypes.c_void_p(0x200000)
+    assert lib.aerial_pusch_eq_host(arr, 5, None, 2, ws, 1024, None) == 1001         # workspace too small
+    assert lib.aerial_pusch_eq_host(arr, 5, None, 2, ctypes.c_void_p(0x200010), 1 << 40, None) == 1001  # misaligned
+    assert lib.aerial_pusch_eq_host(bad, 1, None, 0, ws, 1 << 40, None) == 1001
