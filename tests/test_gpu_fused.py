@@ -159,3 +159,41 @@ def test_multicell_mixed_layer_tiles(aeq, wl, orc, cuda):
         check_against_fp64(orc, c, mixed[k][0], mixed[k][1], -60.0)
         alone = run_fused(aeq, [c], cuda, "bf16x3")[0]
         np.testing.assert_array_equal(alone[0], mixed[k][0])
+
+
+# Launches whose cells all have 8 layers run the exact 8-layer kernel: antenna
+# counts that leave a partial last chunk, fewer antennas than one chunk, and
+# symbol counts from 1 to 16.
+TMA_SHAPES = [  # (nPRB, nAnt, nLayers, nSym, qam)
+    (1, 2, 8, 1, 4),
+    (1, 6, 8, 8, 16),
+    (2, 8, 8, 9, 64),
+    (1, 24, 8, 14, 256),
+    (3, 40, 8, 16, 16),
+    (2, 64, 8, 11, 256),
+    (1, 128, 8, 13, 64),
+    (1, 256, 8, 5, 4),
+]
+
+
+@pytest.mark.parametrize("shape", TMA_SHAPES)
+def test_fused_exact_8_layer_shapes(aeq, wl, orc, cuda, shape):
+    nPRB, A, L, S, q = shape
+    c = wl.make_cell(nPRB, A, L, S, q, 25.0, seed=91)
+    (llr, yeq), = run_fused(aeq, [c], cuda, "bf16x3")
+    check_against_fp64(orc, c, llr, yeq, -60.0)
+    if A >= 16:
+        (llr, yeq), = run_fused(aeq, [c], cuda, "fp16")
+        check_against_fp64(orc, c, llr, yeq, -45.0)
+
+
+def test_fused_exact_8_layer_mix_alone_and_in_mix(aeq, wl, orc, cuda):
+    """Several 8-layer cells of different shapes in one exact-tile launch:
+    each equals its own single-cell launch bit for bit and matches FP64."""
+    cells = [wl.make_cell(p, a, 8, s, q, 25.0, seed=100 + k)
+             for k, (p, a, _, s, q) in enumerate(TMA_SHAPES[2:])]
+    mixed = run_fused(aeq, cells, cuda, "fp16")
+    for k, c in enumerate(cells):
+        alone = run_fused(aeq, [c], cuda, "fp16")[0]
+        np.testing.assert_array_equal(alone[0], mixed[k][0])
+        check_against_fp64(orc, c, mixed[k][0], mixed[k][1], -45.0)

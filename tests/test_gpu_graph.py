@@ -52,3 +52,23 @@ def test_graph_update_rejects_new_shapes(aeq, wl, cuda):
             g.update(d2)
     finally:
         g.close()
+
+
+def test_graph_of_exact_tile_launch(aeq, wl, cuda):
+    """All cells with 8 layers: the graph node runs the exact 8-layer kernel."""
+    cells_a = [wl.make_cell(3, 64, 8, 11, 256, 25.0, seed=81), wl.make_cell(2, 24, 8, 9, 16, 20.0, seed=82)]
+    cells_b = [wl.make_cell(3, 64, 8, 11, 256, 25.0, seed=83), wl.make_cell(2, 24, 8, 9, 16, 20.0, seed=84)]
+    ref_a, da = _descs(aeq, cells_a, cuda)
+    aeq.pusch_eq_fused(da)
+    ref_b, db = _descs(aeq, cells_b, cuda)
+    aeq.pusch_eq_fused(db)
+    torch.cuda.synchronize()
+    got_a, ga = _descs(aeq, cells_a, cuda)
+    got_b, gb = _descs(aeq, cells_b, cuda)
+    with aeq.FusedGraph(ga) as g:
+        g.launch()
+        g.update(gb)
+        g.launch()
+        torch.cuda.synchronize()
+    for r, o in zip(ref_a + ref_b, got_a + got_b):
+        np.testing.assert_array_equal(o[2].cpu().numpy(), r[2].cpu().numpy())
