@@ -53,6 +53,7 @@ struct FusedParams {
     int stageBytes;  // per operand stage (bytes)
     int exactTile;   // shared exact layer tile (2, 4, 8, 16) or 0: selects the kernel
     int nStages;     // operand stages per warp of that kernel
+    int exactChunks; // with an exact tile: every cell has nAnt == 16 * exactChunks (2, 4, 8), else 0
     long totalGroups;
 };
 
@@ -871,6 +872,172 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
 }
 
 // ---------------------------------------------------------------------------
+// Exact-antenna variant: every cell of the launch has nLayers == LTF and
+// nAnt == 16 * NCH.  A subcarrier's NCH chunks are unrolled, so the stage
+// the producer fills at each step (chunk k + NST - 1 of this subcarrier, or
+// an early chunk of the next one) is known at compile time, and its copies
+// are a per-lane subcarrier pointer plus immediate offsets.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int stages_of_a(int ltf, int nch) {
+    return stages_of(ltf) < nch + 1 ? stages_of(ltf) : nch + 1;
+}
+
+// One subcarrier's operands as the producing lane sees them: its first
+// channel piece, its first received piece, its count of received rows.
+struct ScPtr {
+    const float2* h;
+    const float2* y;
+    int yk;
+};
+
+// Chunk j of subcarrier s into the stage at st (A = 16 NCH antennas).
+template <int LF, int NCH>
+__device__ __forceinline__ void stage_chunk(uint32_t st, uint32_t hLaneS, uint32_t yLaneS, const ScPtr& s, int j,
+                                            int lane) {
+    constexpr int HRS = hrs_of(LF);
+    constexpr int HALF = LF / 2;
+    constexpr int NP = CHUNK * HALF;
+    constexpr int RPK = 32 / HALF;
+    constexpr int A = CHUNK * NCH;
+#pragma unroll
+    for (int k = 0; k < (NP + 31) / 32; k++)
+        if (NP >= 32 * (k + 1) || lane < NP - 32 * k)
+            cp_async16(st + hLaneS + k * RPK * HRS, s.h + CHUNK * j * LF + 64 * k);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        if (k < s.yk) cp_async16(st + yLaneS + 512 * k, s.y + CHUNK * j + 4 * k * A);
+}
+
+template <int P, int LTF, int NCH>
+__global__ void __launch_bounds__(256, 2) fused_eq_kernel_a(const __grid_constant__ FusedParams p) {
+    constexpr int NST = stages_of_a(LTF, NCH);
+    constexpr int A = CHUNK * NCH;
+    constexpr int HRS = hrs_of(LTF);
+    constexpr long HSC = (long)A * LTF;               // channel float2 per subcarrier
+    extern __shared__ float4 smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warpsPerCta = blockDim.x >> 5;
+    const int g = lane >> 2, c = lane & 3;
+    const int warpBytes = p.epiBytes + NST * p.stageBytes;
+    const int smemOff = wib * (warpBytes / 8);
+    float2* sm = reinterpret_cast<float2*>(smem_raw) + smemOff;
+    const uint32_t stBase =
+        (uint32_t)__cvta_generic_to_shared(reinterpret_cast<char*>(smem_raw) + (long)wib * warpBytes + p.epiBytes);
+    const long gw = (long)blockIdx.x * warpsPerCta + wib;
+    const long nw = (long)gridDim.x * warpsPerCta;
+    const long total = p.totalGroups;
+    if (gw >= total) return;
+
+    constexpr int HALF = LTF / 2;
+    const uint32_t hLaneS = (lane / HALF) * HRS + (lane % HALF) * 16;
+    const uint32_t yLaneS = CHUNK * HRS + (lane >> 3) * 128 + (((lane & 7) ^ (((lane >> 3) & 1) << 2)) << 4);
+    const int yLaneG = (lane >> 3) * A + 2 * (lane & 7);
+
+    // first subcarrier of group grp (in cell ci) as seen by this lane
+    auto first_sc = [&](int cell, long grp) -> ScPtr {
+        const FusedCell& cl = p.cell[cell];
+        const long sc = (grp - cl.group0) * cl.GS;
+        ScPtr s;
+        s.h = cl.H + sc * HSC + 2 * lane;
+        s.y = cl.Y + sc * cl.nSym * A + yLaneG;
+        s.yk = min(4, max(0, (cl.nSym - (lane >> 3) + 3) >> 2));
+        return s;
+    };
+
+    long grp = gw;
+    int ci = 0;
+    while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+    int nValid, nSym;
+    bool z2;
+    uint32_t yo[2][2];
+    auto load_cell = [&]() {
+        const FusedCell& cl = p.cell[ci];
+        nValid = group_valid(cl, grp);
+        nSym = cl.nSym;
+        z2 = nSym > 8;
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) {
+                const int r = 8 * nt + g;
+                const int ra = r < nSym ? r : 0;         // rows past nSym are not staged: read row 0 instead
+                yo[kk][nt] = CHUNK * HRS + ra * 128 + (((4 * kk + c) ^ ((ra & 1) << 2)) << 4);
+            }
+    };
+    load_cell();
+    ScPtr cur = first_sc(ci, grp);
+
+    int pslot = 0, cslot = 0;
+#pragma unroll
+    for (int j = 0; j < NST - 1; j++) {
+        stage_chunk<LTF, NCH>(stBase + pslot * p.stageBytes, hLaneS, yLaneS, cur, j, lane);
+        cp_async_commit();
+        pslot = pslot == NST - 1 ? 0 : pslot + 1;
+    }
+
+    float gacc[3][4], zacc[2][2][4];
+    int q = 0;
+    while (true) {
+        // the subcarrier after this one in the warp's order, if any
+        ScPtr nxt = cur;
+        bool hasNxt = true;
+        if (q + 1 < nValid) {
+            nxt.h = cur.h + HSC;
+            nxt.y = cur.y + (long)nSym * A;
+        } else {
+            const long ng = grp + nw;
+            hasNxt = ng < total;
+            if (hasNxt) {
+                int nc = ci;
+                while (nc + 1 < p.nCells && ng >= p.cell[nc + 1].group0) nc++;
+                nxt = first_sc(nc, ng);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
+#pragma unroll
+        for (int k = 0; k < NCH; k++) {
+            __syncwarp();                              // every lane is done with the slot refilled now
+            const uint32_t pst = stBase + pslot * p.stageBytes;
+            if (k + NST - 1 < NCH)
+                stage_chunk<LTF, NCH>(pst, hLaneS, yLaneS, cur, k + NST - 1, lane);
+            else if (hasNxt)
+                stage_chunk<LTF, NCH>(pst, hLaneS, yLaneS, nxt, k + NST - 1 - NCH, lane);
+            cp_async_commit();
+            pslot = pslot == NST - 1 ? 0 : pslot + 1;
+            cp_async_wait<NST - 1>();                  // this chunk's copies (own lane) have landed
+            __syncwarp();                              // ... and every lane's
+            mma_stage<LTF, P, true, true>(stBase + cslot * p.stageBytes, HRS, CHUNK, LTF, yo, gacc, zacc, z2, g,
+                                          c);
+            cslot = cslot == NST - 1 ? 0 : cslot + 1;
+        }
+        store_acc<LTF>(sm, gacc, zacc, q, g, c);
+        cur = nxt;
+        if (++q < nValid) continue;
+        __syncwarp();
+        {
+            const FusedCell& cl = p.cell[ci];
+            solve_group<LTF, P>(view_of(cl), (grp - cl.group0) * cl.GS, nValid, smemOff, lane);
+        }
+        q = 0;
+        grp += nw;
+        if (grp >= total) break;
+        while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+        load_cell();
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 static int layer_tile(int L) {
@@ -939,7 +1106,16 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
     p.epiBytes = epi_bytes_of(p);
     p.stageBytes = stage_bytes_of(p);
     p.exactTile = exact_tile(p);
-    p.nStages = stages_of(p.exactTile);
+    p.exactChunks = 0;
+    if (p.exactTile) {
+        const int a = p.cell[0].A;
+        // (16-layer tiles keep the runtime chunk loop: unrolling their
+        // larger k-step bodies measured slower)
+        bool same = p.exactTile <= 8 && (a == 32 || a == 64 || a == 128);
+        for (int i = 1; i < nCells && same; i++) same = p.cell[i].A == a;
+        if (same) p.exactChunks = a / CHUNK;
+    }
+    p.nStages = p.exactChunks ? stages_of_a(p.exactTile, p.exactChunks) : stages_of(p.exactTile);
     warpBytes = p.epiBytes + p.nStages * p.stageBytes;
     return AERIAL_OK;
 }
@@ -1014,8 +1190,46 @@ static int plan_v(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPla
     return AERIAL_OK;
 }
 
+template <int P, int LTF, int NCH>
+static int plan_a(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
+    static int configured = 0;
+    const int bytes = sh.warps * warpBytes;
+    if (bytes > 48 * 1024 && bytes > configured) {
+        cudaError_t e =
+            cudaFuncSetAttribute(fused_eq_kernel_a<P, LTF, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return (int)e;
+        configured = bytes;
+    }
+    long need = (p.totalGroups + sh.warps - 1) / sh.warps;
+    long grid = (long)sm_count() * sh.ctasPerSm;
+    if (grid > need) grid = need;
+    if (grid < 1) grid = 1;
+    out.func = reinterpret_cast<const void*>(fused_eq_kernel_a<P, LTF, NCH>);
+    out.grid = dim3((unsigned)grid);
+    out.block = dim3(sh.warps * 32);
+    out.smem = bytes;
+    return AERIAL_OK;
+}
+
+template <int P, int LTF>
+static int plan_an(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
+    switch (p.exactChunks) {
+        case 2: return plan_a<P, LTF, 2>(p, warpBytes, sh, out);
+        case 4: return plan_a<P, LTF, 4>(p, warpBytes, sh, out);
+        default: return plan_a<P, LTF, 8>(p, warpBytes, sh, out);
+    }
+}
+
 template <int P>
 static int plan_p(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
+    if (p.exactChunks) {
+        switch (p.exactTile) {
+            case 2: return plan_an<P, 2>(p, warpBytes, sh, out);
+            case 4: return plan_an<P, 4>(p, warpBytes, sh, out);
+            case 8: return plan_an<P, 8>(p, warpBytes, sh, out);
+            default: return plan_an<P, 16>(p, warpBytes, sh, out);
+        }
+    }
     switch (p.exactTile) {
         case 2: return plan_v<P, 2>(p, warpBytes, sh, out);
         case 4: return plan_v<P, 4>(p, warpBytes, sh, out);
@@ -1232,9 +1446,31 @@ static int prepare_v() {
     return e == cudaSuccess ? AERIAL_OK : (int)e;
 }
 
+template <int P, int LTF, int NCH>
+static int prepare_a() {
+    cudaFuncAttributes at;
+    cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_a<P, LTF, NCH>);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fused_eq_kernel_a<P, LTF, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 220 * 1024);
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
+template <int P, int LTF>
+static int prepare_an() {
+    int s = prepare_a<P, LTF, 2>();
+    if (!s) s = prepare_a<P, LTF, 4>();
+    if (!s) s = prepare_a<P, LTF, 8>();
+    return s;
+}
+
 template <int P>
 static int prepare_p() {
-    int s = prepare_v<P, 0>();
+    int s = prepare_an<P, 2>();
+    if (!s) s = prepare_an<P, 4>();
+    if (!s) s = prepare_an<P, 8>();
+    if (!s) s = prepare_an<P, 16>();
+    if (!s) s = prepare_v<P, 0>();
     if (!s) s = prepare_v<P, 2>();
     if (!s) s = prepare_v<P, 4>();
     if (!s) s = prepare_v<P, 8>();

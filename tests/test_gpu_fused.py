@@ -162,11 +162,11 @@ def test_multicell_mixed_layer_tiles(aeq, wl, orc, cuda):
 
 
 # Launches whose cells all have 8 layers run the exact 8-layer kernel: antenna
-# counts that leave a partial last chunk, fewer antennas than one chunk, and
-# symbol counts from 1 to 16.
+# counts that leave a partial last chunk, fewer antennas than one chunk (but
+# at least as many as layers), and symbol counts from 1 to 16.
 TMA_SHAPES = [  # (nPRB, nAnt, nLayers, nSym, qam)
-    (1, 2, 8, 1, 4),
-    (1, 6, 8, 8, 16),
+    (1, 12, 8, 1, 4),
+    (1, 14, 8, 8, 16),
     (2, 8, 8, 9, 64),
     (1, 24, 8, 14, 256),
     (3, 40, 8, 16, 16),
@@ -197,3 +197,22 @@ def test_fused_exact_8_layer_mix_alone_and_in_mix(aeq, wl, orc, cuda):
         alone = run_fused(aeq, [c], cuda, "fp16")[0]
         np.testing.assert_array_equal(alone[0], mixed[k][0])
         check_against_fp64(orc, c, mixed[k][0], mixed[k][1], -45.0)
+
+
+@pytest.mark.parametrize("L", [2, 4, 8, 16])
+@pytest.mark.parametrize("A", [32, 64, 128])
+def test_fused_exact_antenna_kernels(aeq, wl, orc, cuda, L, A):
+    """Launches whose cells share nLayers and nAnt in {32, 64, 128} run the
+    kernel with the antenna chunks unrolled; adding a cell with another
+    antenna count switches the launch to the runtime-chunk kernel.  Each cell's
+    results are the same bit for bit in both, and match FP64."""
+    cells = [wl.make_cell(2, A, L, 11, 256, 25.0, seed=200 + A + L),
+             wl.make_cell(1, A, L, 5, 16, 20.0, seed=300 + A + L),
+             wl.make_cell(1, A, L, 14, 64, 25.0, seed=400 + A + L)]
+    other = wl.make_cell(1, 48, L, 7, 4, 15.0, seed=500 + A + L)
+    exact = run_fused(aeq, cells, cuda, "bf16x3")
+    mixed = run_fused(aeq, cells + [other], cuda, "bf16x3")
+    for k, c in enumerate(cells):
+        np.testing.assert_array_equal(exact[k][0], mixed[k][0])
+        np.testing.assert_array_equal(exact[k][1], mixed[k][1])
+        check_against_fp64(orc, c, exact[k][0], exact[k][1], -60.0)
