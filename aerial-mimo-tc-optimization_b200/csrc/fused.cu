@@ -390,30 +390,97 @@ __device__ __forceinline__ void emit1(float* lp, float2* ye, float2 x, float inv
 
 // X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs (FP32 fma chains), then
 // unbias and demap; lp / ye walk the row's LLRs and equalized symbols.
+// Packed FP32 pairs (fma.rn.f32x2 and friends, two IEEE operations per
+// instruction on sm_100a).
+__device__ __forceinline__ unsigned long long pk2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ void lds2x64(uint32_t a, unsigned long long& v0, unsigned long long& v1) {
+    asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];\n" : "=l"(v0), "=l"(v1) : "r"(a));
+}
+
+// X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs, then unbias and demap;
+// lp / ye walk the row's LLRs and equalized symbols.  Up to 8-layer tiles the
+// sums run on packed pairs: with Z[m][s] = (zr, zi) as stored,
+//   P_s = sum_m (Re g_m, Re g_m) * (zr, zi),  Q_s = sum_m (Im g_m, Im g_m) * (zr, zi)
+//   X_s = (P.x - Q.y, P.y + Q.x),
+// four packed FMAs per m and symbol pair instead of eight scalar ones.
 template <int LT, int N, bool YE>
 __device__ __forceinline__ void emit_row(const float2* sZ, const float2* gi, float* lp, float2* ye, int nSym,
                                          float invMu, float scl, const float* d) {
     using W = WarpSmem<LT>;
-#pragma unroll 1
-    for (int s = 0; s < nSym; s += 2) {
-        float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
+    if constexpr (LT <= 8) {
+        unsigned long long gr[LT], gq[LT];
 #pragma unroll
         for (int m = 0; m < LT; m++) {
-            const float2 a = gi[m];
-            const float4 z = *reinterpret_cast<const float4*>(sZ + m * W::ZS + s);
-            x0.x = fmaf(a.x, z.x, x0.x);
-            x0.x = fmaf(-a.y, z.y, x0.x);
-            x0.y = fmaf(a.x, z.y, x0.y);
-            x0.y = fmaf(a.y, z.x, x0.y);
-            x1.x = fmaf(a.x, z.z, x1.x);
-            x1.x = fmaf(-a.y, z.w, x1.x);
-            x1.y = fmaf(a.x, z.w, x1.y);
-            x1.y = fmaf(a.y, z.z, x1.y);
+            gr[m] = pk2(gi[m].x, gi[m].x);
+            gq[m] = pk2(gi[m].y, gi[m].y);
         }
-        emit1<N, YE>(lp, ye, x0, invMu, scl, d);
-        if (s + 1 < nSym) emit1<N, YE>(lp + 2 * N, ye + 1, x1, invMu, scl, d);
-        lp += 4 * N;
-        if constexpr (YE) ye += 2;
+        const uint32_t zb = (uint32_t)__cvta_generic_to_shared(sZ);
+#pragma unroll 1
+        for (int s = 0; s < nSym; s += 2) {
+            unsigned long long P0, Q0, P1, Q1;
+#pragma unroll
+            for (int m = 0; m < LT; m++) {
+                unsigned long long z0, z1;
+                lds2x64(zb + (m * W::ZS + s) * 8, z0, z1);
+                if (m == 0) {
+                    P0 = mul2(gr[0], z0);
+                    Q0 = mul2(gq[0], z0);
+                    P1 = mul2(gr[0], z1);
+                    Q1 = mul2(gq[0], z1);
+                } else {
+                    P0 = fma2(gr[m], z0, P0);
+                    Q0 = fma2(gq[m], z0, Q0);
+                    P1 = fma2(gr[m], z1, P1);
+                    Q1 = fma2(gq[m], z1, Q1);
+                }
+            }
+            const float2 p0 = upk2(P0), q0 = upk2(Q0), p1 = upk2(P1), q1 = upk2(Q1);
+            emit1<N, YE>(lp, ye, make_float2(p0.x - q0.y, p0.y + q0.x), invMu, scl, d);
+            if (s + 1 < nSym) emit1<N, YE>(lp + 2 * N, ye + 1, make_float2(p1.x - q1.y, p1.y + q1.x), invMu, scl, d);
+            lp += 4 * N;
+            if constexpr (YE) ye += 2;
+        }
+    } else {
+#pragma unroll 1
+        for (int s = 0; s < nSym; s += 2) {
+            float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int m = 0; m < LT; m++) {
+                const float2 a = gi[m];
+                const float4 z = *reinterpret_cast<const float4*>(sZ + m * W::ZS + s);
+                x0.x = fmaf(a.x, z.x, x0.x);
+                x0.x = fmaf(-a.y, z.y, x0.x);
+                x0.y = fmaf(a.x, z.y, x0.y);
+                x0.y = fmaf(a.y, z.x, x0.y);
+                x1.x = fmaf(a.x, z.z, x1.x);
+                x1.x = fmaf(-a.y, z.w, x1.x);
+                x1.y = fmaf(a.x, z.w, x1.y);
+                x1.y = fmaf(a.y, z.z, x1.y);
+            }
+            emit1<N, YE>(lp, ye, x0, invMu, scl, d);
+            if (s + 1 < nSym) emit1<N, YE>(lp + 2 * N, ye + 1, x1, invMu, scl, d);
+            lp += 4 * N;
+            if constexpr (YE) ye += 2;
+        }
     }
 }
 
