@@ -83,12 +83,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_slot():
-    """DRAM bytes per cell-slot of the fused kernel from the committed ncu summary."""
+def ncu_traffic_per_slot(config: int):
+    """DRAM bytes per cell-slot of the fused kernel for this benchmark
+    configuration, from the committed ncu summary (None if not captured)."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get("fused_eq_kernel", {}).get("dram_bytes_per_slot")
+        return d.get("fused_eq_kernel", {}).get(f"config{config}", {}).get("dram_bytes_per_slot")
     return None
 
 
@@ -341,7 +342,7 @@ def main():
     value = whole_job_rate(res_per_step, a.steps, world, elapsed_ms)
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_step / (launch_avg_ms / 1e3) / 1e9
-    tr = ncu_traffic_per_slot()
+    tr = ncu_traffic_per_slot(a.config)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (tr * S) if tr else None, "peak_kind": peak_kind,
             "algorithmic_bytes_per_launch": bytes_per_step}
