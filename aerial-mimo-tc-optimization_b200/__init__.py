@@ -27,6 +27,7 @@ LIB_PATH = os.path.join(_HERE, "libaerial_eq.so")
 AERIAL_OK = 0
 PREC_FP16, PREC_BF16, PREC_BF16X3, PREC_FP32 = 0, 1, 2, 3
 PREC_NAMES = {"fp16": PREC_FP16, "bf16": PREC_BF16, "bf16x3": PREC_BF16X3, "fp32": PREC_FP32}
+FMT_CF32, FMT_CF16 = 0, 1          # cell storage formats (aerial_cell_desc.format)
 MAX_CELLS = 64
 
 
@@ -53,6 +54,7 @@ class CellDesc(ctypes.Structure):
         ("nLayers", ctypes.c_int),
         ("nSym", ctypes.c_int),
         ("nPamBits", ctypes.c_int),
+        ("format", ctypes.c_int),
     ]
 
 
@@ -257,7 +259,9 @@ def srs_to_channel(H, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, stream=No
 # fused chain
 # ---------------------------------------------------------------------------
 
-def cell_desc(H, Y_rx, llr_out, sigma2, nPRB, nAnt, nLayers, nSym, nPamBits, Y_eq=None) -> CellDesc:
+def cell_desc(H, Y_rx, llr_out, sigma2, nPRB, nAnt, nLayers, nSym, nPamBits, Y_eq=None, fmt=FMT_CF32) -> CellDesc:
+    """One cell-slot on device tensors.  fmt=FMT_CF16: H, Y_rx, Y_eq are complex
+    half stored as (re, im) float16 pairs and the LLRs float16."""
     d = CellDesc()
     d.H = _ptr(H).value
     d.Y_rx = _ptr(Y_rx).value
@@ -265,6 +269,7 @@ def cell_desc(H, Y_rx, llr_out, sigma2, nPRB, nAnt, nLayers, nSym, nPamBits, Y_e
     d.Y_eq = _ptr(Y_eq).value if Y_eq is not None else None
     d.sigma2 = float(sigma2)
     d.nPRB, d.nAnt, d.nLayers, d.nSym, d.nPamBits = int(nPRB), int(nAnt), int(nLayers), int(nSym), int(nPamBits)
+    d.format = int(fmt)
     return d
 
 
@@ -319,7 +324,7 @@ def _host_ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-def host_cell_desc(H, Y_rx, llr_out, sigma2, nPRB, nAnt, nLayers, nSym, nPamBits, Y_eq=None) -> CellDesc:
+def host_cell_desc(H, Y_rx, llr_out, sigma2, nPRB, nAnt, nLayers, nSym, nPamBits, Y_eq=None, fmt=FMT_CF32) -> CellDesc:
     """A cell whose buffers are host tensors, for pusch_eq_host."""
     d = CellDesc()
     d.H = _host_ptr(H).value
@@ -328,6 +333,7 @@ def host_cell_desc(H, Y_rx, llr_out, sigma2, nPRB, nAnt, nLayers, nSym, nPamBits
     d.Y_eq = _host_ptr(Y_eq).value if Y_eq is not None else None
     d.sigma2 = float(sigma2)
     d.nPRB, d.nAnt, d.nLayers, d.nSym, d.nPamBits = int(nPRB), int(nAnt), int(nLayers), int(nSym), int(nPamBits)
+    d.format = int(fmt)
     return d
 
 

@@ -54,6 +54,7 @@ struct FusedParams {
     int exactTile;   // shared exact layer tile (2, 4, 8, 16) or 0: selects the kernel
     int nStages;     // operand stages per warp of that kernel
     int exactChunks; // with an exact tile: every cell has nAnt == 16 * exactChunks (2, 4, 8), else 0
+    int fmt;         // AERIAL_FMT_* shared by every cell
     long totalGroups;
 };
 
@@ -347,6 +348,25 @@ __device__ __forceinline__ void write_llr(float* dst, const float* o) {
     }
 }
 
+// The same LLRs stored as __half (the reference's LLR storage), rounded to
+// nearest from the clamped FP32 values: 2N halves = 4N bytes per symbol.
+__device__ __forceinline__ unsigned half2_bits(float lo, float hi) {
+    const __half2 h = __floats2half2_rn(lo, hi);
+    return *reinterpret_cast<const unsigned*>(&h);
+}
+template <int N>
+__device__ __forceinline__ void write_llr_h(char* dst, const float* o) {
+    if constexpr (N == 4) {
+        __stcs(reinterpret_cast<uint4*>(dst), make_uint4(half2_bits(o[0], o[1]), half2_bits(o[2], o[3]),
+                                                          half2_bits(o[4], o[5]), half2_bits(o[6], o[7])));
+    } else if constexpr (N == 2) {
+        __stcs(reinterpret_cast<uint2*>(dst), make_uint2(half2_bits(o[0], o[1]), half2_bits(o[2], o[3])));
+    } else {
+#pragma unroll
+        for (int j = 0; j < 2 * N; j += 2) __stcs(reinterpret_cast<unsigned*>(dst + 2 * j), half2_bits(o[j], o[j + 1]));
+    }
+}
+
 // Max-log PAM demapper of the fused epilogue: the formula of llr_v1_baseline
 // (src/llr/aerial_llr_v3.cu:90-107) evaluated on a scaled axis.  With
 // r = sqrt(noiseInv), the soft estimate and the distances D_i scaled by r,
@@ -379,13 +399,22 @@ __device__ __forceinline__ void pam_llr_scaled(float pI, float pQ, const float* 
     }
 }
 
-// One symbol of a layer row: Y_eq = x / mu (when YE), LLRs of x * r / mu at lp.
-template <int N, bool YE>
-__device__ __forceinline__ void emit1(float* lp, float2* ye, float2 x, float invMu, float scl, const float* d) {
-    if constexpr (YE) __stcs(ye, make_float2(x.x * invMu, x.y * invMu));
+// One symbol of a layer row: Y_eq = x / mu (when YE), LLRs of x * r / mu at
+// lp; H16: Y_eq as half2 and LLRs as __half.
+template <int N, bool YE, bool H16>
+__device__ __forceinline__ void emit1(char* lp, char* ye, float2 x, float invMu, float scl, const float* d) {
+    if constexpr (YE) {
+        if constexpr (H16)
+            __stcs(reinterpret_cast<unsigned*>(ye), half2_bits(x.x * invMu, x.y * invMu));
+        else
+            __stcs(reinterpret_cast<float2*>(ye), make_float2(x.x * invMu, x.y * invMu));
+    }
     float o[2 * N];
     pam_llr_scaled<N>(x.x * scl, x.y * scl, d, o);
-    write_llr<N>(lp, o);
+    if constexpr (H16)
+        write_llr_h<N>(lp, o);
+    else
+        write_llr<N>(reinterpret_cast<float*>(lp), o);
 }
 
 // X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs (FP32 fma chains), then
@@ -422,10 +451,12 @@ __device__ __forceinline__ void lds2x64(uint32_t a, unsigned long long& v0, unsi
 //   P_s = sum_m (Re g_m, Re g_m) * (zr, zi),  Q_s = sum_m (Im g_m, Im g_m) * (zr, zi)
 //   X_s = (P.x - Q.y, P.y + Q.x),
 // four packed FMAs per m and symbol pair instead of eight scalar ones.
-template <int LT, int N, bool YE>
-__device__ __forceinline__ void emit_row(const float2* sZ, const float2* gi, float* lp, float2* ye, int nSym,
+template <int LT, int N, bool YE, bool H16>
+__device__ __forceinline__ void emit_row(const float2* sZ, const float2* gi, char* lp, char* ye, int nSym,
                                          float invMu, float scl, const float* d) {
     using W = WarpSmem<LT>;
+    constexpr int LB = 2 * N * (H16 ? 2 : 4);      // LLR bytes per symbol
+    constexpr int YB = H16 ? 4 : 8;                // Y_eq bytes per symbol
     if constexpr (LT <= 8) {
         unsigned long long gr[LT], gq[LT];
 #pragma unroll
@@ -454,10 +485,11 @@ __device__ __forceinline__ void emit_row(const float2* sZ, const float2* gi, flo
                 }
             }
             const float2 p0 = upk2(P0), q0 = upk2(Q0), p1 = upk2(P1), q1 = upk2(Q1);
-            emit1<N, YE>(lp, ye, make_float2(p0.x - q0.y, p0.y + q0.x), invMu, scl, d);
-            if (s + 1 < nSym) emit1<N, YE>(lp + 2 * N, ye + 1, make_float2(p1.x - q1.y, p1.y + q1.x), invMu, scl, d);
-            lp += 4 * N;
-            if constexpr (YE) ye += 2;
+            emit1<N, YE, H16>(lp, ye, make_float2(p0.x - q0.y, p0.y + q0.x), invMu, scl, d);
+            if (s + 1 < nSym)
+                emit1<N, YE, H16>(lp + LB, ye + YB, make_float2(p1.x - q1.y, p1.y + q1.x), invMu, scl, d);
+            lp += 2 * LB;
+            if constexpr (YE) ye += 2 * YB;
         }
     } else {
 #pragma unroll 1
@@ -476,31 +508,32 @@ __device__ __forceinline__ void emit_row(const float2* sZ, const float2* gi, flo
                 x1.y = fmaf(a.x, z.w, x1.y);
                 x1.y = fmaf(a.y, z.z, x1.y);
             }
-            emit1<N, YE>(lp, ye, x0, invMu, scl, d);
-            if (s + 1 < nSym) emit1<N, YE>(lp + 2 * N, ye + 1, x1, invMu, scl, d);
-            lp += 4 * N;
-            if constexpr (YE) ye += 2;
+            emit1<N, YE, H16>(lp, ye, x0, invMu, scl, d);
+            if (s + 1 < nSym) emit1<N, YE, H16>(lp + LB, ye + YB, x1, invMu, scl, d);
+            lp += 2 * LB;
+            if constexpr (YE) ye += 2 * YB;
         }
     }
 }
 
 // Lane (sc, i): layer row i of subcarrier sc.  Lanes without an output row
 // return at once.
-template <int LT, int N>
+template <int LT, int N, bool H16>
 __device__ __forceinline__ void solve_emit(const CellView& cl, const float2* sZ, const float2* gi, long sc, int i,
                                            bool out, float invMu, float nInv) {
     if (!out) return;
     const long row = sc * cl.L + i;
-    float* lp = cl.llr + row * cl.nSym * (2 * N);
+    char* lp = reinterpret_cast<char*>(cl.llr) + row * cl.nSym * (2 * N) * (H16 ? 2 : 4);
     const float r = sqrtf(nInv);
     const float scl = invMu * r;
     float d[N];
 #pragma unroll
     for (int k = 0; k < N; k++) d[k] = cl.lut.d[k] * r;
     if (cl.yeq)
-        emit_row<LT, N, true>(sZ, gi, lp, cl.yeq + row * cl.nSym, cl.nSym, invMu, scl, d);
+        emit_row<LT, N, true, H16>(sZ, gi, lp, reinterpret_cast<char*>(cl.yeq) + row * cl.nSym * (H16 ? 4 : 8),
+                                   cl.nSym, invMu, scl, d);
     else
-        emit_row<LT, N, false>(sZ, gi, lp, nullptr, cl.nSym, invMu, scl, d);
+        emit_row<LT, N, false, H16>(sZ, gi, lp, nullptr, cl.nSym, invMu, scl, d);
 }
 
 __device__ __forceinline__ float shfl_f(float v, int src, int width) {
@@ -514,7 +547,8 @@ __device__ __forceinline__ float2 shfl_c(float2 v, int src, int width) {
 // The FP32 solve of one group of GS subcarriers whose G and Z are in the
 // warp's epilogue region: LT lanes per subcarrier.
 // ---------------------------------------------------------------------------
-template <int LT, int P>
+// H16: Y_eq and LLRs are stored as half precision (the FP16 I/O format).
+template <int LT, int P, bool H16 = false>
 __device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid, int smemOff, int lane) {
     using W = WarpSmem<LT>;
     extern __shared__ float4 smem_raw[];
@@ -603,10 +637,10 @@ __device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid
     const float nInv = mu / fmaxf(t, 1e-30f);
     const bool out = scValid && real;
     switch (cl.nPam) {
-        case 1: solve_emit<LT, 1>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
-        case 2: solve_emit<LT, 2>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
-        case 3: solve_emit<LT, 3>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
-        default: solve_emit<LT, 4>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
+        case 1: solve_emit<LT, 1, H16>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
+        case 2: solve_emit<LT, 2, H16>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
+        case 3: solve_emit<LT, 3, H16>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
+        default: solve_emit<LT, 4, H16>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
     }
     __syncwarp();   // shared memory is reused by the next group
 }
@@ -1105,6 +1139,190 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_a(const __grid_constan
 }
 
 // ---------------------------------------------------------------------------
+// FP16 I/O variant (cell format AERIAL_FMT_CF16): H and Y_rx are complex
+// half (4 bytes) in HBM, Y_eq is written as complex half and the LLRs as
+// __half.  Same tile, unrolled chunks and epilogue as fused_eq_kernel_a with
+// FP16 operands; the staged samples ARE the MMA operand registers, so no
+// conversion runs between shared memory and the tensor cores.
+//
+// Stage layout (bytes): 16 channel rows of LF half2 at stride hrs16_of(LF)
+// (48 B for 8 layers, 16 B for 4), then up to 16 received rows of 64 B
+// (16 antennas) whose 8-byte antenna-pair granules are XOR-swizzled by
+// (sym & 2) << 1; both make every fragment read of a warp conflict-free.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int hrs16_of(int L) { return L == 8 ? 48 : 16; }
+
+struct ScPtrH {
+    const char* h;   // the lane's channel piece of the subcarrier's first chunk
+    const char* y;   // the lane's received piece (row lane / 4, antennas 4 (lane % 4) ..)
+    int yk;          // rows (lane / 4) and (lane / 4 + 8) below nSym: 0, 1 or 2
+};
+
+template <int LF, int NCH>
+__device__ __forceinline__ void stage_chunk_h(uint32_t st, uint32_t hLaneS, uint32_t yLaneS, const ScPtrH& s,
+                                              int j, int lane) {
+    constexpr int NP = CHUNK * LF / 4;                 // 16-byte channel pieces per chunk
+    constexpr int A = CHUNK * NCH;
+    if (NP >= 32 || lane < NP) cp_async16(st + hLaneS, s.h + j * CHUNK * LF * 4);
+    if (s.yk > 0) cp_async16(st + yLaneS, s.y + j * 64);
+    if (s.yk > 1) cp_async16(st + yLaneS + 512, s.y + j * 64 + 8 * A * 4);
+}
+
+__device__ __forceinline__ uint32_t lds32(uint32_t a) {
+    uint32_t v;
+    asm volatile("ld.shared.b32 %0, [%1];\n" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ uint2 lds64u(uint32_t a) {
+    uint2 v;
+    asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];\n" : "=r"(v.x), "=r"(v.y) : "r"(a));
+    return v;
+}
+
+// One full chunk: hb = stage + the lane's channel offset (antenna 2c, layer g),
+// yo[kk][nt] = its received-pair offsets.
+template <int LT>
+__device__ __forceinline__ void mma_stage_h(uint32_t st, uint32_t hb, const uint32_t (&yo)[2][2],
+                                            float (*gacc)[4], float (*zacc)[2][4], bool z2) {
+    constexpr int HRS = hrs16_of(LT);
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+        const uint32_t h0 = lds32(hb + 8 * kk * HRS);
+        const uint32_t h1 = lds32(hb + (8 * kk + 1) * HRS);
+        const uint2 y0 = lds64u(st + yo[kk][0]);
+        const uint2 y1 = lds64u(st + yo[kk][1]);
+        const uint32_t r0 = jrot(h0), r1 = jrot(h1);
+        mma16816<AERIAL_PREC_FP16>(gacc[0], h0, r0, h1, r1, h0, h1);
+        mma16816<AERIAL_PREC_FP16>(zacc[0][0], h0, r0, h1, r1, y0.x, y0.y);
+        if (z2) mma16816<AERIAL_PREC_FP16>(zacc[0][1], h0, r0, h1, r1, y1.x, y1.y);
+    }
+}
+
+template <int LTF, int NCH>
+__global__ void __launch_bounds__(256, 2) fused_eq_kernel_h(const __grid_constant__ FusedParams p) {
+    constexpr int NST = stages_of_a(LTF, NCH);
+    constexpr int A = CHUNK * NCH;
+    constexpr int HRS = hrs16_of(LTF);
+    constexpr long HSCB = (long)A * LTF * 4;          // channel bytes per subcarrier
+    extern __shared__ float4 smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warpsPerCta = blockDim.x >> 5;
+    const int g = lane >> 2, c = lane & 3;
+    const int warpBytes = p.epiBytes + NST * p.stageBytes;
+    const int smemOff = wib * (warpBytes / 8);
+    float2* sm = reinterpret_cast<float2*>(smem_raw) + smemOff;
+    const uint32_t stBase =
+        (uint32_t)__cvta_generic_to_shared(reinterpret_cast<char*>(smem_raw) + (long)wib * warpBytes + p.epiBytes);
+    const long gw = (long)blockIdx.x * warpsPerCta + wib;
+    const long nw = (long)gridDim.x * warpsPerCta;
+    const long total = p.totalGroups;
+    if (gw >= total) return;
+
+    const int s0 = lane >> 2, q4 = lane & 3;
+    const uint32_t hLaneS = LTF == 8 ? (lane >> 1) * HRS + (lane & 1) * 16 : lane * HRS;
+    const uint32_t yLaneS = CHUNK * HRS + s0 * 64 + ((q4 ^ (((s0 >> 1) & 1) << 1)) << 4);
+    const long yLaneB = (long)(s0 * A + 4 * q4) * 4;
+
+    auto first_sc = [&](int cell, long grp) -> ScPtrH {
+        const FusedCell& cl = p.cell[cell];
+        const long sc = (grp - cl.group0) * cl.GS;
+        ScPtrH s;
+        s.h = reinterpret_cast<const char*>(cl.H) + sc * HSCB + 16 * lane;
+        s.y = reinterpret_cast<const char*>(cl.Y) + sc * cl.nSym * A * 4 + yLaneB;
+        s.yk = (s0 < cl.nSym ? 1 : 0) + (s0 + 8 < cl.nSym ? 1 : 0);
+        return s;
+    };
+
+    long grp = gw;
+    int ci = 0;
+    while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+    int nValid, nSym;
+    bool z2;
+    uint32_t yo[2][2];
+    auto load_cell = [&]() {
+        const FusedCell& cl = p.cell[ci];
+        nValid = group_valid(cl, grp);
+        nSym = cl.nSym;
+        z2 = nSym > 8;
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) {
+                const int r = 8 * nt + g;
+                const int ra = r < nSym ? r : 0;         // rows past nSym are not staged: read row 0 instead
+                yo[kk][nt] = CHUNK * HRS + ra * 64 + (((4 * kk + c) ^ ((ra & 2) << 1)) << 3);
+            }
+    };
+    load_cell();
+    ScPtrH cur = first_sc(ci, grp);
+    const uint32_t hoff = 2 * c * HRS + 4 * g;
+
+    int pslot = 0, cslot = 0;
+#pragma unroll
+    for (int j = 0; j < NST - 1; j++) {
+        stage_chunk_h<LTF, NCH>(stBase + pslot * p.stageBytes, hLaneS, yLaneS, cur, j, lane);
+        cp_async_commit();
+        pslot = pslot == NST - 1 ? 0 : pslot + 1;
+    }
+
+    float gacc[3][4], zacc[2][2][4];
+    int q = 0;
+    while (true) {
+        ScPtrH nxt = cur;
+        bool hasNxt = true;
+        if (q + 1 < nValid) {
+            nxt.h = cur.h + HSCB;
+            nxt.y = cur.y + (long)nSym * A * 4;
+        } else {
+            const long ng = grp + nw;
+            hasNxt = ng < total;
+            if (hasNxt) {
+                int nc = ci;
+                while (nc + 1 < p.nCells && ng >= p.cell[nc + 1].group0) nc++;
+                nxt = first_sc(nc, ng);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 4; e++) gacc[0][e] = 0.f;
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) zacc[0][nt][e] = 0.f;
+#pragma unroll
+        for (int k = 0; k < NCH; k++) {
+            __syncwarp();                              // every lane is done with the slot refilled now
+            const uint32_t pst = stBase + pslot * p.stageBytes;
+            if (k + NST - 1 < NCH)
+                stage_chunk_h<LTF, NCH>(pst, hLaneS, yLaneS, cur, k + NST - 1, lane);
+            else if (hasNxt)
+                stage_chunk_h<LTF, NCH>(pst, hLaneS, yLaneS, nxt, k + NST - 1 - NCH, lane);
+            cp_async_commit();
+            pslot = pslot == NST - 1 ? 0 : pslot + 1;
+            cp_async_wait<NST - 1>();                  // this chunk's copies (own lane) have landed
+            __syncwarp();                              // ... and every lane's
+            const uint32_t st = stBase + cslot * p.stageBytes;
+            mma_stage_h<LTF>(st, st + hoff, yo, gacc, zacc, z2);
+            cslot = cslot == NST - 1 ? 0 : cslot + 1;
+        }
+        store_acc<LTF>(sm, gacc, zacc, q, g, c);
+        cur = nxt;
+        if (++q < nValid) continue;
+        __syncwarp();
+        {
+            const FusedCell& cl = p.cell[ci];
+            solve_group<LTF, AERIAL_PREC_FP16, true>(view_of(cl), (grp - cl.group0) * cl.GS, nValid, smemOff, lane);
+        }
+        q = 0;
+        grp += nw;
+        if (grp >= total) break;
+        while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+        load_cell();
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 static int layer_tile(int L) {
@@ -1170,6 +1388,10 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
     }
     p.nCells = nCells;
     p.totalGroups = g0;
+    p.fmt = cells[0].format;
+    for (int i = 0; i < nCells; i++)
+        if (cells[i].format != p.fmt || (p.fmt != AERIAL_FMT_CF32 && p.fmt != AERIAL_FMT_CF16))
+            return AERIAL_ERR_INVALID_ARG;
     p.epiBytes = epi_bytes_of(p);
     p.stageBytes = stage_bytes_of(p);
     p.exactTile = exact_tile(p);
@@ -1181,6 +1403,17 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
         bool same = p.exactTile <= 8 && (a == 32 || a == 64 || a == 128);
         for (int i = 1; i < nCells && same; i++) same = p.cell[i].A == a;
         if (same) p.exactChunks = a / CHUNK;
+    }
+    if (p.fmt == AERIAL_FMT_CF16) {
+        // half-format cells run the FP16 I/O kernel: exact 4- or 8-layer
+        // tile, 32 / 64 / 128 antennas, 16-byte aligned H and Y_rx
+        if ((p.exactTile != 4 && p.exactTile != 8) || !p.exactChunks) return AERIAL_ERR_UNSUPPORTED;
+        int b = 0;
+        for (int i = 0; i < nCells; i++) {
+            const int v = CHUNK * hrs16_of(p.cell[i].L) + 64 * p.cell[i].nSym;
+            b = v > b ? v : b;
+        }
+        p.stageBytes = (b + 15) & ~15;
     }
     p.nStages = p.exactChunks ? stages_of_a(p.exactTile, p.exactChunks) : stages_of(p.exactTile);
     warpBytes = p.epiBytes + p.nStages * p.stageBytes;
@@ -1287,8 +1520,42 @@ static int plan_an(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPl
     }
 }
 
+template <int LTF, int NCH>
+static int plan_h(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
+    static int configured = 0;
+    const int bytes = sh.warps * warpBytes;
+    if (bytes > 48 * 1024 && bytes > configured) {
+        cudaError_t e =
+            cudaFuncSetAttribute(fused_eq_kernel_h<LTF, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return (int)e;
+        configured = bytes;
+    }
+    long need = (p.totalGroups + sh.warps - 1) / sh.warps;
+    long grid = (long)sm_count() * sh.ctasPerSm;
+    if (grid > need) grid = need;
+    if (grid < 1) grid = 1;
+    out.func = reinterpret_cast<const void*>(fused_eq_kernel_h<LTF, NCH>);
+    out.grid = dim3((unsigned)grid);
+    out.block = dim3(sh.warps * 32);
+    out.smem = bytes;
+    return AERIAL_OK;
+}
+
+template <int LTF>
+static int plan_hn(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
+    switch (p.exactChunks) {
+        case 2: return plan_h<LTF, 2>(p, warpBytes, sh, out);
+        case 4: return plan_h<LTF, 4>(p, warpBytes, sh, out);
+        default: return plan_h<LTF, 8>(p, warpBytes, sh, out);
+    }
+}
+
 template <int P>
 static int plan_p(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
+    if (p.fmt == AERIAL_FMT_CF16) {
+        if (P != AERIAL_PREC_FP16) return AERIAL_ERR_UNSUPPORTED;
+        return p.exactTile == 4 ? plan_hn<4>(p, warpBytes, sh, out) : plan_hn<8>(p, warpBytes, sh, out);
+    }
     if (p.exactChunks) {
         switch (p.exactTile) {
             case 2: return plan_an<P, 2>(p, warpBytes, sh, out);
@@ -1500,8 +1767,8 @@ extern "C" int aerial_eq_graph_update(aerial_eq_graph* g, const aerial_cell_desc
     for (int i = 0; i < nCells; i++) {
         const FusedCell &a = np.cell[i], &b = g->params.cell[i];
         if (a.nSC != b.nSC || a.A != b.A || a.L != b.L || a.nSym != b.nSym || a.nPam != b.nPam ||
-            a.vecH != b.vecH || a.vecY != b.vecY)
-            return AERIAL_ERR_UNSUPPORTED;      // a new shape needs a new graph
+            a.vecH != b.vecH || a.vecY != b.vecY || np.fmt != g->params.fmt)
+            return AERIAL_ERR_UNSUPPORTED;      // a new shape or format needs a new graph
     }
     g->params = np;
     void* args[] = {&g->params};
@@ -1558,6 +1825,16 @@ static int prepare_an() {
     return s;
 }
 
+template <int LTF, int NCH>
+static int prepare_h() {
+    cudaFuncAttributes at;
+    cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_h<LTF, NCH>);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fused_eq_kernel_h<LTF, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 220 * 1024);
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
 template <int P>
 static int prepare_p() {
     int s = prepare_an<P, 2>();
@@ -1574,6 +1851,12 @@ static int prepare_p() {
 
 int prepare_fused_kernels() {
     int s = prepare_p<AERIAL_PREC_FP16>();
+    if (!s) s = prepare_h<4, 2>();
+    if (!s) s = prepare_h<4, 4>();
+    if (!s) s = prepare_h<4, 8>();
+    if (!s) s = prepare_h<8, 2>();
+    if (!s) s = prepare_h<8, 4>();
+    if (!s) s = prepare_h<8, 8>();
     if (!s) s = prepare_p<AERIAL_PREC_BF16>();
     if (!s) s = prepare_p<AERIAL_PREC_BF16X3>();
     return s;

@@ -34,13 +34,16 @@ struct CellBytes {
     size_t h, y, llr, yeq;
 };
 
+// Complex samples are 8 bytes and LLRs 4 in AERIAL_FMT_CF32, half that in
+// AERIAL_FMT_CF16.
 static CellBytes cell_bytes(const aerial_cell_desc& c) {
     const size_t nSC = (size_t)c.nPRB * 12;
+    const size_t cs = c.format == AERIAL_FMT_CF16 ? 4 : 8;
     CellBytes b;
-    b.h = nSC * c.nAnt * c.nLayers * 8;
-    b.y = nSC * c.nSym * c.nAnt * 8;
-    b.llr = nSC * c.nLayers * c.nSym * 2 * c.nPamBits * 4;
-    b.yeq = c.Y_eq ? nSC * c.nLayers * c.nSym * 8 : 0;
+    b.h = nSC * c.nAnt * c.nLayers * cs;
+    b.y = nSC * c.nSym * c.nAnt * cs;
+    b.llr = nSC * c.nLayers * c.nSym * 2 * c.nPamBits * (cs / 2);
+    b.yeq = c.Y_eq ? nSC * c.nLayers * c.nSym * cs : 0;
     return b;
 }
 
@@ -54,7 +57,7 @@ static size_t cell_footprint(const aerial_cell_desc& c) {
 static bool host_cell_ok(const aerial_cell_desc& c) {
     return c.H && c.Y_rx && c.llr && c.nPRB >= 1 && c.nAnt >= 1 && c.nAnt <= AERIAL_MAX_ANTS && c.nLayers >= 1 &&
            c.nLayers <= AERIAL_MAX_LAYERS && c.nSym >= 1 && c.nSym <= AERIAL_MAX_SYMS && c.nPamBits >= 1 &&
-           c.nPamBits <= 4 && c.sigma2 >= 0.f;
+           c.nPamBits <= 4 && c.sigma2 >= 0.f && (c.format == AERIAL_FMT_CF32 || c.format == AERIAL_FMT_CF16);
 }
 
 // Cells per batch: the caller's value, or the smallest count whose input

@@ -300,6 +300,7 @@ extern "C" int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, 
         int nSC = c.nPRB * 12;
         if (!c.H || !c.Y_rx || !c.llr || c.nPamBits < 1 || c.nPamBits > 4 || !shape_ok(nSC, c.nSym, c.nLayers, c.nAnt))
             return AERIAL_ERR_INVALID_ARG;
+        if (c.format != AERIAL_FMT_CF32) return AERIAL_ERR_UNSUPPORTED;   // the FP32 chain reads complex64 only
         if (plain_ws_cell(c) > wsBytes) return AERIAL_ERR_INVALID_ARG;
         auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
         char* p = (char*)workspace;

@@ -143,7 +143,19 @@ int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, const aerial_ch
 /* Y_eq stay on chip, only LLRs (and optionally Y_eq) are written.           */
 /* ------------------------------------------------------------------------ */
 
-/* One cell-slot.  nSC = 12 * nPRB.  Y_eq may be NULL. */
+/* Storage format of a cell's buffers (aerial_cell_desc.format).
+ *  AERIAL_FMT_CF32: H, Y_rx, Y_eq complex float32 (aerial_cf32), LLRs float32
+ *                   -- the drop-in layout.
+ *  AERIAL_FMT_CF16: H, Y_rx, Y_eq complex half (aerial_ch2), LLRs __half --
+ *                   half the bytes; the LLR storage of the reference's
+ *                   demapper (src/llr/aerial_llr_v3.cu:84-108).  Supported for
+ *                   launches whose cells all have nLayers 4 or 8, nAnt 32, 64
+ *                   or 128, with FP16 operands (else AERIAL_ERR_UNSUPPORTED). */
+enum { AERIAL_FMT_CF32 = 0, AERIAL_FMT_CF16 = 1 };
+
+/* One cell-slot.  nSC = 12 * nPRB.  Y_eq may be NULL.  Pointer types name
+ * the AERIAL_FMT_CF32 layout; with AERIAL_FMT_CF16 they point at the half
+ * formats of the same shapes.  All cells of one launch share a format. */
 typedef struct {
     const aerial_cf32* H;      /* [nSC][nAnt][nLayers] */
     const aerial_cf32* Y_rx;   /* [nSC][nSym][nAnt] */
@@ -151,6 +163,7 @@ typedef struct {
     aerial_cf32* Y_eq;         /* optional [nSC][nLayers][nSym] (unbiased) */
     float sigma2;              /* noise variance per receive antenna */
     int nPRB, nAnt, nLayers, nSym, nPamBits;
+    int format;                /* AERIAL_FMT_*; 0 (zero-initialised) = CF32 */
 } aerial_cell_desc;
 
 /* Operand precision of the tensor-core products. */

@@ -1,0 +1,115 @@
+"""GPU tests of the FP16 I/O cell format (AERIAL_FMT_CF16): H, Y_rx and Y_eq
+as complex half, LLRs as __half.
+
+On inputs that are exactly representable in half precision the FP16 I/O
+kernel and the complex64 layout with FP16 operands feed identical operands to
+identical tensor-core tiles and the same FP32 epilogue, so the half outputs
+must equal the complex64 path's outputs rounded to half, bit for bit."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from test_gpu_fused import check_against_fp64
+
+pytestmark = pytest.mark.gpu
+
+
+def half_pairs(z):
+    """complex64 tensor -> contiguous float16 (re, im) pairs."""
+    return torch.view_as_real(z).to(torch.float16).contiguous()
+
+
+def run_pair(aeq, cells, cuda, want_yeq=True):
+    """The same half-representable cells through both formats."""
+    d32, d16, out32, out16 = [], [], [], []
+    for c in cells:
+        H16, Y16 = half_pairs(c.H).to(cuda), half_pairs(c.Y).to(cuda)
+        H32 = torch.view_as_complex(H16.float()).contiguous()
+        Y32 = torch.view_as_complex(Y16.float()).contiguous()
+        l32 = torch.full((c.llr_numel,), float("nan"), dtype=torch.float32, device=cuda)
+        l16 = torch.full((c.llr_numel,), float("nan"), dtype=torch.float16, device=cuda)
+        n = c.nSC * c.nLayers * c.nSym
+        y32 = torch.full((n,), float("nan"), dtype=torch.complex64, device=cuda) if want_yeq else None
+        y16 = torch.full((n, 2), float("nan"), dtype=torch.float16, device=cuda) if want_yeq else None
+        d32.append(aeq.cell_desc(H32, Y32, l32, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, Y_eq=y32))
+        d16.append(aeq.cell_desc(H16, Y16, l16, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, Y_eq=y16,
+                                 fmt=aeq.FMT_CF16))
+        out32.append((H32, Y32, l32, y32))
+        out16.append((H16, Y16, l16, y16))
+    t = aeq.make_tuning("fp16")
+    aeq.pusch_eq_fused(d32, t)
+    aeq.pusch_eq_fused(d16, t)
+    torch.cuda.synchronize()
+    return out32, out16
+
+
+@pytest.mark.parametrize("L", [4, 8])
+@pytest.mark.parametrize("A", [32, 64, 128])
+def test_fp16_io_equals_complex64_path_rounded(aeq, wl, cuda, L, A):
+    cells = [wl.make_cell(2, A, L, 11, 256, 25.0, seed=600 + A + L),
+             wl.make_cell(1, A, L, 5, 16, 20.0, seed=700 + A + L),
+             wl.make_cell(3, A, L, 14, 64, 25.0, seed=800 + A + L)]
+    out32, out16 = run_pair(aeq, cells, cuda)
+    for (_, _, l32, y32), (_, _, l16, y16) in zip(out32, out16):
+        assert torch.isfinite(l16.float()).all()
+        assert torch.equal(l16, l32.to(torch.float16))
+        assert torch.equal(y16, torch.view_as_real(y32).to(torch.float16))
+
+
+def test_fp16_io_vs_fp64(aeq, wl, orc, cuda):
+    """The headline cell in FP16 I/O against the FP64 model of its own
+    (half-rounded) inputs, at the FP16 bar."""
+    c = wl.config_cell(2, seed=31)
+    out32, out16 = run_pair(aeq, [c], cuda)
+    H16, Y16, l16, y16 = out16[0]
+    hc = type(c)(**{**c.__dict__, "H": torch.view_as_complex(H16.float()).cpu(),
+                    "Y": torch.view_as_complex(Y16.float()).cpu()})
+    llr = l16.float().cpu().numpy()
+    yeq = torch.view_as_complex(y16.float()).cpu().numpy()
+    check_against_fp64(orc, hc, llr, yeq, -45.0)
+
+
+def test_fp16_io_host_pipeline(aeq, wl, cuda):
+    """Host half buffers through aerial_pusch_eq_host equal the resident launch."""
+    cells = [wl.make_cell(2, 64, 8, 11, 256, 25.0, seed=900 + k) for k in range(5)]
+    _, out16 = run_pair(aeq, cells, cuda, want_yeq=False)
+    hd, hl, keep = [], [], []
+    for c, (H16, Y16, _, _) in zip(cells, out16):
+        hH, hY = H16.cpu().pin_memory(), Y16.cpu().pin_memory()
+        l = torch.full((c.llr_numel,), float("nan"), dtype=torch.float16).pin_memory()
+        keep += [hH, hY]
+        hl.append(l)
+        hd.append(aeq.host_cell_desc(hH, hY, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits,
+                                     fmt=aeq.FMT_CF16))
+    ws = torch.empty(aeq.pusch_eq_host_workspace(hd, 2), dtype=torch.uint8, device=cuda)
+    aeq.pusch_eq_host(hd, ws, aeq.make_tuning("fp16"), 2)
+    torch.cuda.synchronize()
+    for l, (_, _, l16, _) in zip(hl, out16):
+        assert torch.equal(l, l16.cpu())
+
+
+def test_fp16_io_unsupported_cases(aeq, wl, cuda):
+    def desc(c, fmt=1):
+        H16, Y16 = half_pairs(c.H).to(cuda), half_pairs(c.Y).to(cuda)
+        l16 = torch.empty(c.llr_numel, dtype=torch.float16, device=cuda)
+        return (H16, Y16, l16), aeq.cell_desc(H16, Y16, l16, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits,
+                                             fmt=fmt)
+    k1, d_l2 = desc(wl.make_cell(1, 32, 2, 11, 16, 20.0, seed=1))          # 2 layers
+    k2, d_a48 = desc(wl.make_cell(1, 48, 8, 11, 16, 20.0, seed=2))         # 48 antennas
+    k3, d_ok = desc(wl.make_cell(1, 64, 8, 11, 16, 20.0, seed=3))
+    for d in (d_l2, d_a48):
+        with pytest.raises(aeq.AerialError):
+            aeq.pusch_eq_fused([d], aeq.make_tuning("fp16"))
+    with pytest.raises(aeq.AerialError):                                    # FP16 operands only
+        aeq.pusch_eq_fused([d_ok], aeq.make_tuning("bf16x3"))
+    c = wl.make_cell(1, 64, 8, 11, 16, 20.0, seed=4)
+    H, Y = c.H.to(cuda), c.Y.to(cuda)
+    l = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+    d32 = aeq.cell_desc(H, Y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+    with pytest.raises(aeq.AerialError):                                    # one format per launch
+        aeq.pusch_eq_fused([d32, d_ok], aeq.make_tuning("fp16"))
+    ws = torch.empty(aeq.pusch_eq_plain_workspace([d_ok]), dtype=torch.uint8, device=cuda)
+    with pytest.raises(aeq.AerialError):                                    # the FP32 chain reads complex64 only
+        aeq.pusch_eq_plain([d_ok], ws)
