@@ -64,6 +64,9 @@ def parse():
                     help="benchmark configuration (2 = the headline 100 MHz cell)")
     ap.add_argument("--slots", type=int, default=0, help="cell-slots per step per GPU (0 = the config's default)")
     ap.add_argument("--precision", default="", choices=["", "fp16", "bf16", "bf16x3"])
+    ap.add_argument("--io", default="cf32", choices=["cf32", "fp16"],
+                    help="storage of H / Y_rx / LLRs: cf32 = the drop-in complex64 layout (default); fp16 = complex "
+                         "half in, __half LLRs out (configs 1 and 2, FP16 operands), reported as its own line")
     ap.add_argument("--duration", type=float, default=1.0, help="serving run length in seconds (config 5)")
     ap.add_argument("--window-us", type=float, default=0.0, help="serving batching window (config 5; 0 = launch at once)")
     ap.add_argument("--min-batch", type=int, default=0, help="serving minimum batch before the window ends")
@@ -287,17 +290,29 @@ def main():
         return
     S = a.slots
     cells = build_cells(wl, a.config, S, rank, dev)
-    llrs = [torch.empty(c.llr_numel, dtype=torch.float32, device=dev) for c in cells]
-    descs = [aeq.cell_desc(c.H, c.Y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+    half = a.io == "fp16"
+    if half:
+        if a.config not in (1, 2) or a.precision != "fp16":
+            raise SystemExit("--io fp16 runs configurations 1 and 2 with fp16 operands")
+        a.no_extras = True          # the extras run the complex64 plain chain
+        # the same slots stored as complex half; the complex64 copies are dropped
+        for c in cells:
+            c.H = torch.view_as_real(c.H).to(torch.float16).contiguous()
+            c.Y = torch.view_as_real(c.Y).to(torch.float16).contiguous()
+        torch.cuda.empty_cache()
+    fmt = aeq.FMT_CF16 if half else aeq.FMT_CF32
+    ldt = torch.float16 if half else torch.float32
+    llrs = [torch.empty(c.llr_numel, dtype=ldt, device=dev) for c in cells]
+    descs = [aeq.cell_desc(c.H, c.Y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, fmt=fmt)
              for c, l in zip(cells, llrs)]
     tun = aeq.make_tuning(a.precision)
     if os.environ.get("AERIAL_AUTOTUNE", "1") == "1":
         tun, _ = aeq.autotune(descs, a.precision)
     stream = torch.cuda.current_stream()
     res_per_step = sum(c.n_re for c in cells)
-    bytes_per_step = sum(c.algorithmic_bytes() for c in cells)
-    in_bytes_per_step = sum(8 * (c.H.numel() + c.Y.numel()) for c in cells)
-    out_bytes_per_step = sum(4 * c.llr_numel for c in cells)
+    bytes_per_step = sum(c.algorithmic_bytes() for c in cells) // (2 if half else 1)
+    in_bytes_per_step = sum(c.H.numel() * c.H.element_size() + c.Y.numel() * c.Y.element_size() for c in cells)
+    out_bytes_per_step = sum(l.numel() * l.element_size() for l in llrs)
 
     def step():
         aeq.pusch_eq_fused(descs, tun, stream)
@@ -342,7 +357,7 @@ def main():
     value = whole_job_rate(res_per_step, a.steps, world, elapsed_ms)
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_step / (launch_avg_ms / 1e3) / 1e9
-    tr = ncu_traffic_per_slot(a.config)
+    tr = None if half else ncu_traffic_per_slot(a.config)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": (tr * S) if tr else None, "peak_kind": peak_kind,
             "algorithmic_bytes_per_launch": bytes_per_step}
@@ -352,8 +367,8 @@ def main():
     if not a.no_e2e:
         hH = [c.H.cpu().pin_memory() for c in cells]
         hY = [c.Y.cpu().pin_memory() for c in cells]
-        hL = [torch.empty(c.llr_numel, dtype=torch.float32).pin_memory() for c in cells]
-        hd = [aeq.host_cell_desc(h, y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+        hL = [torch.empty(c.llr_numel, dtype=ldt).pin_memory() for c in cells]
+        hd = [aeq.host_cell_desc(h, y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, fmt=fmt)
               for c, h, y, l in zip(cells, hH, hY, hL)]
         ws = torch.empty(aeq.pusch_eq_host_workspace(hd), dtype=torch.uint8, device=dev)
 
@@ -406,15 +421,18 @@ def main():
     if rank != 0:
         return
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "metric": METRIC + (" with FP16 I/O" if half else ""), "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": a.precision + " operands / fp32 accumulate and solve", "data": "synthetic (seeded, generated on device)",
+        "dtype": a.precision + " operands / fp32 accumulate and solve" + ("; complex-half in, __half LLRs out"
+                                                                           if half else ""),
+        "data": "synthetic (seeded, generated on device)",
         "config": {"workload": WORKLOADS[a.config], "benchmark_config": a.config, "cells_per_step": len(cells),
                    "slots_per_step_per_gpu": S, "res_per_step_per_gpu": res_per_step,
                    "l2": (f"inputs larger than L2 ({bytes_per_step / 1e6:.0f} MB touched per step per GPU)"
                           if flush is None else
                           f"L2 flushed before each timed launch ({bytes_per_step / 1e6:.0f} MB per step)"),
-                   "precision": a.precision, "tuning": {"warps_per_cta": tun.warps_per_cta,
+                   "precision": a.precision, "io": a.io, "tuning": {"warps_per_cta": tun.warps_per_cta,
                                                          "ctas_per_sm": tun.ctas_per_sm},
                    "parallelism": f"independent cell-slots per GPU x{world}"},
         "roofline": roof,
