@@ -1595,6 +1595,9 @@ int launch_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, 
 }
 
 // Resolve precision and launch shape from an optional tuning struct.
+// A shape tuned on one batch may be applied to another whose cells need more
+// shared memory per warp (a host-pipeline sub-batch, say): its CTAs per SM
+// are then reduced to what fits instead of failing the launch.
 static void resolve_tuning(const aerial_tuning* tuning, int warpBytes, int& prec, LaunchShape& sh) {
     sh = default_shape(warpBytes);
     prec = AERIAL_PREC_FP16;
@@ -1602,6 +1605,10 @@ static void resolve_tuning(const aerial_tuning* tuning, int warpBytes, int& prec
         prec = tuning->precision;
         if (tuning->warps_per_cta) sh.warps = tuning->warps_per_cta;
         if (tuning->ctas_per_sm) sh.ctasPerSm = tuning->ctas_per_sm;
+        if (sh.warps >= 1 && sh.ctasPerSm > 1 && (long)sh.warps * warpBytes * sh.ctasPerSm > kSmemPerSm) {
+            const int k = kSmemPerSm / (sh.warps * warpBytes);
+            sh.ctasPerSm = k >= 1 ? k : 1;
+        }
     }
 }
 

@@ -405,6 +405,7 @@ def main():
         extras = bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a)
         if a.config == 4:
             extras["tiles"] = compare_tiles(aeq, descs, tun, stream, a, flush)
+            extras["per_cell_streams_vs_batched"] = compare_streams(aeq, descs, tun, a, flush)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         from oracle import oracle as orc
 
@@ -562,6 +563,73 @@ def compare_tiles(aeq, descs, tuned, stream, a, flush):
     fixed = aeq.make_tuning(a.precision)
     return {"autotuned_us": timed(tuned), "fixed_default_us": timed(fixed),
             "autotuned_shape": {"warps_per_cta": tuned.warps_per_cta, "ctas_per_sm": tuned.ctas_per_sm}}
+
+
+def compare_streams(aeq, descs, tuned, a, flush):
+    """Configuration 4, the reference's multi-cell stream study
+    (src/multicell_contention.cu:205-235) restated for this path: the 16 cells
+    as one launch per cell on 16 concurrent streams (per-cell latency and
+    makespan, against each cell alone) versus all cells in one persistent
+    batched launch."""
+    import torch
+
+    n = len(descs)
+    streams = [torch.cuda.Stream() for _ in range(n)]
+    main = torch.cuda.current_stream()
+    reps = 10
+
+    def med(v):
+        v = sorted(v)
+        return v[len(v) // 2]
+
+    alone = []
+    for d in descs:
+        t = []
+        for r in range(reps):
+            if flush is not None:
+                flush.fill_(float(r))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(main)
+            aeq.pusch_eq_fused([d], tuned, main)
+            e1.record(main)
+            torch.cuda.synchronize()
+            t.append(1e3 * e0.elapsed_time(e1))
+        alone.append(med(t))
+    per_cell, span = [[] for _ in range(n)], []
+    for r in range(reps):
+        if flush is not None:
+            flush.fill_(float(r))
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g0.record(main)
+        ev = []
+        for d, st in zip(descs, streams):
+            st.wait_event(g0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            aeq.pusch_eq_fused([d], tuned, st)
+            e1.record(st)
+            ev.append((e0, e1))
+        torch.cuda.synchronize()
+        for c, (e0, e1) in enumerate(ev):
+            per_cell[c].append(1e3 * e0.elapsed_time(e1))
+        span.append(max(1e3 * g0.elapsed_time(e1) for _, e1 in ev))
+    batched = []
+    for r in range(reps):
+        if flush is not None:
+            flush.fill_(float(r))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        aeq.pusch_eq_fused(descs, tuned, main)
+        e1.record(main)
+        torch.cuda.synchronize()
+        batched.append(1e3 * e0.elapsed_time(e1))
+    lat = [med(v) for v in per_cell]
+    return {"cells": n, "alone_us_mean": sum(alone) / n,
+            "streams_per_cell_latency_us_mean": sum(lat) / n,
+            "streams_mean_degradation_vs_alone": sum(l / al for l, al in zip(lat, alone)) / n,
+            "streams_makespan_us": med(span), "batched_launch_us": med(batched),
+            "makespan_ratio_streams_over_batched": med(span) / med(batched)}
 
 
 def bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a):

@@ -174,7 +174,9 @@ enum {
     AERIAL_PREC_FP32 = 3       /* FP32 CUDA-core products (no tensor cores) */
 };
 
-/* Launch shape; zero fields take the autotuned / default value. */
+/* Launch shape; zero fields take the autotuned / default value.  A shape
+ * whose CTAs per SM do not fit the launch's shared memory (e.g. one tuned on
+ * a different batch) runs with the CTAs per SM that fit. */
 typedef struct {
     int precision;             /* AERIAL_PREC_* */
     int warps_per_cta;         /* 0 = default */

@@ -216,3 +216,13 @@ def test_fused_exact_antenna_kernels(aeq, wl, orc, cuda, L, A):
         np.testing.assert_array_equal(exact[k][0], mixed[k][0])
         np.testing.assert_array_equal(exact[k][1], mixed[k][1])
         check_against_fp64(orc, c, exact[k][0], exact[k][1], -60.0)
+
+
+def test_tuned_shape_that_does_not_fit_is_reduced(aeq, wl, cuda):
+    """A shape tuned on a light batch (2 warps x 8 CTAs) applied to a 16-layer
+    cell whose warps need far more shared memory runs with the CTAs per SM
+    that fit, and gives the default shape's results."""
+    c = wl.make_cell(1, 128, 16, 14, 256, 30.0, seed=61)
+    ref = run_fused(aeq, [c], cuda, "fp16")[0]
+    got = run_fused(aeq, [c], cuda, "fp16", tuning=aeq.make_tuning("fp16", 2, 8))[0]
+    np.testing.assert_array_equal(got[0], ref[0])
