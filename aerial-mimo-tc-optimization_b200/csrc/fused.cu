@@ -371,29 +371,34 @@ __device__ __forceinline__ void write_llr_h(char* dst, const float* o) {
 // (src/llr/aerial_llr_v3.cu:90-107) evaluated on a scaled axis.  With
 // r = sqrt(noiseInv), the soft estimate and the distances D_i scaled by r,
 //   (pm_i - t^2) * noiseInv = (r m_i)^2 - (r t)^2,
-// so each LLR is one fma(-t', t', m'^2) with no noise multiply.  The +-65504
-// clamp is applied to the magnitude and the soft bit's sign copied in with
-// one bit operation.  It differs from the reference's rounding by a few FP32
-// ulps of each LLR (the plain chain keeps the bit-exact form).
+// so each LLR is one fma(-t', t', m'^2) with no noise multiply.  For the last
+// soft bit m = D + a and t = a - D with the same a, so m^2 - t^2 = 4 D a
+// exactly: one multiply (and QPSK is that term alone).  The +-65504 clamp is
+// applied to the magnitude and the soft bit's sign copied in with one bit
+// operation.  It differs from the reference's rounding by a few FP32 ulps of
+// each LLR (the plain chain keeps the bit-exact form).
 template <int N>
 __device__ __forceinline__ void pam_llr_scaled(float pI, float pQ, const float* d, float* out) {
     const float dist = d[N - 1];
+    const float dist4 = 4.f * dist;
 #pragma unroll
     for (int iq = 0; iq < 2; iq++) {
         float sb = iq ? pQ : pI;
         float pm[N], sg[N];
 #pragma unroll
-        for (int i = 0; i < N; i++) {
+        for (int i = 0; i < N - 1; i++) {
             const float a = fabsf(sb);
             const float m = dist + a;
             pm[i] = m * m;
             sg[i] = sb;
-            if (i < N - 1) sb = d[i] - a;
+            sb = d[i] - a;
         }
-        const float t = fabsf(sb) - dist;
+        sg[N - 1] = sb;
+        const float aL = fabsf(sb);
+        const float t = aL - dist;
 #pragma unroll
         for (int i = 0; i < N; i++) {
-            const float v = fminf(fmaf(-t, t, pm[i]), 65504.f);
+            const float v = fminf(i == N - 1 ? dist4 * aL : fmaf(-t, t, pm[i]), 65504.f);
             out[2 * i + iq] = __int_as_float(__float_as_int(v) ^ (__float_as_int(sg[i]) & 0x80000000));
         }
     }
