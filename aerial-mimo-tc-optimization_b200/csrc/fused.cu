@@ -32,6 +32,17 @@ namespace aeq {
 
 constexpr int kMaxCells = AERIAL_MAX_CELLS;
 
+// Subcarriers per group: 32 / LT fills every lane of the solve, but for the
+// 1-, 2- and 4-layer tiles that makes one warp's operand pass over a group
+// 32, 16 or 8 subcarriers long, and a small uneven batch then waits on those
+// few long groups.  Capping the group at 4 keeps groups short (the uneven
+// 16-cell batch: 90 -> 74 us; large batches unchanged); the idle solve lanes
+// cost little at those tile sizes.
+#ifndef AEQ_MAX_GROUP_SC
+#define AEQ_MAX_GROUP_SC 4
+#endif
+constexpr int kMaxGroupSC = AEQ_MAX_GROUP_SC;
+
 struct FusedCell {
     const float2* H;
     const float2* Y;
@@ -40,7 +51,7 @@ struct FusedCell {
     long group0;     // first global group index of this cell
     float sigma2;
     int nSC, A, L, nSym, nPam, LT, vecY, vecH, lgHalfL;
-    int GS;          // subcarriers per group = 32 / LT
+    int GS;          // subcarriers per group = min(32 / LT, kMaxGroupSC)
     int nChunk;      // 16-antenna chunks per subcarrier
     int hrs;         // staged channel-row stride (bytes)
     PamLut lut;
@@ -1384,12 +1395,12 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
         }
         f.lut = pam_lut(c.nPamBits);
         f.group0 = g0;
-        f.GS = 32 / f.LT;
+        f.GS = 32 / f.LT < kMaxGroupSC ? 32 / f.LT : kMaxGroupSC;
         f.nChunk = (c.nAnt + CHUNK - 1) / CHUNK;
         f.hrs = hrs_of(c.nLayers);
         // LLR rows of 2*nPam floats are written as float4 for nPam 2/4: need 16 B alignment
         if ((c.nPamBits == 2 || c.nPamBits == 4) && ((uintptr_t)c.llr & 15)) return AERIAL_ERR_INVALID_ARG;
-        g0 += (nSC + (32 / f.LT) - 1) / (32 / f.LT);
+        g0 += (nSC + f.GS - 1) / f.GS;
     }
     p.nCells = nCells;
     p.totalGroups = g0;
