@@ -824,6 +824,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     int pci = 0;
     while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
     int pq = 0, pch = 0, pslot = 0, pValid, pNChunk, pNFull, pYStep, pYLane, pYk;
+    int pExact = 0;                                       // generic kernel: this cell's exact tile, or 0
     long pHsc, pYsc;
     const float2* phs;
     const float2* pys;
@@ -841,6 +842,16 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
         pYStep = 4 * A;                                   // received rows s and s + 4
         pYLane = (lane >> 3) * A + 2 * (lane & 7);        // this lane's first piece
         pYk = min(4, max(0, (nSym - (lane >> 3) + 3) >> 2));
+        if constexpr (LTF == 0) {
+            // a cell whose layers fill its tile stages full chunks like the
+            // exact-tile kernels, with this cell's lane offsets
+            pExact = (cl.L == cl.LT && cl.LT >= 2 && cl.vecH && cl.vecY) ? cl.LT : 0;
+            if (pExact) {
+                const int half = cl.L / 2;
+                hLaneS = (lane / half) * cl.hrs + (lane % half) * 16;
+                yLaneS = CHUNK * cl.hrs + (lane >> 3) * 128 + (((lane & 7) ^ (((lane >> 3) & 1) << 2)) << 4);
+            }
+        }
     };
     load_pcell();
     auto produce = [&]() {
@@ -853,7 +864,18 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
                 else
                     stage_item_exact<LTF>(p.cell[pci], phs, pys, pch, st, lane);
             } else {
-                stage_item(p.cell[pci], phs, pys, pch, st, lane);
+                if (pExact && pch < pNFull) {
+                    const float2* hsrc = phs + CHUNK * pch * pExact;
+                    const float2* ysrc = pys + CHUNK * pch + pYLane;
+                    switch (pExact) {
+                        case 2: stage_full<2>(st, hLaneS, yLaneS, hsrc, ysrc, pYStep, pYk, lane); break;
+                        case 4: stage_full<4>(st, hLaneS, yLaneS, hsrc, ysrc, pYStep, pYk, lane); break;
+                        case 8: stage_full<8>(st, hLaneS, yLaneS, hsrc, ysrc, pYStep, pYk, lane); break;
+                        default: stage_full<16>(st, hLaneS, yLaneS, hsrc, ysrc, pYStep, pYk, lane); break;
+                    }
+                } else {
+                    stage_item(p.cell[pci], phs, pys, pch, st, lane);
+                }
             }
             if (++pch == pNChunk) {
                 pch = 0;
@@ -881,6 +903,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     int ci = 0;
     while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
     int q = 0, ch = 0, cslot = 0, nValid, cNChunk, cNFull, cA, cL, cLT, cHrs;
+    bool cExact = false;                                  // generic kernel: L fills the tile, aligned rows
     bool z2;
     uint32_t yo[2][2];
     auto load_ccell = [&]() {
@@ -892,6 +915,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
         cL = cl.L;
         cLT = LTF != 0 ? LTF : cl.LT;
         cHrs = cl.hrs;
+        cExact = cl.L == cl.LT && cl.LT >= 2 && cl.vecH && cl.vecY;
         z2 = cl.nSym > 8;
         const uint32_t ys = CHUNK * (LTF != 0 ? hrs_of(LTF) : cl.hrs);
 #pragma unroll
@@ -930,7 +954,14 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
                 mma_stage<LTF, P, true, false>(st, hrs_of(LTF), cA - CHUNK * ch, LTF, yo, gacc, zacc, z2, g, c);
         } else {
             const int nRows = min(CHUNK, cA - CHUNK * ch);
-            switch (cLT) {
+            if (cExact && nRows == CHUNK) {
+                switch (cLT) {
+                    case 2: mma_stage<2, P, true, true>(st, cHrs, CHUNK, 2, yo, gacc, zacc, z2, g, c); break;
+                    case 4: mma_stage<4, P, true, true>(st, cHrs, CHUNK, 4, yo, gacc, zacc, z2, g, c); break;
+                    case 8: mma_stage<8, P, true, true>(st, cHrs, CHUNK, 8, yo, gacc, zacc, z2, g, c); break;
+                    default: mma_stage<16, P, true, true>(st, cHrs, CHUNK, 16, yo, gacc, zacc, z2, g, c); break;
+                }
+            } else switch (cLT) {
                 case 1: mma_stage<1, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
                 case 2: mma_stage<2, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
                 case 4: mma_stage<4, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
