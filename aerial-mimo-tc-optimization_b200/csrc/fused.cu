@@ -26,11 +26,16 @@
 // n-tile B = H, i.e. the same registers as A.  Thread (g = lane/4, c = lane%4)
 // covers antennas 8j+2c and 8j+2c+1 of k-step j (the K order is permuted
 // inside each k-step; A and B use the same permutation).
+#include <atomic>
+#include <mutex>
+
 #include "common.cuh"
 
 namespace aeq {
 
 constexpr int kMaxCells = AERIAL_MAX_CELLS;
+constexpr int kMaxDevices = 64;                 // devices with cached per-device state
+constexpr int kMaxSmemPerCta = 227 * 1024;      // B200 dynamic shared memory per block
 
 // Subcarriers per group: 32 / LT fills every lane of the solve, but for the
 // 1-, 2- and 4-layer tiles that makes one warp's operand pass over a group
@@ -1467,16 +1472,38 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
     return AERIAL_OK;
 }
 
+// SM count of the current device, looked up once per device.
 static int sm_count() {
-    static int n = 0;
+    static std::atomic<int> cache[kMaxDevices];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const bool cached = dev >= 0 && dev < kMaxDevices;
+    int n = cached ? cache[dev].load(std::memory_order_relaxed) : 0;
     if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
         if (n <= 0) n = 148;
+        if (cached) cache[dev].store(n, std::memory_order_relaxed);
     }
     return n;
 }
+
+// Raises kernel K's dynamic shared-memory limit to the per-block maximum,
+// once per device (the launch's own request then sets its occupancy).
+template <auto K>
+static int allow_max_smem() {
+    static std::mutex mu;
+    static bool done[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < kMaxDevices && done[dev]) return AERIAL_OK;
+    e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerCta);
+    if (e != cudaSuccess) return (int)e;
+    if (dev >= 0 && dev < kMaxDevices) done[dev] = true;
+    return AERIAL_OK;
+}
+
 
 struct LaunchShape {
     int warps, ctasPerSm;
@@ -1516,45 +1543,31 @@ struct LaunchPlan {
     int smem;
 };
 
-template <int P, int LTF>
-static int plan_v(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
-    const int bytes = sh.warps * warpBytes;
-    static int configured = 0;
-    if (bytes > 48 * 1024 && bytes > configured) {
-        cudaError_t e =
-            cudaFuncSetAttribute(fused_eq_kernel<P, LTF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e != cudaSuccess) return (int)e;
-        configured = bytes;
-    }
+// Grid: enough CTAs for every group, at most ctasPerSm per SM.
+static void fill_plan(const void* func, const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
     long need = (p.totalGroups + sh.warps - 1) / sh.warps;
     long grid = (long)sm_count() * sh.ctasPerSm;
     if (grid > need) grid = need;
     if (grid < 1) grid = 1;
-    out.func = reinterpret_cast<const void*>(fused_eq_kernel<P, LTF>);
+    out.func = func;
     out.grid = dim3((unsigned)grid);
     out.block = dim3(sh.warps * 32);
-    out.smem = bytes;
+    out.smem = sh.warps * warpBytes;
+}
+
+template <int P, int LTF>
+static int plan_v(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
+    const int s = allow_max_smem<fused_eq_kernel<P, LTF>>();
+    if (s) return s;
+    fill_plan(reinterpret_cast<const void*>(fused_eq_kernel<P, LTF>), p, warpBytes, sh, out);
     return AERIAL_OK;
 }
 
 template <int P, int LTF, int NCH>
 static int plan_a(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
-    static int configured = 0;
-    const int bytes = sh.warps * warpBytes;
-    if (bytes > 48 * 1024 && bytes > configured) {
-        cudaError_t e =
-            cudaFuncSetAttribute(fused_eq_kernel_a<P, LTF, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e != cudaSuccess) return (int)e;
-        configured = bytes;
-    }
-    long need = (p.totalGroups + sh.warps - 1) / sh.warps;
-    long grid = (long)sm_count() * sh.ctasPerSm;
-    if (grid > need) grid = need;
-    if (grid < 1) grid = 1;
-    out.func = reinterpret_cast<const void*>(fused_eq_kernel_a<P, LTF, NCH>);
-    out.grid = dim3((unsigned)grid);
-    out.block = dim3(sh.warps * 32);
-    out.smem = bytes;
+    const int s = allow_max_smem<fused_eq_kernel_a<P, LTF, NCH>>();
+    if (s) return s;
+    fill_plan(reinterpret_cast<const void*>(fused_eq_kernel_a<P, LTF, NCH>), p, warpBytes, sh, out);
     return AERIAL_OK;
 }
 
@@ -1569,22 +1582,9 @@ static int plan_an(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPl
 
 template <int LTF, int NCH>
 static int plan_h(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
-    static int configured = 0;
-    const int bytes = sh.warps * warpBytes;
-    if (bytes > 48 * 1024 && bytes > configured) {
-        cudaError_t e =
-            cudaFuncSetAttribute(fused_eq_kernel_h<LTF, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e != cudaSuccess) return (int)e;
-        configured = bytes;
-    }
-    long need = (p.totalGroups + sh.warps - 1) / sh.warps;
-    long grid = (long)sm_count() * sh.ctasPerSm;
-    if (grid > need) grid = need;
-    if (grid < 1) grid = 1;
-    out.func = reinterpret_cast<const void*>(fused_eq_kernel_h<LTF, NCH>);
-    out.grid = dim3((unsigned)grid);
-    out.block = dim3(sh.warps * 32);
-    out.smem = bytes;
+    const int s = allow_max_smem<fused_eq_kernel_h<LTF, NCH>>();
+    if (s) return s;
+    fill_plan(reinterpret_cast<const void*>(fused_eq_kernel_h<LTF, NCH>), p, warpBytes, sh, out);
     return AERIAL_OK;
 }
 
@@ -1855,20 +1855,15 @@ namespace aeq {
 template <int P, int LTF>
 static int prepare_v() {
     cudaFuncAttributes at;
-    cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel<P, LTF>);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fused_eq_kernel<P, LTF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    return e == cudaSuccess ? AERIAL_OK : (int)e;
+    const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel<P, LTF>);
+    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel<P, LTF>>() : (int)e;
 }
 
 template <int P, int LTF, int NCH>
 static int prepare_a() {
     cudaFuncAttributes at;
-    cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_a<P, LTF, NCH>);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fused_eq_kernel_a<P, LTF, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 220 * 1024);
-    return e == cudaSuccess ? AERIAL_OK : (int)e;
+    const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_a<P, LTF, NCH>);
+    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_a<P, LTF, NCH>>() : (int)e;
 }
 
 template <int P, int LTF>
@@ -1882,11 +1877,8 @@ static int prepare_an() {
 template <int LTF, int NCH>
 static int prepare_h() {
     cudaFuncAttributes at;
-    cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_h<LTF, NCH>);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fused_eq_kernel_h<LTF, NCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 220 * 1024);
-    return e == cudaSuccess ? AERIAL_OK : (int)e;
+    const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_h<LTF, NCH>);
+    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_h<LTF, NCH>>() : (int)e;
 }
 
 template <int P>

@@ -113,3 +113,32 @@ def test_fp16_io_unsupported_cases(aeq, wl, cuda):
     ws = torch.empty(aeq.pusch_eq_plain_workspace([d_ok]), dtype=torch.uint8, device=cuda)
     with pytest.raises(aeq.AerialError):                                    # the FP32 chain reads complex64 only
         aeq.pusch_eq_plain([d_ok], ws)
+
+
+def test_fp16_io_graph_replay_and_update(aeq, wl, cuda):
+    """The FP16 I/O launch as a CUDA graph: replay equals the direct launch, and
+    re-pointing it at another slot's half buffers gives that slot's results."""
+    def descs(cells):
+        keep, ds = [], []
+        for c in cells:
+            H16, Y16 = half_pairs(c.H).to(cuda), half_pairs(c.Y).to(cuda)
+            l16 = torch.full((c.llr_numel,), float("nan"), dtype=torch.float16, device=cuda)
+            keep.append((H16, Y16, l16))
+            ds.append(aeq.cell_desc(H16, Y16, l16, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits,
+                                    fmt=aeq.FMT_CF16))
+        return keep, ds
+    ca = [wl.make_cell(2, 64, 8, 11, 256, 25.0, seed=950 + k) for k in range(3)]
+    cb = [wl.make_cell(2, 64, 8, 11, 256, 25.0, seed=960 + k) for k in range(3)]
+    ref_a, da = descs(ca)
+    ref_b, db = descs(cb)
+    aeq.pusch_eq_fused(da, aeq.make_tuning("fp16"))
+    aeq.pusch_eq_fused(db, aeq.make_tuning("fp16"))
+    got_a, ga = descs(ca)
+    got_b, gb = descs(cb)
+    with aeq.FusedGraph(ga, aeq.make_tuning("fp16")) as g:
+        g.launch()
+        g.update(gb)
+        g.launch()
+        torch.cuda.synchronize()
+    for r, o in zip(ref_a + ref_b, got_a + got_b):
+        assert torch.equal(o[2], r[2])
