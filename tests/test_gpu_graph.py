@@ -72,3 +72,25 @@ def test_graph_of_exact_tile_launch(aeq, wl, cuda):
         torch.cuda.synchronize()
     for r, o in zip(ref_a + ref_b, got_a + got_b):
         np.testing.assert_array_equal(o[2].cpu().numpy(), r[2].cpu().numpy())
+
+
+def test_fused_launch_captures_into_a_cuda_graph(aeq, wl, cuda):
+    """aerial_pusch_eq_fused issues nothing but its kernel launch once the
+    kernel is loaded, so stream capture records it; the replayed graph gives
+    the direct launch's results."""
+    cells = [wl.make_cell(2, 64, 8, 11, 256, 25.0, seed=91), wl.make_cell(3, 32, 4, 11, 16, 20.0, seed=92)]
+    ref, dr = _descs(aeq, cells, cuda)
+    t = aeq.make_tuning("fp16")
+    aeq.pusch_eq_fused(dr, t)               # first call: loads the kernel and sets its limits
+    torch.cuda.synchronize()
+    got, dg = _descs(aeq, cells, cuda)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        aeq.pusch_eq_fused(dg, t)
+    for o in got:
+        o[2].fill_(float("nan"))
+    graph.replay()
+    torch.cuda.synchronize()
+    for r, o in zip(ref, got):
+        np.testing.assert_array_equal(o[2].cpu().numpy(), r[2].cpu().numpy())
+    del graph
