@@ -203,7 +203,10 @@ int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, const aeria
  * aerial_pusch_eq_host_workspace) stages the batches.  Everything is
  * enqueued asynchronously behind the work already on `stream`, and `stream`
  * waits for all of it: synchronize `stream` before reading the outputs.  Any
- * number of cells; the first call on a device creates the internal streams.
+ * number of cells; the first call on a device creates the internal streams,
+ * and calls from several host threads take turns while they enqueue.  On an
+ * error return the batches enqueued before the failing one still run, and
+ * `stream` still waits for them.
  * Replaces the reference's blocking cudaMemcpy staging around its launches
  * (src/aerial_coef_wmma.cu:396-397, :414-416). */
 int aerial_pusch_eq_host_workspace(const aerial_cell_desc* cells, int nCells, int cellsPerBatch,
