@@ -1,5 +1,6 @@
 // fused.cu -- the fused PUSCH equalization kernel: Gram + matched filter on
-// the tensor cores, FP32 Cholesky MMSE solve, unbiasing and max-log LLR, in
+// the tensor cores, FP32 MMSE solve (LDL^H elimination with the inverse
+// accumulated in the same sweep), unbiasing and max-log LLR, in
 // one persistent launch over any mix of cells.  Only H and Y_rx are read
 // from HBM and only LLRs (optionally Y_eq) are written; G, C and Y_eq stay in
 // registers / shared memory.
@@ -115,23 +116,6 @@ __device__ __forceinline__ void mma16816(float* d, uint32_t a0, uint32_t a1, uin
     }
 }
 
-// complex helpers (FP32)
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-// acc - a * b
-__device__ __forceinline__ float2 csub_mul(float2 acc, float2 a, float2 b) {
-    return make_float2(acc.x - a.x * b.x + a.y * b.y, acc.y - a.x * b.y - a.y * b.x);
-}
-// acc - conj(a) * b
-__device__ __forceinline__ float2 csub_cmul(float2 acc, float2 a, float2 b) {
-    return make_float2(acc.x - a.x * b.x - a.y * b.y, acc.y - a.x * b.y + a.y * b.x);
-}
-// acc - a * conj(b)
-__device__ __forceinline__ float2 csub_mulc(float2 acc, float2 a, float2 b) {
-    return make_float2(acc.x - a.x * b.x - a.y * b.y, acc.y - a.y * b.x + a.x * b.y);
-}
-
 // ---------------------------------------------------------------------------
 // per-warp shared-memory layout for layer tile LT (GS = 32/LT subcarriers), in
 // float2 units.  G rows (later Lc^-1 rows) and Z rows of each subcarrier;
@@ -142,7 +126,7 @@ __device__ __forceinline__ float2 csub_mulc(float2 acc, float2 a, float2 b) {
 template <int LT>
 struct WarpSmem {
     static constexpr int GS = 32 / LT;
-    static constexpr int RS = (LT + 3) & ~1;         // G / Linv row stride (even: float4-aligned)
+    static constexpr int RS = (LT + 3) & ~1;         // G row stride (even: float4-aligned)
     static constexpr int ZS = 16 + 2;                // Z row stride (16 symbols)
     static constexpr int GB = LT * RS + 2;           // per-subcarrier G block
     static constexpr int ZB = LT * ZS + 2;           // per-subcarrier Z block
@@ -467,8 +451,8 @@ __device__ __forceinline__ void lds2x64(uint32_t a, unsigned long long& v0, unsi
 }
 
 // X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs, then unbias and demap;
-// lp / ye walk the row's LLRs and equalized symbols.  Up to 8-layer tiles the
-// sums run on packed pairs: with Z[m][s] = (zr, zi) as stored,
+// lp / ye walk the row's LLRs and equalized symbols.  The sums run on packed
+// pairs: with Z[m][s] = (zr, zi) as stored,
 //   P_s = sum_m (Re g_m, Re g_m) * (zr, zi),  Q_s = sum_m (Im g_m, Im g_m) * (zr, zi)
 //   X_s = (P.x - Q.y, P.y + Q.x),
 // four packed FMAs per m and symbol pair instead of eight scalar ones.
@@ -478,62 +462,38 @@ __device__ __forceinline__ void emit_row(const float2* sZ, const float2* gi, cha
     using W = WarpSmem<LT>;
     constexpr int LB = 2 * N * (H16 ? 2 : 4);      // LLR bytes per symbol
     constexpr int YB = H16 ? 4 : 8;                // Y_eq bytes per symbol
-    if constexpr (LT <= 8) {
-        unsigned long long gr[LT], gq[LT];
+    unsigned long long gr[LT], gq[LT];
+#pragma unroll
+    for (int m = 0; m < LT; m++) {
+        gr[m] = pk2(gi[m].x, gi[m].x);
+        gq[m] = pk2(gi[m].y, gi[m].y);
+    }
+    const uint32_t zb = (uint32_t)__cvta_generic_to_shared(sZ);
+#pragma unroll 1
+    for (int s = 0; s < nSym; s += 2) {
+        unsigned long long P0, Q0, P1, Q1;
 #pragma unroll
         for (int m = 0; m < LT; m++) {
-            gr[m] = pk2(gi[m].x, gi[m].x);
-            gq[m] = pk2(gi[m].y, gi[m].y);
-        }
-        const uint32_t zb = (uint32_t)__cvta_generic_to_shared(sZ);
-#pragma unroll 1
-        for (int s = 0; s < nSym; s += 2) {
-            unsigned long long P0, Q0, P1, Q1;
-#pragma unroll
-            for (int m = 0; m < LT; m++) {
-                unsigned long long z0, z1;
-                lds2x64(zb + (m * W::ZS + s) * 8, z0, z1);
-                if (m == 0) {
-                    P0 = mul2(gr[0], z0);
-                    Q0 = mul2(gq[0], z0);
-                    P1 = mul2(gr[0], z1);
-                    Q1 = mul2(gq[0], z1);
-                } else {
-                    P0 = fma2(gr[m], z0, P0);
-                    Q0 = fma2(gq[m], z0, Q0);
-                    P1 = fma2(gr[m], z1, P1);
-                    Q1 = fma2(gq[m], z1, Q1);
-                }
+            unsigned long long z0, z1;
+            lds2x64(zb + (m * W::ZS + s) * 8, z0, z1);
+            if (m == 0) {
+                P0 = mul2(gr[0], z0);
+                Q0 = mul2(gq[0], z0);
+                P1 = mul2(gr[0], z1);
+                Q1 = mul2(gq[0], z1);
+            } else {
+                P0 = fma2(gr[m], z0, P0);
+                Q0 = fma2(gq[m], z0, Q0);
+                P1 = fma2(gr[m], z1, P1);
+                Q1 = fma2(gq[m], z1, Q1);
             }
-            const float2 p0 = upk2(P0), q0 = upk2(Q0), p1 = upk2(P1), q1 = upk2(Q1);
-            emit1<N, YE, H16>(lp, ye, make_float2(p0.x - q0.y, p0.y + q0.x), invMu, scl, d);
-            if (s + 1 < nSym)
-                emit1<N, YE, H16>(lp + LB, ye + YB, make_float2(p1.x - q1.y, p1.y + q1.x), invMu, scl, d);
-            lp += 2 * LB;
-            if constexpr (YE) ye += 2 * YB;
         }
-    } else {
-#pragma unroll 1
-        for (int s = 0; s < nSym; s += 2) {
-            float2 x0 = make_float2(0.f, 0.f), x1 = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int m = 0; m < LT; m++) {
-                const float2 a = gi[m];
-                const float4 z = *reinterpret_cast<const float4*>(sZ + m * W::ZS + s);
-                x0.x = fmaf(a.x, z.x, x0.x);
-                x0.x = fmaf(-a.y, z.y, x0.x);
-                x0.y = fmaf(a.x, z.y, x0.y);
-                x0.y = fmaf(a.y, z.x, x0.y);
-                x1.x = fmaf(a.x, z.z, x1.x);
-                x1.x = fmaf(-a.y, z.w, x1.x);
-                x1.y = fmaf(a.x, z.w, x1.y);
-                x1.y = fmaf(a.y, z.z, x1.y);
-            }
-            emit1<N, YE, H16>(lp, ye, x0, invMu, scl, d);
-            if (s + 1 < nSym) emit1<N, YE, H16>(lp + LB, ye + YB, x1, invMu, scl, d);
-            lp += 2 * LB;
-            if constexpr (YE) ye += 2 * YB;
-        }
+        const float2 p0 = upk2(P0), q0 = upk2(Q0), p1 = upk2(P1), q1 = upk2(Q1);
+        emit1<N, YE, H16>(lp, ye, make_float2(p0.x - q0.y, p0.y + q0.x), invMu, scl, d);
+        if (s + 1 < nSym)
+            emit1<N, YE, H16>(lp + LB, ye + YB, make_float2(p1.x - q1.y, p1.y + q1.x), invMu, scl, d);
+        lp += 2 * LB;
+        if constexpr (YE) ye += 2 * YB;
     }
 }
 
@@ -557,11 +517,37 @@ __device__ __forceinline__ void solve_emit(const CellView& cl, const float2* sZ,
         emit_row<LT, N, false, H16>(sZ, gi, lp, nullptr, cl.nSym, invMu, scl, d);
 }
 
-__device__ __forceinline__ float shfl_f(float v, int src, int width) {
-    return __shfl_sync(0xffffffffu, v, src, width);
+// 1/x: the approximate reciprocal plus one Newton-Raphson step y (2 - x y).
+__device__ __forceinline__ float rcp_nr(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y * fmaf(-x, y, 2.f);
 }
-__device__ __forceinline__ float2 shfl_c(float2 v, int src, int width) {
-    return make_float2(__shfl_sync(0xffffffffu, v.x, src, width), __shfl_sync(0xffffffffu, v.y, src, width));
+
+// Row of LT complex values <-> shared memory (16-byte pieces; rows start
+// 16-byte aligned, WarpSmem keeps every row stride even).
+template <int LT>
+__device__ __forceinline__ void put_row(float2* row, const float2 (&r)[LT]) {
+    if constexpr (LT == 1) {
+        row[0] = r[0];
+    } else {
+#pragma unroll
+        for (int m = 0; m < LT; m += 2)
+            *reinterpret_cast<float4*>(row + m) = make_float4(r[m].x, r[m].y, r[m + 1].x, r[m + 1].y);
+    }
+}
+template <int LT>
+__device__ __forceinline__ void get_row(const float2* row, float2 (&b)[LT]) {
+    if constexpr (LT == 1) {
+        b[0] = row[0];
+    } else {
+#pragma unroll
+        for (int m = 0; m < LT; m += 2) {
+            const float4 t = *reinterpret_cast<const float4*>(row + m);
+            b[m] = make_float2(t.x, t.y);
+            b[m + 1] = make_float2(t.z, t.w);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -575,10 +561,8 @@ __device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid
     extern __shared__ float4 smem_raw[];
     float2* sm = reinterpret_cast<float2*>(smem_raw) + smemOff;
     // ---- solve phase: lane = (q, i), LT lanes per subcarrier ----
-    // Cholesky G = Lc Lc^H and Linv = Lc^-1 with rows in registers and the
-    // column / row broadcasts done by width-LT shuffles (no branches, no
-    // shared memory); then Ginv = Linv^H Linv and X = Ginv Z from shared
-    // memory (no lane-to-lane dependency).
+    // G^-1 by Gauss-Jordan elimination in place, lane i holding row i in
+    // registers; X = G^-1 Z then reads Z from shared memory.
     const int q = lane / LT, i = lane % LT;
     const long sc = sc0 + q;
     const bool scValid = q < nValid;
@@ -587,81 +571,92 @@ __device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid
     const float2* sZ = sm + W::offZ + q * W::ZB;
     const float s2 = cl.s2;
 
-    float2 gr[LT];
+    // Row i of G + s2 I.  The 16-layer tile keeps the Gram blocks (0,0),
+    // (1,0) and (1,1) only, so rows 0-7 take columns 8-15 as conj(G[m][i]).
+    // Subcarriers past the group's end solve s2 I (never stored).
+    float2 r[LT];
+    if constexpr (LT > 8) {
+        float2 lo[8];
+        get_row<8>(sG + i * W::RS, lo);
+#pragma unroll
+        for (int m = 0; m < 8; m++) r[m] = lo[m];
+        const bool up = i < 8;
+#pragma unroll
+        for (int m = 8; m < LT; m++) {
+            const float2 v = sG[up ? m * W::RS + i : i * W::RS + m];
+            r[m] = make_float2(v.x, up ? -v.y : v.y);
+        }
+    } else {
+        get_row<LT>(sG + i * W::RS, r);
+    }
 #pragma unroll
     for (int m = 0; m < LT; m++) {
-        float2 v = (scValid && real) ? sG[i * W::RS + m] : make_float2(0.f, 0.f);
-        if (m > i) v = make_float2(0.f, 0.f);
+        float2 v = (scValid && real) ? r[m] : make_float2(0.f, 0.f);
         if (m == i) v = real ? make_float2(v.x + s2, 0.f) : make_float2(1.f, 0.f);
-        gr[m] = v;
+        r[m] = v;
     }
 
-    // Cholesky, right-looking.  1/sqrt by rsqrt plus one Newton step.
-    float myInv = 1.f;
-#pragma unroll
-    for (int j = 0; j < LT; j++) {
-        const float djj = fmaxf(shfl_f(gr[j].x, j, LT), 1e-30f);
-        float ivj = rsqrtf(djj);
-        ivj = ivj * (1.5f - 0.5f * djj * ivj * ivj);
-        const float2 scaled = make_float2(gr[j].x * ivj, gr[j].y * ivj);
-        const float2 lij = (i > j) ? scaled : make_float2(0.f, 0.f);
-        if (i == j) myInv = ivj;
-        gr[j] = (i > j) ? scaled : ((i == j) ? make_float2(djj * ivj, 0.f) : gr[j]);
-#pragma unroll
-        for (int m = j + 1; m < LT; m++) gr[m] = csub_mulc(gr[m], lij, shfl_c(lij, m, LT));
-    }
-
-    // Linv row i by forward substitution on the identity.
-    float2 e[LT];
-#pragma unroll
-    for (int m = 0; m < LT; m++) e[m] = make_float2(m == i ? 1.f : 0.f, 0.f);
+    // Gauss-Jordan sweep, step k: row k as it stands before the step
+    // (published to shared memory by lane k at the end of step k - 1)
+    // eliminates column k from every other row:
+    //   p = 1 / b_kk,  f_i = r_ik p  (f_k = 1 - p),
+    //   r_ij -= f_i b_kj  (j != k),   r_ik = delta_ik - f_i,
+    // which leaves row k as b_k p and, after LT steps, G^-1 in the rows.  On
+    // the trailing block (i, j > k) the update is the right-looking LDL^H
+    // (square-root-free Cholesky) step of G, and the pivots b_kk are the
+    // diagonal of D in G = L D L^H: real and positive for the Hermitian
+    // positive definite G, so no pivoting is needed.  The other rows and
+    // columns accumulate the inverse in the same sweep.  Every lane does
+    // LT - 1 useful complex multiply-adds per step (no idle triangle), and the
+    // broadcast of row k is LT / 2 shared loads.
+    if (i == 0) put_row<LT>(sG, r);
 #pragma unroll
     for (int k = 0; k < LT; k++) {
-        const float sck = (i == k) ? myInv : 1.f;
+        __syncwarp();
+        const float2* bk = sG + k * W::RS;
+        const float piv = fmaxf(bk[k].x, 1e-30f);
+        const float p = rcp_nr(piv);
+        const bool mine = i == k;
+        const float fx = mine ? 1.f - p : r[k].x * p;
+        const float fy = mine ? 0.f : r[k].y * p;
+        // row k streamed in pairs (keeps the 16-layer tile within registers)
 #pragma unroll
-        for (int m = 0; m <= k; m++) { e[m].x *= sck; e[m].y *= sck; }
-        const float2 lik = (i > k) ? gr[k] : make_float2(0.f, 0.f);
+        for (int j0 = 0; j0 < LT; j0 += (LT == 1 ? 1 : 2)) {
+            float2 b[2];
+            if constexpr (LT == 1) {
+                b[0] = bk[0];
+            } else {
+                const float4 t = *reinterpret_cast<const float4*>(bk + j0);
+                b[0] = make_float2(t.x, t.y);
+                b[1] = make_float2(t.z, t.w);
+            }
 #pragma unroll
-        for (int m = 0; m <= k; m++) e[m] = csub_mul(e[m], lik, shfl_c(e[m], k, LT));
-    }
-    // publish Linv rows (upper part zero) over the G block
-#pragma unroll
-    for (int m = 0; m < LT; m += 2)
-        *reinterpret_cast<float4*>(sG + i * W::RS + m) = make_float4(e[m].x, e[m].y, e[m + 1 < LT ? m + 1 : m].x * (m + 1 < LT), e[m + 1 < LT ? m + 1 : m].y * (m + 1 < LT));
-    __syncwarp();
-
-    // Ginv row i: Ginv[i][j] = sum_m conj(Linv[m][i]) Linv[m][j]
-    float2 gi[LT];
-#pragma unroll
-    for (int j = 0; j < LT; j++) gi[j] = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int m = 0; m < LT; m++) {
-        const float2 a = sG[m * W::RS + i];
-#pragma unroll
-        for (int j = 0; j < LT; j += 2) {
-            if (j > m) break;                          // Linv[m][j] = 0 above the diagonal
-            const float4 b = *reinterpret_cast<const float4*>(sG + m * W::RS + j);
-            gi[j].x = fmaf(a.y, b.y, fmaf(a.x, b.x, gi[j].x));
-            gi[j].y = fmaf(-a.y, b.x, fmaf(a.x, b.y, gi[j].y));
-            if (j + 1 < LT) {
-                gi[j + 1].x = fmaf(a.y, b.w, fmaf(a.x, b.z, gi[j + 1].x));
-                gi[j + 1].y = fmaf(-a.y, b.z, fmaf(a.x, b.w, gi[j + 1].y));
+            for (int u = 0; u < (LT == 1 ? 1 : 2); u++) {
+                const int j = j0 + u;
+                if (j == k) continue;
+                r[j].x = fmaf(-fx, b[u].x, fmaf(fy, b[u].y, r[j].x));
+                r[j].y = fmaf(-fx, b[u].y, fmaf(-fy, b[u].x, r[j].y));
             }
         }
+        r[k] = make_float2(mine ? p : -fx, -fy);
+        if (k + 1 < LT && i == k + 1) put_row<LT>(sG + (k + 1) * W::RS, r);
     }
+    float gii = r[0].x;
+#pragma unroll
+    for (int m = 1; m < LT; m++) gii = (i == m) ? r[m].x : gii;
 
     // X row i = Ginv[i][:] Z, two symbols at a time, each pair demapped and
     // stored as soon as it is complete.
-    const float t = s2 * gi[i].x;       // 1 - mu = s2 (G^-1)_ii
+    const float t = s2 * gii;           // 1 - mu = s2 (G^-1)_ii
     const float mu = fmaxf(1.0f - t, 1e-30f);
     const float invMu = 1.0f / mu;
     const float nInv = mu / fmaxf(t, 1e-30f);
     const bool out = scValid && real;
     switch (cl.nPam) {
-        case 1: solve_emit<LT, 1, H16>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
-        case 2: solve_emit<LT, 2, H16>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
-        case 3: solve_emit<LT, 3, H16>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
-        default: solve_emit<LT, 4, H16>(cl, sZ, gi, sc, i, out, invMu, nInv); break;
+        case 1: solve_emit<LT, 1, H16>(cl, sZ, r, sc, i, out, invMu, nInv); break;
+        case 2: solve_emit<LT, 2, H16>(cl, sZ, r, sc, i, out, invMu, nInv); break;
+        case 3: solve_emit<LT, 3, H16>(cl, sZ, r, sc, i, out, invMu, nInv); break;
+        default: solve_emit<LT, 4, H16>(cl, sZ, r, sc, i, out, invMu, nInv); break;
     }
     __syncwarp();   // shared memory is reused by the next group
 }

@@ -139,8 +139,8 @@ int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, const aerial_ch
                           int foccLen, void* stream);
 
 /* ------------------------------------------------------------------------ */
-/* Fused chain: Gram -> Cholesky MMSE -> apply -> LLR in one kernel; G, C and */
-/* Y_eq stay on chip, only LLRs (and optionally Y_eq) are written.           */
+/* Fused chain: Gram -> FP32 MMSE solve -> apply -> LLR in one kernel; G, C */
+/* and Y_eq stay on chip, only LLRs (and optionally Y_eq) are written.       */
 /* ------------------------------------------------------------------------ */
 
 /* Storage format of a cell's buffers (aerial_cell_desc.format).
