@@ -4,7 +4,9 @@
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
+#include <atomic>
 #include <cmath>
+#include <mutex>
 
 #include "../../include/aerial_eq.h"
 
@@ -19,6 +21,41 @@ inline int launch_status() {
 }
 
 inline cudaStream_t to_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+constexpr int kMaxDevices = 64;                 // devices with cached per-device state
+constexpr int kMaxSmemPerCta = 227 * 1024;      // B200 dynamic shared memory per block
+
+// SM count of the current device, looked up once per device.
+inline int sm_count() {
+    static std::atomic<int> cache[kMaxDevices];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const bool cached = dev >= 0 && dev < kMaxDevices;
+    int n = cached ? cache[dev].load(std::memory_order_relaxed) : 0;
+    if (!n) {
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+        if (cached) cache[dev].store(n, std::memory_order_relaxed);
+    }
+    return n;
+}
+
+// Raises kernel K's dynamic shared-memory limit to the per-block maximum,
+// once per device (the launch's own request then sets its occupancy).
+template <auto K>
+int allow_max_smem() {
+    static std::mutex mu;
+    static bool done[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < kMaxDevices && done[dev]) return AERIAL_OK;
+    e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerCta);
+    if (e != cudaSuccess) return (int)e;
+    if (dev >= 0 && dev < kMaxDevices) done[dev] = true;
+    return AERIAL_OK;
+}
 
 // cma() of src/aerial_coef_wmma.cu:61-64 with the contraction nvcc applies to
 // `acc + a*b - c*d`: re = fma(-a.im, b.im, fma(a.re, b.re, acc.re)),

@@ -27,16 +27,11 @@
 // n-tile B = H, i.e. the same registers as A.  Thread (g = lane/4, c = lane%4)
 // covers antennas 8j+2c and 8j+2c+1 of k-step j (the K order is permuted
 // inside each k-step; A and B use the same permutation).
-#include <atomic>
-#include <mutex>
-
 #include "common.cuh"
 
 namespace aeq {
 
 constexpr int kMaxCells = AERIAL_MAX_CELLS;
-constexpr int kMaxDevices = 64;                 // devices with cached per-device state
-constexpr int kMaxSmemPerCta = 227 * 1024;      // B200 dynamic shared memory per block
 
 // Subcarriers per group: 32 / LT fills every lane of the solve, but for the
 // 1-, 2- and 4-layer tiles that makes one warp's operand pass over a group
@@ -1466,39 +1461,6 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
     warpBytes = p.epiBytes + p.nStages * p.stageBytes;
     return AERIAL_OK;
 }
-
-// SM count of the current device, looked up once per device.
-static int sm_count() {
-    static std::atomic<int> cache[kMaxDevices];
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const bool cached = dev >= 0 && dev < kMaxDevices;
-    int n = cached ? cache[dev].load(std::memory_order_relaxed) : 0;
-    if (!n) {
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-        if (cached) cache[dev].store(n, std::memory_order_relaxed);
-    }
-    return n;
-}
-
-// Raises kernel K's dynamic shared-memory limit to the per-block maximum,
-// once per device (the launch's own request then sets its occupancy).
-template <auto K>
-static int allow_max_smem() {
-    static std::mutex mu;
-    static bool done[kMaxDevices] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return (int)e;
-    std::lock_guard<std::mutex> lock(mu);
-    if (dev >= 0 && dev < kMaxDevices && done[dev]) return AERIAL_OK;
-    e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerCta);
-    if (e != cudaSuccess) return (int)e;
-    if (dev >= 0 && dev < kMaxDevices) done[dev] = true;
-    return AERIAL_OK;
-}
-
 
 struct LaunchShape {
     int warps, ctasPerSm;

@@ -2,85 +2,211 @@
 // src/srs/srs_wmma_bench.cu:57-90 and :102-231):
 //   H_est[blk][ant][k_out][p] = sum_k (W[k_out][k] * FOCC[p][k % F]) * SRS[blk][ant][k]
 // The reference accumulates in FP16 (__hfma in V1, an FP16 accumulator in
-// V2); here the filter taps W*FOCC are formed in FP32 once per CTA and the
-// K-term sums are FP32, rounded once at the store.  complex_conjmul (:43-47)
-// computes the plain product despite its name; the plain product is kept.
+// V2).  Here the sums run on the tensor cores with FP32 accumulation and the
+// FP32 accuracy of a scalar FP32 sum; complex_conjmul (:43-47) computes the
+// plain product despite its name, and the plain product is kept.
 //
-// One CTA per (SRS block, 16-antenna slab): the K*P*K filter taps of the
-// block are built in shared memory laid out [k][k_out][p] so a warp reading
-// tap k for consecutive outputs is conflict-free; the 16 SRS rows of the
-// slab are staged once.  Threads map to outputs in the reference's
-// [ant][k_out][p] order, so the stores are coalesced.
+// Tensor-core form (mma.sync m16n8k16, FP16 operands, FP32 accumulate).  Per
+// SRS block it is the complex GEMM out[ant][n] = sum_k S[ant][k] T[n][k] with
+// n = k_out * P + p and taps T[n][k] = W[k_out][k] FOCC[p][k % F], embedded as
+// a real GEMM:
+//   A[ant][2k + r]   = (Re, Im) of S[ant][k]   -- the SRS row as stored, so a
+//                                                thread's A register IS one
+//                                                complex half2 sample
+//   B[2k][2n] = Re T, B[2k+1][2n] = -Im T     -> column 2n   = Re out
+//   B[2k][2n+1] = Im T, B[2k+1][2n+1] = Re T  -> column 2n+1 = Im out
+// and a thread's accumulator pair (d0, d1) is one complex output.
+// Precision: S is FP16 and exact as an operand.  Each tap, a product of two
+// FP16 values formed in FP32, is split T = T_hi + T_lo into two FP16 parts
+// (22 significant bits), and each k-step issues the two products S T_hi and
+// S T_lo into the same FP32 accumulator.  FP16 x FP16 products are exact, so
+// the result carries the error of an FP32 sum (about 2^-22 relative), not the
+// FP16 rounding of the reference's taps.
+//
+// Work split: the taps of one slice of output tiles are built once per CTA in
+// shared memory, already in the B-fragment order (one 16-byte load per lane
+// gives b0, b1 of T_hi and T_lo), so one build serves every SRS block the CTA
+// visits.  Each warp takes (SRS block, 32-antenna) items in turn: its A
+// fragments (two 16-antenna m-tiles, the whole K) are loaded once from global
+// memory, then it sweeps the slice's output tiles.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace aeq {
 
-constexpr int kSrsAntPerCta = 16;
+constexpr int kSrsWarps = 8;                 // warps per CTA
+constexpr int kSrsAntPerItem = 32;           // antennas per warp item (two m16 tiles)
+constexpr int kSrsMaxK = 48;
+constexpr int kSrsSliceBytes = 96 * 1024;    // taps of one slice of output tiles
+
+__device__ __forceinline__ void mma_f16(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                        uint32_t b1) {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t h2bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+
+// FP16 hi/lo parts of the pair (x, y): hi = rn(v), lo = rn(v - hi).
+__device__ __forceinline__ void split_h2(float x, float y, uint32_t& hi, uint32_t& lo) {
+    const __half2 h = __floats2half2_rn(x, y);
+    const float2 hf = __half22float2(h);
+    hi = h2bits(h);
+    lo = h2bits(__floats2half2_rn(x - hf.x, y - hf.y));
+}
+
+// KS: k-steps of 8 complex taps (K <= 8 KS).  Grid: x = CTAs walking the
+// (block, 32-antenna) items, y = slices of NT output tiles (4 complex outputs
+// per tile).
+template <int KS, bool TO_CHANNEL>
+__global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const __half2* __restrict__ srs,
+                                                                       const __half2* __restrict__ W,
+                                                                       const __half2* __restrict__ focc,
+                                                                       void* __restrict__ out, int nAnt, int nBlocks,
+                                                                       int K, int P, int F, int NT) {
+    extern __shared__ uint4 bfrag[];            // [tile][kstep][lane]: {b0 hi, b1 hi, b0 lo, b1 lo}
+    const int N = K * P;                         // complex outputs per antenna
+    const int nTiles = (N + 3) / 4;
+    const int t0 = blockIdx.y * NT;
+    const int nt = min(NT, nTiles - t0);
+    for (int e = threadIdx.x; e < nt * KS * 32; e += blockDim.x) {
+        const int l = e & 31, ks = (e >> 5) % KS, j = e / (32 * KS);
+        const int g = l >> 2, c = l & 3;
+        const int n = (t0 + j) * 4 + (g >> 1);
+        uint32_t hi[2], lo[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int k = ks * 8 + c + 4 * h;
+            float2 t = make_float2(0.f, 0.f);
+            if (n < N && k < K) {
+                const int ko = n / P, p = n % P;
+                const float2 w = __half22float2(W[ko * K + k]);
+                const float2 f = __half22float2(focc[p * F + (k % F)]);
+                t = make_float2(w.x * f.x - w.y * f.y, w.x * f.y + w.y * f.x);
+            }
+            // even output column: (Re T, -Im T) -> Re out; odd: (Im T, Re T) -> Im out
+            if (g & 1) split_h2(t.y, t.x, hi[h], lo[h]);
+            else split_h2(t.x, -t.y, hi[h], lo[h]);
+        }
+        bfrag[e] = make_uint4(hi[0], hi[1], lo[0], lo[1]);
+    }
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int g = lane >> 2, c = lane & 3;
+    const int antGroups = (nAnt + kSrsAntPerItem - 1) / kSrsAntPerItem;
+    const long items = (long)nBlocks * antGroups;
+    const long nw = (long)gridDim.x * kSrsWarps;
+    const uint32_t fb = (uint32_t)__cvta_generic_to_shared(bfrag) + lane * 16;
+    for (long it = (long)blockIdx.x * kSrsWarps + (threadIdx.x >> 5); it < items; it += nw) {
+        const int blk = (int)(it / antGroups);
+        const int ant0 = (int)(it % antGroups) * kSrsAntPerItem;
+        // A fragments: rows ant0 + 16 mt + g (+8), taps 8 ks + c (+4)
+        uint32_t a[2][KS][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) {
+#pragma unroll
+            for (int rr = 0; rr < 2; rr++) {
+                const int ant = ant0 + 16 * mt + g + 8 * rr;
+                const __half2* row = srs + ((long)blk * nAnt + (ant < nAnt ? ant : 0)) * K;
+#pragma unroll
+                for (int ks = 0; ks < KS; ks++) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int k = ks * 8 + c + 4 * h;
+                        uint32_t v = 0u;
+                        if (ant < nAnt && k < K) v = h2bits(__ldg(row + k));
+                        a[mt][ks][rr + 2 * h] = v;
+                    }
+                }
+            }
+        }
+        for (int j = 0; j < nt; j++) {
+            float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+            for (int ks = 0; ks < KS; ks++) {
+                uint4 b;
+                asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
+                             : "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+                             : "r"(fb + (uint32_t)((j * KS + ks) * 512)));
+#pragma unroll
+                for (int mt = 0; mt < 2; mt++) {
+                    mma_f16(d[mt], a[mt][ks][0], a[mt][ks][1], a[mt][ks][2], a[mt][ks][3], b.x, b.y);
+                    mma_f16(d[mt], a[mt][ks][0], a[mt][ks][1], a[mt][ks][2], a[mt][ks][3], b.z, b.w);
+                }
+            }
+            const int n = (t0 + j) * 4 + c;
+            if (n >= N) continue;
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++) {
+#pragma unroll
+                for (int rr = 0; rr < 2; rr++) {
+                    const int ant = ant0 + 16 * mt + g + 8 * rr;
+                    if (ant >= nAnt) continue;
+                    const float re = d[mt][2 * rr], im = d[mt][2 * rr + 1];
+                    if constexpr (TO_CHANNEL) {
+                        // H[sc = blk*K + ko][ant][layer = p], nLayers = P
+                        const int ko = n / P, p = n % P;
+                        float2* H = reinterpret_cast<float2*>(out);
+                        __stcs(H + (((long)blk * K + ko) * nAnt + ant) * P + p, make_float2(re, im));
+                    } else {
+                        __half2* H = reinterpret_cast<__half2*>(out);
+                        __stcs(reinterpret_cast<unsigned*>(H + ((long)blk * nAnt + ant) * N + n),
+                               h2bits(__floats2half2_rn(re, im)));
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int KS, bool TO_CHANNEL>
+static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
+                         int nBlocks, int K, int P, int F, cudaStream_t st) {
+    auto kern = srs_filter_tc_kernel<KS, TO_CHANNEL>;
+    const int s = allow_max_smem<srs_filter_tc_kernel<KS, TO_CHANNEL>>();
+    if (s != AERIAL_OK) return s;
+    const int nTiles = (K * P + 3) / 4;
+    const int tileBytes = KS * 32 * 16;
+    const int NT = std::min(nTiles, kSrsSliceBytes / tileBytes);
+    const int slices = (nTiles + NT - 1) / NT;
+    const size_t smem = (size_t)NT * tileBytes;
+    int perSm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kSrsWarps * 32, smem);
+    if (e != cudaSuccess) return (int)e;
+    const long items = (long)nBlocks * ((nAnt + kSrsAntPerItem - 1) / kSrsAntPerItem);
+    const long ctasForItems = (items + kSrsWarps - 1) / kSrsWarps;
+    // enough CTAs to fill the GPU once per slice; each walks its share of items
+    long gx = std::max(1L, (long)sm_count() * std::max(1, perSm) / slices);
+    gx = std::min(gx, ctasForItems);
+    dim3 grid((unsigned)gx, (unsigned)slices);
+    kern<<<grid, kSrsWarps * 32, smem, st>>>((const __half2*)SRS, (const __half2*)W, (const __half2*)FOCC, out,
+                                             nAnt, nBlocks, K, P, F, NT);
+    return launch_status();
+}
 
 template <bool TO_CHANNEL>
-__global__ void __launch_bounds__(256) srs_filter_kernel(const __half2* __restrict__ srs,
-                                                          const __half2* __restrict__ W,
-                                                          const __half2* __restrict__ focc, void* __restrict__ out,
-                                                          int nAnt, int K, int P, int F) {
-    extern __shared__ float2 sm[];
-    float2* taps = sm;                          // [K][K][P]: taps[(k*K + ko)*P + p]
-    float2* rows = sm + (long)K * K * P;        // [16][K]
-    const int blk = blockIdx.x;
-    const int ant0 = blockIdx.y * kSrsAntPerCta;
-    const int nA = min(kSrsAntPerCta, nAnt - ant0);
-    const int KP = K * P;
-    for (int e = threadIdx.x; e < K * KP; e += blockDim.x) {
-        const int k = e / KP, r = e % KP, ko = r / P, p = r % P;
-        const float2 w = __half22float2(W[ko * K + k]);
-        const float2 f = __half22float2(focc[p * F + (k % F)]);
-        taps[e] = make_float2(w.x * f.x - w.y * f.y, w.x * f.y + w.y * f.x);
-    }
-    const __half2* s = srs + ((long)blk * nAnt + ant0) * K;
-    for (int e = threadIdx.x; e < nA * K; e += blockDim.x) rows[e] = __half22float2(s[e]);
-    __syncthreads();
-    for (int o = threadIdx.x; o < nA * KP; o += blockDim.x) {
-        const int a = o / KP, r = o % KP;   // r = ko*P + p
-        const float2* row = rows + a * K;
-        float re = 0.f, im = 0.f;
-        for (int k = 0; k < K; k++) {
-            const float2 t = taps[k * KP + r], x = row[k];
-            re = fmaf(t.x, x.x, re);
-            re = fmaf(-t.y, x.y, re);
-            im = fmaf(t.x, x.y, im);
-            im = fmaf(t.y, x.x, im);
-        }
-        const int ant = ant0 + a;
-        if (TO_CHANNEL) {
-            // H[sc = blk*K + ko][ant][layer = p], nLayers = P
-            const int ko = r / P, p = r % P;
-            float2* H = reinterpret_cast<float2*>(out);
-            H[(((long)blk * K + ko) * nAnt + ant) * P + p] = make_float2(re, im);
-        } else {
-            __half2* H = reinterpret_cast<__half2*>(out);
-            H[((long)blk * nAnt + ant) * KP + r] = __floats2half2_rn(re, im);
-        }
+static int launch_srs_ks(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
+                         int nBlocks, int K, int P, int F, cudaStream_t st) {
+    switch ((K + 7) / 8) {
+        case 1: return launch_srs_tc<1, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
+        case 2: return launch_srs_tc<2, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
+        case 3: return launch_srs_tc<3, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
+        case 4: return launch_srs_tc<4, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
+        case 5: return launch_srs_tc<5, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
+        default: return launch_srs_tc<6, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
     }
 }
 
 static int launch_srs(bool toChannel, void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC,
                       int nAnt, int nBlocks, int K, int P, int F, cudaStream_t st) {
-    if (!out || !SRS || !W || !FOCC || nAnt < 1 || nBlocks < 1 || K < 1 || K > 48 || P < 1 || P > 16 || F < 1)
+    if (!out || !SRS || !W || !FOCC || nAnt < 1 || nBlocks < 1 || K < 1 || K > kSrsMaxK || P < 1 || P > 16 || F < 1)
         return AERIAL_ERR_INVALID_ARG;
-    const size_t smem = sizeof(float2) * ((size_t)K * K * P + (size_t)kSrsAntPerCta * K);
-    if (smem > 200 * 1024) return AERIAL_ERR_UNSUPPORTED;
-    dim3 grid(nBlocks, (nAnt + kSrsAntPerCta - 1) / kSrsAntPerCta);
-    if (toChannel) {
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(srs_filter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        srs_filter_kernel<true><<<grid, 256, smem, st>>>((const __half2*)SRS, (const __half2*)W,
-                                                         (const __half2*)FOCC, out, nAnt, K, P, F);
-    } else {
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(srs_filter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        srs_filter_kernel<false><<<grid, 256, smem, st>>>((const __half2*)SRS, (const __half2*)W,
-                                                          (const __half2*)FOCC, out, nAnt, K, P, F);
-    }
-    return launch_status();
+    return toChannel ? launch_srs_ks<true>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st)
+                     : launch_srs_ks<false>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
 }
 
 }  // namespace aeq

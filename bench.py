@@ -415,6 +415,11 @@ def main():
         v, runs, el = cpu_chain_rate(orc, hc, a.cpu_seconds)
         cpu_base = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                     "sample": f"{runs} full slot(s) ({hc.nSC} subcarriers) in {el:.1f} s, OpenMP over subcarriers"}
+        if not half:
+            try:   # the oracle as the checker of slot 0; reported, never fatal for the timing line
+                extras["accuracy_vs_fp64"] = accuracy_vs_fp64(orc, aeq, cells, llrs, descs, tun, stream)
+            except Exception as e:
+                extras["accuracy_vs_fp64"] = {"error": str(e)}
 
     if world > 1:
         dist.barrier()
@@ -633,7 +638,7 @@ def compare_streams(aeq, descs, tuned, a, flush):
 
 
 def bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a):
-    """Plain FP32 chain on the same slots, single-slot latency, accuracy vs FP64."""
+    """Plain FP32 chain on the same slots, single-slot latency, the SRS filter multiply."""
     import numpy as np
     import torch
 
@@ -666,32 +671,68 @@ def bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a):
     lat.sort()
     out["single_slot_latency_us"] = {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                                      "note": f"one {cells[0].nSC}-SC cell per launch, L2 flushed before each"}
-    # accuracy of slot 0 vs the FP64 model
-    try:
-        from oracle import oracle as orc
-
-        c = cells[0]
-        aeq.pusch_eq_fused([descs[0]], tun, stream)
-        torch.cuda.synchronize()
-        H, Y = c.H.cpu().numpy(), c.Y.cpu().numpy()
-        yeq = torch.empty(c.nSC * c.nLayers * c.nSym, dtype=torch.complex64, device=c.H.device)
-        d = aeq.cell_desc(c.H, c.Y, llrs[0], c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, Y_eq=yeq)
-        aeq.pusch_eq_fused([d], tun, stream)
-        torch.cuda.synchronize()
-        y64, _, l64 = orc.chain_f64(H, Y, c.sigma2, c.nSC, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
-        y = yeq.cpu().numpy().astype(np.complex128)
-        l = llrs[0].cpu().numpy().astype(np.float64)
-        evm = 10 * np.log10(np.sum(np.abs(y - y64) ** 2) / np.sum(np.abs(y64) ** 2))
-        bits = c.bits.cpu().numpy().reshape(-1)
-        out["accuracy_vs_fp64"] = {
-            "evm_db": float(evm), "llr_max_abs_err": float(np.abs(l - l64).max()),
-            "llr_scale": float(np.abs(l64).max()),
-            "hard_bit_mismatch": int(np.sum((l < 0) != (l64 < 0))), "bits": int(l.size),
-            "ber_vs_tx": float(np.mean((l < 0).astype(np.uint8) != bits)),
-        }
-    except Exception as e:  # accuracy is reported, never fatal for the timing line
-        out["accuracy_vs_fp64"] = {"error": str(e)}
+    out["srs_filter"] = bench_srs(aeq, llrs[0].device, stream)
     return out
+
+
+def accuracy_vs_fp64(orc, aeq, cells, llrs, descs, tun, stream):
+    """Checker: slot 0's fused result against the FP64 model of the oracle."""
+    import numpy as np
+    import torch
+
+    c = cells[0]
+    H, Y = c.H.cpu().numpy(), c.Y.cpu().numpy()
+    yeq = torch.empty(c.nSC * c.nLayers * c.nSym, dtype=torch.complex64, device=c.H.device)
+    d = aeq.cell_desc(c.H, c.Y, llrs[0], c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, Y_eq=yeq)
+    aeq.pusch_eq_fused([d], tun, stream)
+    torch.cuda.synchronize()
+    y64, _, l64 = orc.chain_f64(H, Y, c.sigma2, c.nSC, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+    y = yeq.cpu().numpy().astype(np.complex128)
+    l = llrs[0].cpu().numpy().astype(np.float64)
+    evm = 10 * np.log10(np.sum(np.abs(y - y64) ** 2) / np.sum(np.abs(y64) ** 2))
+    bits = c.bits.cpu().numpy().reshape(-1)
+    return {
+        "evm_db": float(evm), "llr_max_abs_err": float(np.abs(l - l64).max()),
+        "llr_scale": float(np.abs(l64).max()),
+        "hard_bit_mismatch": int(np.sum((l < 0) != (l64 < 0))), "bits": int(l.size),
+        "ber_vs_tx": float(np.mean((l < 0).astype(np.uint8) != bits)),
+    }
+
+
+def bench_srs(aeq, dev, stream):
+    """SRS filter multiply (srsFilterMultiply, src/srs/srs_wmma_bench.cu:57-90) at the reference's shape -- 66
+    blocks x 64 antennas, K = 24 taps, 4 ports, FOCC length 8 -- for 40 cells x 4 SRS symbols per launch
+    (10,560 blocks, 324 MB touched: larger than L2).  Algorithmic bytes: SRS in + W + FOCC + H_est out (FP16)."""
+    import torch
+
+    K, P, F, nAnt = 24, 4, 8, 64
+    nBlk = 66 * 40 * 4
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    srs = ((torch.rand(nBlk * nAnt * K * 2, generator=g, device=dev) - 0.5) * 1.4).half()
+    W = ((torch.rand(K * K * 2, generator=g, device=dev) - 0.5) * 1.4).half()
+    focc = ((torch.rand(P * F * 2, generator=g, device=dev) - 0.5) * 1.4).half()
+    out = torch.empty(nBlk * nAnt * K * P * 2, dtype=torch.float16, device=dev)
+    for _ in range(3):
+        aeq.srs_filter(out, srs, W, focc, nAnt, nBlk, K, P, F, stream)
+    torch.cuda.synchronize()
+    k = 50
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        aeq.srs_filter(out, srs, W, focc, nAnt, nBlk, K, P, F, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    us = e0.elapsed_time(e1) * 1e3 / k
+    nbytes = 2 * (srs.numel() + W.numel() + focc.numel() + out.numel())
+    flops = 8.0 * nBlk * nAnt * K * P * K
+    peak, kind = measured_peaks()
+    gbs = nbytes / (us * 1e-6) / 1e9
+    return {"us_per_launch": us, "blocks_per_launch": nBlk, "bytes_per_launch": nbytes,
+            "achieved_gbs": gbs, "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": kind,
+            "gflops": flops / (us * 1e-6) / 1e9,
+            "shape": f"{nBlk} blocks x {nAnt} antennas, K={K}, P={P}, FOCC length {F}, FP16 in/out, "
+                     "tensor cores (FP16 operands, taps split hi/lo), FP32 accumulate"}
 
 
 if __name__ == "__main__":
