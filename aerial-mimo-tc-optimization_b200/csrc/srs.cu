@@ -23,12 +23,20 @@
 // the result carries the error of an FP32 sum (about 2^-22 relative), not the
 // FP16 rounding of the reference's taps.
 //
-// Work split: the taps of one slice of output tiles are built once per CTA in
+// Output order.  Output tiles go in groups of four: tile jj of group q puts
+// output n = 16 q + 4 c + jj in its complex column c, so after the four tiles
+// of a group a lane holds four consecutive outputs of its antenna rows (one
+// 16-byte store), and the four tiles give eight independent accumulators.
+// Inside each k-step, K slot c (and c + 4) holds tap 2c (and 2c + 1), so a
+// lane's two A registers of a row are one 8-byte load.  Both are column / row
+// permutations of the same GEMM.
+//
+// Work split: the taps of one slice of groups are built once per CTA in
 // shared memory, already in the B-fragment order (one 16-byte load per lane
 // gives b0, b1 of T_hi and T_lo), so one build serves every SRS block the CTA
 // visits.  Each warp takes (SRS block, 32-antenna) items in turn: its A
 // fragments (two 16-antenna m-tiles, the whole K) are loaded once from global
-// memory, then it sweeps the slice's output tiles.
+// memory, then it sweeps the slice's groups.
 #include <algorithm>
 
 #include "common.cuh"
@@ -38,7 +46,8 @@ namespace aeq {
 constexpr int kSrsWarps = 8;                 // warps per CTA
 constexpr int kSrsAntPerItem = 32;           // antennas per warp item (two m16 tiles)
 constexpr int kSrsMaxK = 48;
-constexpr int kSrsSliceBytes = 96 * 1024;    // taps of one slice of output tiles
+constexpr int kSrsSliceBytes = 96 * 1024;    // taps of one slice of output groups
+constexpr int kSrsGroupBytes = 4 * 32 * 16;  // one k-step of a group: 4 tiles x 32 lanes x 16 B
 
 __device__ __forceinline__ void mma_f16(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
                                         uint32_t b1) {
@@ -59,27 +68,27 @@ __device__ __forceinline__ void split_h2(float x, float y, uint32_t& hi, uint32_
 }
 
 // KS: k-steps of 8 complex taps (K <= 8 KS).  Grid: x = CTAs walking the
-// (block, 32-antenna) items, y = slices of NT output tiles (4 complex outputs
-// per tile).
+// (block, 32-antenna) items, y = slices of NQ output groups (16 complex
+// outputs per group).
 template <int KS, bool TO_CHANNEL>
 __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const __half2* __restrict__ srs,
-                                                                       const __half2* __restrict__ W,
-                                                                       const __half2* __restrict__ focc,
-                                                                       void* __restrict__ out, int nAnt, int nBlocks,
-                                                                       int K, int P, int F, int NT) {
-    extern __shared__ uint4 bfrag[];            // [tile][kstep][lane]: {b0 hi, b1 hi, b0 lo, b1 lo}
+                                                                          const __half2* __restrict__ W,
+                                                                          const __half2* __restrict__ focc,
+                                                                          void* __restrict__ out, int nAnt,
+                                                                          int nBlocks, int K, int P, int F, int NQ) {
+    extern __shared__ uint4 bfrag[];            // [group][kstep][tile][lane]: {b0 hi, b1 hi, b0 lo, b1 lo}
     const int N = K * P;                         // complex outputs per antenna
-    const int nTiles = (N + 3) / 4;
-    const int t0 = blockIdx.y * NT;
-    const int nt = min(NT, nTiles - t0);
-    for (int e = threadIdx.x; e < nt * KS * 32; e += blockDim.x) {
-        const int l = e & 31, ks = (e >> 5) % KS, j = e / (32 * KS);
+    const int nGroups = (N + 15) / 16;
+    const int q0 = blockIdx.y * NQ;
+    const int nq = min(NQ, nGroups - q0);
+    for (int e = threadIdx.x; e < nq * KS * 128; e += blockDim.x) {
+        const int l = e & 31, jj = (e >> 5) & 3, ks = (e >> 7) % KS, q = q0 + e / (128 * KS);
         const int g = l >> 2, c = l & 3;
-        const int n = (t0 + j) * 4 + (g >> 1);
+        const int n = 16 * q + 4 * (g >> 1) + jj;
         uint32_t hi[2], lo[2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const int k = ks * 8 + c + 4 * h;
+            const int k = ks * 8 + 2 * c + h;    // K slot c + 4h
             float2 t = make_float2(0.f, 0.f);
             if (n < N && k < K) {
                 const int ko = n / P, p = n % P;
@@ -101,61 +110,104 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
     const long items = (long)nBlocks * antGroups;
     const long nw = (long)gridDim.x * kSrsWarps;
     const uint32_t fb = (uint32_t)__cvta_generic_to_shared(bfrag) + lane * 16;
+    const bool pairK = (K & 1) == 0;             // taps 2c, 2c + 1 of a row are one 8-byte load
     for (long it = (long)blockIdx.x * kSrsWarps + (threadIdx.x >> 5); it < items; it += nw) {
         const int blk = (int)(it / antGroups);
-        const int ant0 = (int)(it % antGroups) * kSrsAntPerItem;
-        // A fragments: rows ant0 + 16 mt + g (+8), taps 8 ks + c (+4)
+        const int ant0 = (int)(it - (long)blk * antGroups) * kSrsAntPerItem;
+        // A fragments: rows ant0 + 16 mt + g (+8 rr), taps 8 ks + 2c (+1)
         uint32_t a[2][KS][4];
 #pragma unroll
         for (int mt = 0; mt < 2; mt++) {
 #pragma unroll
             for (int rr = 0; rr < 2; rr++) {
                 const int ant = ant0 + 16 * mt + g + 8 * rr;
-                const __half2* row = srs + ((long)blk * nAnt + (ant < nAnt ? ant : 0)) * K;
+                const bool av = ant < nAnt;
+                const __half2* row = srs + ((long)blk * nAnt + (av ? ant : 0)) * K;
 #pragma unroll
                 for (int ks = 0; ks < KS; ks++) {
-#pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int k = ks * 8 + c + 4 * h;
-                        uint32_t v = 0u;
-                        if (ant < nAnt && k < K) v = h2bits(__ldg(row + k));
-                        a[mt][ks][rr + 2 * h] = v;
+                    const int k = ks * 8 + 2 * c;
+                    uint32_t v0 = 0u, v1 = 0u;
+                    if (av && k < K) {
+                        if (pairK) {
+                            const uint2 v = __ldg(reinterpret_cast<const uint2*>(row + k));
+                            v0 = v.x;
+                            v1 = v.y;
+                        } else {
+                            v0 = h2bits(__ldg(row + k));
+                            if (k + 1 < K) v1 = h2bits(__ldg(row + k + 1));
+                        }
                     }
+                    a[mt][ks][rr] = v0;
+                    a[mt][ks][rr + 2] = v1;
                 }
             }
         }
-        for (int j = 0; j < nt; j++) {
-            float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+        for (int q = 0; q < nq; q++) {
+            float d[4][2][4];
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++)
+#pragma unroll
+                for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+                    for (int r = 0; r < 4; r++) d[jj][mt][r] = 0.f;
 #pragma unroll
             for (int ks = 0; ks < KS; ks++) {
-                uint4 b;
-                asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
-                             : "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
-                             : "r"(fb + (uint32_t)((j * KS + ks) * 512)));
 #pragma unroll
-                for (int mt = 0; mt < 2; mt++) {
-                    mma_f16(d[mt], a[mt][ks][0], a[mt][ks][1], a[mt][ks][2], a[mt][ks][3], b.x, b.y);
-                    mma_f16(d[mt], a[mt][ks][0], a[mt][ks][1], a[mt][ks][2], a[mt][ks][3], b.z, b.w);
+                for (int jj = 0; jj < 4; jj++) {
+                    uint4 b;
+                    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
+                                 : "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+                                 : "r"(fb + (uint32_t)(((q * KS + ks) * 4 + jj) * 512)));
+#pragma unroll
+                    for (int mt = 0; mt < 2; mt++) {
+                        mma_f16(d[jj][mt], a[mt][ks][0], a[mt][ks][1], a[mt][ks][2], a[mt][ks][3], b.x, b.y);
+                        mma_f16(d[jj][mt], a[mt][ks][0], a[mt][ks][1], a[mt][ks][2], a[mt][ks][3], b.z, b.w);
+                    }
                 }
             }
-            const int n = (t0 + j) * 4 + c;
-            if (n >= N) continue;
+            // lane holds outputs n0 .. n0 + 3 of rows (mt, rr): (Re, Im) = d[jj][mt][2 rr], [2 rr + 1]
+            const int n0 = 16 * (q0 + q) + 4 * c;
+            if (n0 >= N) continue;
+            const bool full = n0 + 3 < N;
 #pragma unroll
             for (int mt = 0; mt < 2; mt++) {
 #pragma unroll
                 for (int rr = 0; rr < 2; rr++) {
                     const int ant = ant0 + 16 * mt + g + 8 * rr;
                     if (ant >= nAnt) continue;
-                    const float re = d[mt][2 * rr], im = d[mt][2 * rr + 1];
                     if constexpr (TO_CHANNEL) {
                         // H[sc = blk*K + ko][ant][layer = p], nLayers = P
-                        const int ko = n / P, p = n % P;
                         float2* H = reinterpret_cast<float2*>(out);
-                        __stcs(H + (((long)blk * K + ko) * nAnt + ant) * P + p, make_float2(re, im));
+                        if (P == 4 && full) {
+                            float2* dst = H + (((long)blk * K + n0 / 4) * nAnt + ant) * 4;
+                            __stcs(reinterpret_cast<float4*>(dst),
+                                   make_float4(d[0][mt][2 * rr], d[0][mt][2 * rr + 1], d[1][mt][2 * rr],
+                                               d[1][mt][2 * rr + 1]));
+                            __stcs(reinterpret_cast<float4*>(dst + 2),
+                                   make_float4(d[2][mt][2 * rr], d[2][mt][2 * rr + 1], d[3][mt][2 * rr],
+                                               d[3][mt][2 * rr + 1]));
+                        } else {
+#pragma unroll
+                            for (int jj = 0; jj < 4; jj++) {
+                                const int n = n0 + jj;
+                                if (n < N)
+                                    __stcs(H + (((long)blk * K + n / P) * nAnt + ant) * P + n % P,
+                                           make_float2(d[jj][mt][2 * rr], d[jj][mt][2 * rr + 1]));
+                            }
+                        }
                     } else {
-                        __half2* H = reinterpret_cast<__half2*>(out);
-                        __stcs(reinterpret_cast<unsigned*>(H + ((long)blk * nAnt + ant) * N + n),
-                               h2bits(__floats2half2_rn(re, im)));
+                        unsigned* H = reinterpret_cast<unsigned*>(out) + ((long)blk * nAnt + ant) * N + n0;
+                        uint32_t v[4];
+#pragma unroll
+                        for (int jj = 0; jj < 4; jj++)
+                            v[jj] = h2bits(__floats2half2_rn(d[jj][mt][2 * rr], d[jj][mt][2 * rr + 1]));
+                        if (full && (N & 3) == 0) {
+                            __stcs(reinterpret_cast<uint4*>(H), make_uint4(v[0], v[1], v[2], v[3]));
+                        } else {
+#pragma unroll
+                            for (int jj = 0; jj < 4; jj++)
+                                if (n0 + jj < N) __stcs(H + jj, v[jj]);
+                        }
                     }
                 }
             }
@@ -169,11 +221,11 @@ static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, 
     auto kern = srs_filter_tc_kernel<KS, TO_CHANNEL>;
     const int s = allow_max_smem<srs_filter_tc_kernel<KS, TO_CHANNEL>>();
     if (s != AERIAL_OK) return s;
-    const int nTiles = (K * P + 3) / 4;
-    const int tileBytes = KS * 32 * 16;
-    const int NT = std::min(nTiles, kSrsSliceBytes / tileBytes);
-    const int slices = (nTiles + NT - 1) / NT;
-    const size_t smem = (size_t)NT * tileBytes;
+    const int nGroups = (K * P + 15) / 16;
+    const int groupBytes = KS * kSrsGroupBytes;
+    const int NQ = std::min(nGroups, kSrsSliceBytes / groupBytes);
+    const int slices = (nGroups + NQ - 1) / NQ;
+    const size_t smem = (size_t)NQ * groupBytes;
     int perSm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kSrsWarps * 32, smem);
     if (e != cudaSuccess) return (int)e;
@@ -184,7 +236,7 @@ static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, 
     gx = std::min(gx, ctasForItems);
     dim3 grid((unsigned)gx, (unsigned)slices);
     kern<<<grid, kSrsWarps * 32, smem, st>>>((const __half2*)SRS, (const __half2*)W, (const __half2*)FOCC, out,
-                                             nAnt, nBlocks, K, P, F, NT);
+                                             nAnt, nBlocks, K, P, F, NQ);
     return launch_status();
 }
 
