@@ -44,8 +44,8 @@
 namespace aeq {
 
 constexpr int kSrsWarps = 8;                 // warps per CTA
-constexpr int kSrsAntPerItem = 32;           // antennas per warp item (two m16 tiles)
-constexpr int kSrsMaxK = 48;
+constexpr int kSrsMaxK = 48;                 // taps of the SRS filter (H_est layout)
+constexpr int kChestMaxK = 96;               // pilots of the interpolation filter (channel layout)
 constexpr int kSrsSliceBytes = 96 * 1024;    // taps of one slice of output groups
 constexpr int kSrsGroupBytes = 4 * 32 * 16;  // one k-step of a group: 4 tiles x 32 lanes x 16 B
 
@@ -67,17 +67,19 @@ __device__ __forceinline__ void split_h2(float x, float y, uint32_t& hi, uint32_
     lo = h2bits(__floats2half2_rn(x - hf.x, y - hf.y));
 }
 
-// KS: k-steps of 8 complex taps (K <= 8 KS).  Grid: x = CTAs walking the
-// (block, 32-antenna) items, y = slices of NQ output groups (16 complex
-// outputs per group).
-template <int KS, bool TO_CHANNEL>
+// KS: k-steps of 8 complex taps (K <= 8 KS); MT: 16-antenna m-tiles per warp
+// item (two up to 48 taps, one above, to bound the A registers).  K input
+// taps per antenna, Ko filter outputs per block (Ko = K for the SRS filter).
+// Grid: x = CTAs walking the (block, 16 MT-antenna) items, y = slices of NQ
+// output groups (16 complex outputs per group).
+template <int KS, int MT, bool TO_CHANNEL>
 __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const __half2* __restrict__ srs,
                                                                           const __half2* __restrict__ W,
                                                                           const __half2* __restrict__ focc,
                                                                           void* __restrict__ out, int nAnt,
-                                                                          int nBlocks, int K, int P, int F, int NQ) {
+                                                                          int nBlocks, int K, int Ko, int P, int F, int NQ) {
     extern __shared__ uint4 bfrag[];            // [group][kstep][tile][lane]: {b0 hi, b1 hi, b0 lo, b1 lo}
-    const int N = K * P;                         // complex outputs per antenna
+    const int N = Ko * P;                        // complex outputs per antenna
     const int nGroups = (N + 15) / 16;
     const int q0 = blockIdx.y * NQ;
     const int nq = min(NQ, nGroups - q0);
@@ -106,18 +108,19 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
 
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, c = lane & 3;
-    const int antGroups = (nAnt + kSrsAntPerItem - 1) / kSrsAntPerItem;
+    constexpr int kAntPerItem = 16 * MT;
+    const int antGroups = (nAnt + kAntPerItem - 1) / kAntPerItem;
     const long items = (long)nBlocks * antGroups;
     const long nw = (long)gridDim.x * kSrsWarps;
     const uint32_t fb = (uint32_t)__cvta_generic_to_shared(bfrag) + lane * 16;
     const bool pairK = (K & 1) == 0;             // taps 2c, 2c + 1 of a row are one 8-byte load
     for (long it = (long)blockIdx.x * kSrsWarps + (threadIdx.x >> 5); it < items; it += nw) {
         const int blk = (int)(it / antGroups);
-        const int ant0 = (int)(it - (long)blk * antGroups) * kSrsAntPerItem;
+        const int ant0 = (int)(it - (long)blk * antGroups) * kAntPerItem;
         // A fragments: rows ant0 + 16 mt + g (+8 rr), taps 8 ks + 2c (+1)
-        uint32_t a[2][KS][4];
+        uint32_t a[MT][KS][4];
 #pragma unroll
-        for (int mt = 0; mt < 2; mt++) {
+        for (int mt = 0; mt < MT; mt++) {
 #pragma unroll
             for (int rr = 0; rr < 2; rr++) {
                 const int ant = ant0 + 16 * mt + g + 8 * rr;
@@ -143,11 +146,11 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
             }
         }
         for (int q = 0; q < nq; q++) {
-            float d[4][2][4];
+            float d[4][MT][4];
 #pragma unroll
             for (int jj = 0; jj < 4; jj++)
 #pragma unroll
-                for (int mt = 0; mt < 2; mt++)
+                for (int mt = 0; mt < MT; mt++)
 #pragma unroll
                     for (int r = 0; r < 4; r++) d[jj][mt][r] = 0.f;
 #pragma unroll
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
                                  : "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
                                  : "r"(fb + (uint32_t)(((q * KS + ks) * 4 + jj) * 512)));
 #pragma unroll
-                    for (int mt = 0; mt < 2; mt++) {
+                    for (int mt = 0; mt < MT; mt++) {
                         mma_f16(d[jj][mt], a[mt][ks][0], a[mt][ks][1], a[mt][ks][2], a[mt][ks][3], b.x, b.y);
                         mma_f16(d[jj][mt], a[mt][ks][0], a[mt][ks][1], a[mt][ks][2], a[mt][ks][3], b.z, b.w);
                     }
@@ -170,16 +173,16 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
             if (n0 >= N) continue;
             const bool full = n0 + 3 < N;
 #pragma unroll
-            for (int mt = 0; mt < 2; mt++) {
+            for (int mt = 0; mt < MT; mt++) {
 #pragma unroll
                 for (int rr = 0; rr < 2; rr++) {
                     const int ant = ant0 + 16 * mt + g + 8 * rr;
                     if (ant >= nAnt) continue;
                     if constexpr (TO_CHANNEL) {
-                        // H[sc = blk*K + ko][ant][layer = p], nLayers = P
+                        // H[sc = blk*Ko + ko][ant][layer = p], nLayers = P
                         float2* H = reinterpret_cast<float2*>(out);
                         if (P == 4 && full) {
-                            float2* dst = H + (((long)blk * K + n0 / 4) * nAnt + ant) * 4;
+                            float2* dst = H + (((long)blk * Ko + n0 / 4) * nAnt + ant) * 4;
                             __stcs(reinterpret_cast<float4*>(dst),
                                    make_float4(d[0][mt][2 * rr], d[0][mt][2 * rr + 1], d[1][mt][2 * rr],
                                                d[1][mt][2 * rr + 1]));
@@ -191,7 +194,7 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
                             for (int jj = 0; jj < 4; jj++) {
                                 const int n = n0 + jj;
                                 if (n < N)
-                                    __stcs(H + (((long)blk * K + n / P) * nAnt + ant) * P + n % P,
+                                    __stcs(H + (((long)blk * Ko + n / P) * nAnt + ant) * P + n % P,
                                            make_float2(d[jj][mt][2 * rr], d[jj][mt][2 * rr + 1]));
                             }
                         }
@@ -217,11 +220,12 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
 
 template <int KS, bool TO_CHANNEL>
 static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
-                         int nBlocks, int K, int P, int F, cudaStream_t st) {
-    auto kern = srs_filter_tc_kernel<KS, TO_CHANNEL>;
-    const int s = allow_max_smem<srs_filter_tc_kernel<KS, TO_CHANNEL>>();
+                         int nBlocks, int K, int Ko, int P, int F, cudaStream_t st) {
+    constexpr int MT = KS <= 6 ? 2 : 1;
+    auto kern = srs_filter_tc_kernel<KS, MT, TO_CHANNEL>;
+    const int s = allow_max_smem<srs_filter_tc_kernel<KS, MT, TO_CHANNEL>>();
     if (s != AERIAL_OK) return s;
-    const int nGroups = (K * P + 15) / 16;
+    const int nGroups = (Ko * P + 15) / 16;
     const int groupBytes = KS * kSrsGroupBytes;
     const int NQ = std::min(nGroups, kSrsSliceBytes / groupBytes);
     const int slices = (nGroups + NQ - 1) / NQ;
@@ -229,36 +233,53 @@ static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, 
     int perSm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kSrsWarps * 32, smem);
     if (e != cudaSuccess) return (int)e;
-    const long items = (long)nBlocks * ((nAnt + kSrsAntPerItem - 1) / kSrsAntPerItem);
+    const long items = (long)nBlocks * ((nAnt + 16 * MT - 1) / (16 * MT));
     const long ctasForItems = (items + kSrsWarps - 1) / kSrsWarps;
     // enough CTAs to fill the GPU once per slice; each walks its share of items
     long gx = std::max(1L, (long)sm_count() * std::max(1, perSm) / slices);
     gx = std::min(gx, ctasForItems);
     dim3 grid((unsigned)gx, (unsigned)slices);
     kern<<<grid, kSrsWarps * 32, smem, st>>>((const __half2*)SRS, (const __half2*)W, (const __half2*)FOCC, out,
-                                             nAnt, nBlocks, K, P, F, NQ);
+                                             nAnt, nBlocks, K, Ko, P, F, NQ);
     return launch_status();
 }
 
-template <bool TO_CHANNEL>
-static int launch_srs_ks(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
-                         int nBlocks, int K, int P, int F, cudaStream_t st) {
+// H_est layout (the SRS filter): up to 48 taps.
+static int launch_srs_est(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
+                          int nBlocks, int K, int P, int F, cudaStream_t st) {
     switch ((K + 7) / 8) {
-        case 1: return launch_srs_tc<1, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
-        case 2: return launch_srs_tc<2, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
-        case 3: return launch_srs_tc<3, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
-        case 4: return launch_srs_tc<4, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
-        case 5: return launch_srs_tc<5, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
-        default: return launch_srs_tc<6, TO_CHANNEL>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
+        case 1: return launch_srs_tc<1, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 2: return launch_srs_tc<2, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 3: return launch_srs_tc<3, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 4: return launch_srs_tc<4, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 5: return launch_srs_tc<5, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        default: return launch_srs_tc<6, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
     }
 }
 
-static int launch_srs(bool toChannel, void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC,
-                      int nAnt, int nBlocks, int K, int P, int F, cudaStream_t st) {
-    if (!out || !SRS || !W || !FOCC || nAnt < 1 || nBlocks < 1 || K < 1 || K > kSrsMaxK || P < 1 || P > 16 || F < 1)
-        return AERIAL_ERR_INVALID_ARG;
-    return toChannel ? launch_srs_ks<true>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st)
-                     : launch_srs_ks<false>(out, SRS, W, FOCC, nAnt, nBlocks, K, P, F, st);
+// Channel layout H[blk*Ko + ko][ant][p]: up to 96 input taps.
+static int launch_srs_chan(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
+                           int nBlocks, int K, int Ko, int P, int F, cudaStream_t st) {
+    switch ((K + 7) / 8) {
+        case 1: return launch_srs_tc<1, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 2: return launch_srs_tc<2, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 3: return launch_srs_tc<3, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 4: return launch_srs_tc<4, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 5: return launch_srs_tc<5, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 6: return launch_srs_tc<6, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 7: return launch_srs_tc<7, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 8: return launch_srs_tc<8, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 9: return launch_srs_tc<9, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 10: return launch_srs_tc<10, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 11: return launch_srs_tc<11, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        default: return launch_srs_tc<12, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+    }
+}
+
+static bool srs_args_ok(const void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
+                        int nBlocks, int K, int maxK, int Ko, int P, int F) {
+    return out && SRS && W && FOCC && nAnt >= 1 && nBlocks >= 1 && K >= 1 && K <= maxK && Ko >= 1 && Ko <= 4096 &&
+           P >= 1 && P <= 16 && F >= 1;
 }
 
 }  // namespace aeq
@@ -267,11 +288,20 @@ using namespace aeq;
 
 extern "C" int aerial_srs_filter(aerial_ch2* H_est, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC,
                                  int nAnt, int nBlocks, int K, int nPorts, int foccLen, void* stream) {
-    return launch_srs(false, H_est, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, to_stream(stream));
+    if (!srs_args_ok(H_est, SRS, W, FOCC, nAnt, nBlocks, K, kSrsMaxK, K, nPorts, foccLen)) return AERIAL_ERR_INVALID_ARG;
+    return launch_srs_est(H_est, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, to_stream(stream));
 }
 
 extern "C" int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, const aerial_ch2* W,
                                      const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts, int foccLen,
                                      void* stream) {
-    return launch_srs(true, H, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, to_stream(stream));
+    if (!srs_args_ok(H, SRS, W, FOCC, nAnt, nBlocks, K, kSrsMaxK, K, nPorts, foccLen)) return AERIAL_ERR_INVALID_ARG;
+    return launch_srs_chan(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
+}
+
+extern "C" int aerial_chest_interp(aerial_cf32* H, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC,
+                                   int nAnt, int nBlocks, int nPilot, int nOut, int nPorts, int occLen, void* stream) {
+    if (!srs_args_ok(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, kChestMaxK, nOut, nPorts, occLen))
+        return AERIAL_ERR_INVALID_ARG;
+    return launch_srs_chan(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
 }

@@ -415,6 +415,12 @@ def main():
         v, runs, el = cpu_chain_rate(orc, hc, a.cpu_seconds)
         cpu_base = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                     "sample": f"{runs} full slot(s) ({hc.nSC} subcarriers) in {el:.1f} s, OpenMP over subcarriers"}
+        if "srs_filter" in extras:
+            r, runs, el = srs_cpu_rate(orc, min(5.0, a.cpu_seconds))
+            extras["srs_filter"]["cpu_baseline"] = {
+                "value": r, "unit": "SRS blocks/s", "cores": cores, "kind": "port",
+                "sample": f"{runs} x the reference's 66-block launch (srs_filter_v1_scalar restated, FP16 "
+                          f"arithmetic) in {el:.1f} s, OpenMP over outputs"}
         if not half:
             try:   # the oracle as the checker of slot 0; reported, never fatal for the timing line
                 extras["accuracy_vs_fp64"] = accuracy_vs_fp64(orc, aeq, cells, llrs, descs, tun, stream)
@@ -672,6 +678,7 @@ def bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a):
     out["single_slot_latency_us"] = {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                                      "note": f"one {cells[0].nSC}-SC cell per launch, L2 flushed before each"}
     out["srs_filter"] = bench_srs(aeq, llrs[0].device, stream)
+    out["chest_interp"] = bench_chest(aeq, llrs[0].device, stream)
     return out
 
 
@@ -699,6 +706,66 @@ def accuracy_vs_fp64(orc, aeq, cells, llrs, descs, tun, stream):
     }
 
 
+def _time_launches(fn, stream, k=50):
+    import torch
+
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e3 / k
+
+
+def bench_chest(aeq, dev, stream):
+    """DMRS frequency-interpolation filter: the [64 x 96] x [96 x 4] product per output subcarrier named by the
+    reference (README.md:200) -- 64 antennas, 96 pilot REs and 96 output subcarriers per 8-PRB block, 4 ports,
+    OCC length 2 -- over 34 blocks (272 PRB) x 40 cells x 2 DMRS symbols = 2,720 blocks per launch, written as
+    the complex64 PUSCH channel (602 MB touched: larger than L2)."""
+    import torch
+
+    nPilot, nOut, P, F, nAnt = 96, 96, 4, 2, 64
+    nBlk = 34 * 40 * 2
+    g = torch.Generator(device=dev)
+    g.manual_seed(9)
+    yp = ((torch.rand(nBlk * nAnt * nPilot * 2, generator=g, device=dev) - 0.5) * 1.4).half()
+    wf = ((torch.rand(nOut * nPilot * 2, generator=g, device=dev) - 0.5) * 0.1).half()
+    occ = ((torch.rand(P * F * 2, generator=g, device=dev) - 0.5) * 1.4).half()
+    H = torch.empty(nBlk * nOut * nAnt * P, dtype=torch.complex64, device=dev)
+    us = _time_launches(lambda: aeq.chest_interp(H, yp, wf, occ, nAnt, nBlk, nPilot, nOut, P, F, stream), stream)
+    nbytes = 2 * (yp.numel() + wf.numel() + occ.numel()) + 8 * H.numel()
+    flops = 8.0 * nBlk * nAnt * nPilot * nOut * P
+    peak, kind = measured_peaks()
+    gbs = nbytes / (us * 1e-6) / 1e9
+    return {"us_per_launch": us, "blocks_per_launch": nBlk, "bytes_per_launch": nbytes,
+            "achieved_gbs": gbs, "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": kind,
+            "gflops": flops / (us * 1e-6) / 1e9, "tensor_gflops": 2 * flops / (us * 1e-6) / 1e9,
+            "shape": f"{nBlk} blocks x {nAnt} antennas, {nPilot} pilots -> {nOut} subcarriers x {P} ports, "
+                     f"OCC length {F}; FP16 in, complex64 channel out; tensor cores (FP16 operands, taps split "
+                     "hi/lo), FP32 accumulate"}
+
+
+def srs_cpu_rate(orc, seconds: float):
+    """The reference's srs_filter_v1_scalar (FP16 arithmetic) restated in C, on the host cores: SRS blocks/s on
+    the reference's own launch (66 blocks x 64 antennas, K = 24, 4 ports, FOCC length 8), repeated."""
+    K, P, F, nBlk, nAnt = 24, 4, 8, 66, 64
+    s, w, f = orc.ref_srs_inputs(42, nBlk * nAnt * K, K * K, P * F)
+    orc.srs_v1_f16(s, w, f, nAnt, nBlk, K, P, F)
+    t0 = time.perf_counter()
+    runs = 0
+    while True:
+        orc.srs_v1_f16(s, w, f, nAnt, nBlk, K, P, F)
+        runs += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return runs * nBlk / el, runs, el
+
+
 def bench_srs(aeq, dev, stream):
     """SRS filter multiply (srsFilterMultiply, src/srs/srs_wmma_bench.cu:57-90) at the reference's shape -- 66
     blocks x 64 antennas, K = 24 taps, 4 ports, FOCC length 8 -- for 40 cells x 4 SRS symbols per launch
@@ -713,22 +780,13 @@ def bench_srs(aeq, dev, stream):
     W = ((torch.rand(K * K * 2, generator=g, device=dev) - 0.5) * 1.4).half()
     focc = ((torch.rand(P * F * 2, generator=g, device=dev) - 0.5) * 1.4).half()
     out = torch.empty(nBlk * nAnt * K * P * 2, dtype=torch.float16, device=dev)
-    for _ in range(3):
-        aeq.srs_filter(out, srs, W, focc, nAnt, nBlk, K, P, F, stream)
-    torch.cuda.synchronize()
-    k = 50
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(k):
-        aeq.srs_filter(out, srs, W, focc, nAnt, nBlk, K, P, F, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    us = e0.elapsed_time(e1) * 1e3 / k
+    us = _time_launches(lambda: aeq.srs_filter(out, srs, W, focc, nAnt, nBlk, K, P, F, stream), stream)
     nbytes = 2 * (srs.numel() + W.numel() + focc.numel() + out.numel())
     flops = 8.0 * nBlk * nAnt * K * P * K
     peak, kind = measured_peaks()
     gbs = nbytes / (us * 1e-6) / 1e9
-    return {"us_per_launch": us, "blocks_per_launch": nBlk, "bytes_per_launch": nbytes,
+    return {"us_per_launch": us, "blocks_per_launch": nBlk, "blocks_per_s": nBlk / (us * 1e-6),
+            "bytes_per_launch": nbytes,
             "achieved_gbs": gbs, "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": kind,
             "gflops": flops / (us * 1e-6) / 1e9,
             "shape": f"{nBlk} blocks x {nAnt} antennas, K={K}, P={P}, FOCC length {F}, FP16 in/out, "

@@ -138,6 +138,22 @@ int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, const aerial_ch
                           const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts,
                           int foccLen, void* stream);
 
+/* Frequency-interpolation filter of DMRS channel estimation, straight into
+ * the PUSCH channel layout (complex64):
+ *   H[blk*nOut + o][ant][p] = sum_k Wf[o][k] * OCC[p][k % occLen] * Yp[blk][ant][k]
+ * for k < nPilot (<= 96) received pilot REs per filter block and nOut output
+ * subcarriers per block; Wf is [nOut][nPilot], OCC [nPorts][occLen], all
+ * complex half.  This is the [64 x 96] x [96 x 4] GEMM per output subcarrier
+ * (64 antennas, 96 pilots, 4 ports, batched over subcarriers, symbols and
+ * blocks) that the reference names as future work (README.md:200, cuPHY
+ * channel_est.cu, not in the reference); it has no reference kernel, and the
+ * sum is the SRS filter multiply's with nOut != nPilot allowed (nOut ==
+ * nPilot gives aerial_srs_to_channel's result bit for bit).  FP32
+ * accumulation. */
+int aerial_chest_interp(aerial_cf32* H, const aerial_ch2* Yp, const aerial_ch2* Wf,
+                        const aerial_ch2* OCC, int nAnt, int nBlocks, int nPilot, int nOut,
+                        int nPorts, int occLen, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Fused chain: Gram -> FP32 MMSE solve -> apply -> LLR in one kernel; G, C */
 /* and Y_eq stay on chip, only LLRs (and optionally Y_eq) are written.       */

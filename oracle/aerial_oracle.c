@@ -705,3 +705,35 @@ void orc_srs_f64(const uint16_t* srs, const uint16_t* W, const uint16_t* focc, d
         out[2 * i + 1] = ei;
     }
 }
+
+/* FP64 frequency-interpolation filter of DMRS channel estimation, written in
+ * the PUSCH channel layout: H[blk*nOut + o][ant][p] = sum_{k < nPilot}
+ * Wf[o][k] * OCC[p][k % F] * Yp[blk][ant][k] on the FP16 inputs.  No
+ * reference kernel exists for it (the reference names it as future work,
+ * README.md:200); it is the SRS filter multiply above with nOut output
+ * subcarriers per block instead of K, so nOut == nPilot reproduces
+ * orc_srs_f64 transposed into [sc][ant][port]. */
+void orc_chest_f64(const uint16_t* yp, const uint16_t* Wf, const uint16_t* occ, double* out, int nAnt,
+                   int nBlocks, int nPilot, int nOut, int P, int F) {
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nBlocks * nOut * nAnt * P; i++) {
+        int p = (int)(i % P);
+        long ant = (i / P) % nAnt;
+        long o = (i / ((long)P * nAnt)) % nOut;
+        long blk = i / ((long)P * nAnt * nOut);
+        const uint16_t* s = yp + 2 * ((blk * nAnt + ant) * nPilot);
+        const uint16_t* w = Wf + 2 * (o * nPilot);
+        const uint16_t* f = occ + 2 * ((long)p * F);
+        double er = 0, ei = 0;
+        for (int k = 0; k < nPilot; k++) {
+            double ar = h2f(w[2 * k]), ai = h2f(w[2 * k + 1]);
+            double br = h2f(f[2 * (k % F)]), bi = h2f(f[2 * (k % F) + 1]);
+            double wr = ar * br - ai * bi, wi = ar * bi + ai * br;
+            double sr = h2f(s[2 * k]), si = h2f(s[2 * k + 1]);
+            er += wr * sr - wi * si;
+            ei += wr * si + wi * sr;
+        }
+        out[2 * i] = er;
+        out[2 * i + 1] = ei;
+    }
+}

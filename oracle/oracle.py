@@ -13,6 +13,7 @@ Reference functions restated (paths inside ebaenamar/aerial-mimo-tc-optimization
   llr_v1_baseline        src/llr/aerial_llr_v3.cu:84-108
   cpu_ref (FP64)         src/llr/aerial_llr_v3.cu:61-79
   srs_filter_v1_scalar   src/srs/srs_wmma_bench.cu:57-90   (FP16 arithmetic)
+plus an FP64 DMRS interpolation filter (no reference kernel; README.md:200).
 """
 from __future__ import annotations
 
@@ -63,6 +64,7 @@ def lib():
         "orc_chain_f64": (None, [_f32p, _f32p, ctypes.c_double, _L, _I, _I, _I, _I, _f64p, _f64p, _f64p]),
         "orc_srs_v1_f16": (None, [_u16p, _u16p, _u16p, _u16p, _I, _I, _I, _I, _I]),
         "orc_srs_f64": (None, [_u16p, _u16p, _u16p, _f64p, _I, _I, _I, _I, _I]),
+        "orc_chest_f64": (None, [_u16p, _u16p, _u16p, _f64p, _I, _I, _I, _I, _I, _I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -216,4 +218,12 @@ def srs_f64(srs_u16, w_u16, focc_u16, n_ant, n_blocks, K, P, F) -> np.ndarray:
     out = np.empty(2 * n_blocks * n_ant * K * P, np.float64)
     lib().orc_srs_f64(_c(srs_u16, np.uint16), _c(w_u16, np.uint16), _c(focc_u16, np.uint16), out,
                       n_ant, n_blocks, K, P, F)
+    return out.view(np.complex128)
+
+
+def chest_f64(yp_u16, wf_u16, occ_u16, n_ant, n_blocks, n_pilot, n_out, P, F) -> np.ndarray:
+    """FP64 DMRS interpolation filter in the channel layout [blk*n_out + o][ant][p] (no reference kernel)."""
+    out = np.empty(2 * n_blocks * n_out * n_ant * P, np.float64)
+    lib().orc_chest_f64(_c(yp_u16, np.uint16), _c(wf_u16, np.uint16), _c(occ_u16, np.uint16), out,
+                        n_ant, n_blocks, n_pilot, n_out, P, F)
     return out.view(np.complex128)

@@ -54,6 +54,10 @@ def test_invalid_arguments_rejected_before_any_launch():
     assert lib.aerial_llr(fake, fake, fake, 10, 5, None) == 1001       # nPamBits > 4
     assert lib.aerial_coef_apply(fake, fake, fake, 10, 17, 8, 64, None) == 1001   # nSym > 16
     assert lib.aerial_coef_apply(fake, fake, fake, 10, 11, 17, 64, None) == 1001  # nLayers > 16
+    assert lib.aerial_srs_filter(fake, fake, fake, fake, 64, 66, 49, 4, 8, None) == 1001   # K > 48
+    assert lib.aerial_chest_interp(fake, fake, fake, fake, 64, 34, 97, 96, 4, 4, None) == 1001  # nPilot > 96
+    assert lib.aerial_chest_interp(fake, fake, fake, fake, 64, 34, 96, 0, 4, 4, None) == 1001   # nOut < 1
+    assert lib.aerial_chest_interp(None, fake, fake, fake, 64, 34, 96, 96, 4, 4, None) == 1001
     cells = (pkg.CellDesc * 1)()
     assert lib.aerial_pusch_eq_fused(cells, 1, None, None) == 1001     # null buffers
     assert lib.aerial_pusch_eq_fused(cells, 0, None, None) == 1001

@@ -53,6 +53,36 @@ def test_srs_to_channel_layout(aeq, orc, cuda):
     assert evm_db(H.cpu().numpy(), ref) < -120
 
 
+# DMRS interpolation filter: (nPilot, nOut, ports, OCC length, antennas).  96 pilots x 4 ports over 64
+# antennas is the [64 x 96] x [96 x 4] product of the reference's README.md:200.
+CHEST_CFGS = [(96, 96, 4, 4, 64), (48, 96, 2, 2, 64), (96, 48, 4, 2, 33), (24, 12, 1, 1, 16), (56, 40, 3, 5, 48)]
+
+
+@pytest.mark.parametrize("nPilot,nOut,P,F,nAnt", CHEST_CFGS)
+def test_chest_interp_vs_fp64(aeq, orc, cuda, nPilot, nOut, P, F, nAnt):
+    nBlk = 7
+    s, w, f = orc.ref_srs_inputs(11, nBlk * nAnt * nPilot, nOut * nPilot, P * F)
+    H = torch.empty(nBlk * nOut, nAnt, P, dtype=torch.complex64, device=cuda)
+    aeq.chest_interp(H, _d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda),
+                     nAnt, nBlk, nPilot, nOut, P, F)
+    torch.cuda.synchronize()
+    ref = orc.chest_f64(s, w, f, nAnt, nBlk, nPilot, nOut, P, F).reshape(nBlk * nOut, nAnt, P)
+    # taps split into two FP16 parts, FP32 accumulation: the error of an FP32 sum
+    assert evm_db(H.cpu().numpy(), ref) < -120
+
+
+def test_chest_interp_square_filter_equals_srs_to_channel(aeq, orc, cuda):
+    K, P, F, nBlk, nAnt = 24, 4, 8, 66, 64
+    s, w, f = orc.ref_srs_inputs(43, nBlk * nAnt * K, K * K, P * F)
+    args = (_d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda))
+    H1 = torch.empty(nBlk * K, nAnt, P, dtype=torch.complex64, device=cuda)
+    H2 = torch.empty_like(H1)
+    aeq.srs_to_channel(H1, *args, nAnt, nBlk, K, P, F)
+    aeq.chest_interp(H2, *args, nAnt, nBlk, K, K, P, F)
+    torch.cuda.synchronize()
+    assert torch.equal(H1, H2)
+
+
 @pytest.mark.parametrize("shape", [(1584, 11, 8, 64), (288, 11, 4, 32), (48, 14, 16, 128), (12, 3, 5, 33)])
 def test_coef_apply_tc_vs_v2_model(aeq, orc, cuda, shape):
     nSC, S, L, A = shape

@@ -136,6 +136,17 @@ def test_srs_f16_restatement_close_to_fp64(orc, K, P, F):
     assert cosine(v16.view(np.complex64), o64) > 0.9999
 
 
+def test_chest_f64_square_filter_is_the_srs_filter(orc):
+    """The interpolation model with nOut == nPilot is the SRS filter multiply
+    (srs_filter_v1_scalar's sum, src/srs/srs_wmma_bench.cu:57-90) in the
+    channel layout [blk*K + k_out][ant][port]."""
+    K, P, F, nBlk, nAnt = 24, 4, 8, 3, 16
+    s, w, f = orc.ref_srs_inputs(5, nBlk * nAnt * K, K * K, P * F)
+    srs = orc.srs_f64(s, w, f, nAnt, nBlk, K, P, F).reshape(nBlk, nAnt, K, P).transpose(0, 2, 1, 3)
+    ch = orc.chest_f64(s, w, f, nAnt, nBlk, K, K, P, F).reshape(nBlk, K, nAnt, P)
+    np.testing.assert_array_equal(ch, srs)
+
+
 # ---------------------------------------------------------------------------
 # The oracle against the reference's OWN kernels run on a B200 (compiled
 # unchanged for sm_100a): SHA-256 of the full-size outputs, regenerated here
