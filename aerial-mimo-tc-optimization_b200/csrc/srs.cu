@@ -38,6 +38,10 @@
 // fragments (two 16-antenna m-tiles, the whole K) are loaded once from global
 // memory, then it sweeps the slice's groups.
 #include <algorithm>
+#include <mutex>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "common.cuh"
 
@@ -218,6 +222,311 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
     }
 }
 
+// ---------------------------------------------------------------------------
+// The interpolation filter on the 5th-generation tensor cores (tcgen05).
+//
+// The filter taps are shared by every block, so blocks stack along M with no
+// wasted products: one GEMM C[m][n] = sum_k A[m][k] B[k][n] with m = (block,
+// antenna) rows of the pilot input as stored (row-major, K = (pilot, re/im)
+// interleaved FP16: K-major), and n = (output subcarrier, port, re/im).
+//   - A tiles of 128 rows x 64 K arrive by TMA with the 128-byte swizzle, the
+//     canonical K-major layout of the UMMA shared-memory descriptor.
+//   - B (taps, real-embedded as in the mma.sync kernel, split hi/lo) is built
+//     once per CTA in shared memory in the same swizzled layout, for the
+//     CTA's tile of 128 real output columns (64 complex outputs).
+//   - One elected thread issues tcgen05.mma (M = 128, N = 128, K = 16, FP16
+//     operands, FP32 accumulate in TMEM): the hi products then the lo
+//     products into one accumulator.  Two TMEM accumulators (256 columns) let
+//     the epilogue of one M tile overlap the MMAs of the next.
+//   - Warps 2-5 read the accumulator rows with tcgen05.ld (one TMEM lane =
+//     one (block, antenna) row per thread) and store the channel layout;
+//     for 4 ports a thread's 4 consecutive outputs are one 32-byte store and
+//     a warp's 32 antennas are 1 KB contiguous.
+// Warp roles: 0 = TMA producer, 1 = TMEM owner + MMA issuer, 2-5 = epilogue.
+// Every wait is bounded: on a timeout the CTA raises an abort flag, every
+// role leaves its loop, and the kernel still frees its TMEM and returns
+// (counted in g_umma_timeouts).
+// ---------------------------------------------------------------------------
+constexpr int kUmmaM = 128;                  // rows per M tile (TMEM lanes)
+constexpr int kUmmaN = 128;                  // real output columns per CTA tile
+constexpr int kUmmaKB = 64;                  // K elements per swizzle atom (128 bytes of FP16)
+constexpr int kUmmaAtomBytes = kUmmaM * 128; // one 128 x 64 FP16 atom column block: 16 KB
+constexpr int kUmmaThreads = 192;
+constexpr long kUmmaWaitLimit = 1L << 22;    // mbarrier polls before a wait gives up
+
+__device__ unsigned g_umma_timeouts;         // waits that gave up (diagnostic; stays 0)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
+    for (long i = 0; i < kUmmaWaitLimit; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if ((i & 1023) == 1023 && *abort) return false;
+    }
+    *abort = 1;
+    atomicAdd(&g_umma_timeouts, 1u);
+    return false;
+}
+
+// UMMA shared-memory descriptor, K-major, 128-byte swizzle: start address,
+// LBO = 16 B (unused by swizzled K-major), SBO = 1024 B (8 rows of 128 B),
+// version 1, base offset 0, layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+// Instruction descriptor, kind::f16: FP32 accumulator, FP16 A and B, both
+// K-major, N = 128, M = 128.
+constexpr uint32_t kUmmaIdesc = (1u << 4) | ((uint32_t)(kUmmaN >> 3) << 17) | ((uint32_t)(kUmmaM >> 4) << 24);
+
+// Byte offset of FP16 element (row r, k) in a K-major 128-byte-swizzled atom
+// column block of 128-byte rows (k < 64): 16-byte chunk index XOR (r mod 8).
+__device__ __forceinline__ uint32_t sw128_off(int r, int k) {
+    return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) ^ r) & 7) << 4) + (k & 7) * 2);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                                      const __half2* __restrict__ Wf,
+                                                                      const __half2* __restrict__ occ,
+                                                                      float2* __restrict__ H, int nAnt, int nBlocks,
+                                                                      int nPilot, int nOut, int P, int F) {
+    extern __shared__ __align__(1024) uint8_t usm_raw[];
+    // 128-byte swizzle atoms must start on 1024-byte boundaries of the shared window
+    uint8_t* usm = usm_raw + ((1024u - (smem_u32(usm_raw) & 1023u)) & 1023u);
+    // layout: A stages [2][KB atoms] | B [hi, lo][KB atoms] | barriers | TMEM slot
+    uint8_t* sA = usm;
+    uint8_t* sB = usm + 2 * KB * kUmmaAtomBytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + 2 * KB * kUmmaAtomBytes);
+    // bars: full[2], empty[2], tfull[2], tempty[2]
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 8);
+    volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int N = nOut * P;                       // complex outputs per row
+    const int nt = blockIdx.y;                    // tile of 64 complex outputs
+    const long M = (long)nBlocks * nAnt;
+    const long nMT = (M + kUmmaM - 1) / kUmmaM;
+
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 8; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bars + b)),
+                         "r"(b >= 6 ? 4 : 1));   // tempty: one arrival per epilogue warp
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;\n" ::"r"(smem_u32(tslot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
+    }
+    // B tile: rows r = 2 j + (re/im output) for complex output n = 64 nt + j,
+    // K columns 2 kc + (re/im input); (Re T, -Im T) / (Im T, Re T) pairs.
+    for (int e = threadIdx.x; e < 64 * nPilot; e += blockDim.x) {
+        const int j = e / nPilot, kc = e - j * nPilot;
+        const int n = 64 * nt + j;
+        float2 t = make_float2(0.f, 0.f);
+        if (n < N) {
+            const float2 w = __half22float2(Wf[(n / P) * nPilot + kc]);
+            const float2 f = __half22float2(occ[(n % P) * F + (kc % F)]);
+            t = make_float2(w.x * f.x - w.y * f.y, w.x * f.y + w.y * f.x);
+        }
+        uint32_t hi0, lo0, hi1, lo1;
+        split_h2(t.x, -t.y, hi0, lo0);           // row 2j: Re out
+        split_h2(t.y, t.x, hi1, lo1);            // row 2j+1: Im out
+        const int k = 2 * kc, kb = k >> 6, kin = k & 63;
+        uint8_t* bh = sB + kb * kUmmaAtomBytes;
+        uint8_t* bl = sB + (KB + kb) * kUmmaAtomBytes;
+        *reinterpret_cast<uint32_t*>(bh + sw128_off(2 * j, kin)) = hi0;
+        *reinterpret_cast<uint32_t*>(bl + sw128_off(2 * j, kin)) = lo0;
+        *reinterpret_cast<uint32_t*>(bh + sw128_off(2 * j + 1, kin)) = hi1;
+        *reinterpret_cast<uint32_t*>(bl + sw128_off(2 * j + 1, kin)) = lo1;
+    }
+    // rows 128..: none (64 outputs x 2 = 128 rows exactly); K beyond 2 nPilot inside the last atom is never read
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tbase = *tslot;
+
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + 2), tfull0 = smem_u32(bars + 4),
+                   tempty0 = smem_u32(bars + 6);
+    if (warp == 0) {
+        if (lane == 0) {
+            long i = 0;
+            for (long mt = blockIdx.x; mt < nMT && !*abort; mt += gridDim.x, i++) {
+                const int s = (int)(i & 1);
+                if (!mbar_wait(empty0 + 8 * s, (uint32_t)(((i >> 1) & 1) ^ 1), abort)) break;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(full0 + 8 * s),
+                             "r"(KB * kUmmaAtomBytes)
+                             : "memory");
+#pragma unroll
+                for (int kb = 0; kb < KB; kb++)
+                    asm volatile(
+                        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                        "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(sA + (s * KB + kb) * kUmmaAtomBytes)),
+                        "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(kb * kUmmaKB), "r"((int)(mt * kUmmaM)),
+                        "r"(full0 + 8 * s)
+                        : "memory");
+            }
+            // leave no copy in flight: the last two stages' loads have landed
+            for (long d = (i > 2 ? i - 2 : 0); d < i; d++) mbar_wait(full0 + 8 * (d & 1), (uint32_t)((d >> 1) & 1), abort);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            long i = 0;
+            for (long mt = blockIdx.x; mt < nMT && !*abort; mt += gridDim.x, i++) {
+                const int s = (int)(i & 1), a = (int)(i & 1);
+                const uint32_t ph = (uint32_t)((i >> 1) & 1);
+                if (!mbar_wait(tempty0 + 8 * a, ph ^ 1, abort)) break;
+                if (!mbar_wait(full0 + 8 * s, ph, abort)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t dt = tbase + (uint32_t)(a * kUmmaN);
+                const uint32_t a0 = smem_u32(sA + s * KB * kUmmaAtomBytes);
+                const uint32_t b0 = smem_u32(sB);
+#pragma unroll
+                for (int part = 0; part < 2; part++) {
+#pragma unroll
+                    for (int kb = 0; kb < KB; kb++) {
+#pragma unroll
+                        for (int kk = 0; kk < kUmmaKB / 16; kk++) {
+                            const uint64_t ad = umma_desc_sw128(a0 + kb * kUmmaAtomBytes + kk * 32);
+                            const uint64_t bd = umma_desc_sw128(b0 + (part * KB + kb) * kUmmaAtomBytes + kk * 32);
+                            const uint32_t acc = (part | kb | kk) ? 1u : 0u;
+                            asm volatile(
+                                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dt),
+                                "l"(ad), "l"(bd), "r"(kUmmaIdesc), "r"(acc)
+                                : "memory");
+                        }
+                    }
+                }
+                // stage s is free and accumulator a is full once these MMAs complete
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                                 empty0 + 8 * s)
+                             : "memory");
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                                 tfull0 + 8 * a)
+                             : "memory");
+            }
+        }
+    } else {
+        // epilogue: TMEM sub-partition (warp mod 4) holds rows 32 (warp mod 4) .. +31
+        const int sp = warp & 3;
+        const int row = sp * 32 + lane;
+        long i = 0;
+        for (long mt = blockIdx.x; mt < nMT && !*abort; mt += gridDim.x, i++) {
+            const int a = (int)(i & 1);
+            if (!mbar_wait(tfull0 + 8 * a, (uint32_t)((i >> 1) & 1), abort)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const long m = mt * kUmmaM + row;
+            const bool mv = m < M;
+            const int blk = mv ? (int)(m / nAnt) : 0;
+            const int ant = mv ? (int)(m - (long)blk * nAnt) : 0;
+#pragma unroll 1
+            for (int c = 0; c < kUmmaN / 32; c++) {
+                uint32_t v[32];
+                const uint32_t ta = tbase + ((uint32_t)(sp * 32) << 16) + (uint32_t)(a * kUmmaN + c * 32);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];\n"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                      "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                      "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                      "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(ta));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                if (!mv) continue;
+                const int nb = 64 * nt + 16 * c;  // complex outputs nb .. nb + 15 of this row
+                if (P == 4) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (nb + 4 * q >= N) break;
+                        float4* dst = reinterpret_cast<float4*>(
+                            H + (((long)blk * nOut + (nb >> 2) + q) * nAnt + ant) * 4);
+                        __stcs(dst, make_float4(__uint_as_float(v[8 * q]), __uint_as_float(v[8 * q + 1]),
+                                                __uint_as_float(v[8 * q + 2]), __uint_as_float(v[8 * q + 3])));
+                        __stcs(dst + 1, make_float4(__uint_as_float(v[8 * q + 4]), __uint_as_float(v[8 * q + 5]),
+                                                    __uint_as_float(v[8 * q + 6]), __uint_as_float(v[8 * q + 7])));
+                    }
+                } else {
+#pragma unroll
+                    for (int jj = 0; jj < 16; jj++) {
+                        const int n = nb + jj;
+                        if (n < N)
+                            __stcs(H + (((long)blk * nOut + n / P) * nAnt + ant) * P + n % P,
+                                   make_float2(__uint_as_float(v[2 * jj]), __uint_as_float(v[2 * jj + 1])));
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(tempty0 + 8 * a) : "memory");
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;\n" ::"r"(tbase));
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Shapes the tcgen05 kernel takes: whole 64-element K atoms (nPilot a
+// multiple of 32, up to 96) and a 16-byte aligned pilot array.
+static bool chest_umma_ok(const aerial_ch2* Yp, int nPilot) {
+    return nPilot % 32 == 0 && nPilot <= 96 && (reinterpret_cast<uintptr_t>(Yp) & 15) == 0;
+}
+
+template <int KB>
+static int launch_chest_umma(float2* H, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
+                             int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
+    auto enc = tensor_map_encoder();
+    if (!enc) return AERIAL_ERR_UNSUPPORTED;
+    const long M = (long)nBlocks * nAnt;
+    CUtensorMap tm;
+    const cuuint64_t dims[2] = {(cuuint64_t)(2 * nPilot), (cuuint64_t)M};
+    const cuuint64_t strides[1] = {(cuuint64_t)(4 * nPilot)};
+    const cuuint32_t box[2] = {(cuuint32_t)kUmmaKB, (cuuint32_t)kUmmaM};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<aerial_ch2*>(Yp), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return AERIAL_ERR_UNSUPPORTED;
+    const int s = allow_max_smem<chest_umma_kernel<KB>>();
+    if (s != AERIAL_OK) return s;
+    // + barriers, TMEM slot, abort flag and the 1024-byte alignment slack; at
+    // least 120 KB so one CTA (256 TMEM columns) runs per SM
+    const size_t smem = std::max<size_t>((size_t)4 * KB * kUmmaAtomBytes + 8 * sizeof(uint64_t) + 16 + 1024,
+                                         120 * 1024);
+    const int nNT = (2 * nOut * P + kUmmaN - 1) / kUmmaN;
+    const long nMT = (M + kUmmaM - 1) / kUmmaM;
+    long gx = std::max(1L, (long)sm_count() / nNT);
+    gx = std::min(gx, nMT);
+    dim3 grid((unsigned)gx, (unsigned)nNT);
+    chest_umma_kernel<KB><<<grid, kUmmaThreads, smem, st>>>(tm, (const __half2*)Wf, (const __half2*)OCC, H, nAnt,
+                                                            nBlocks, nPilot, nOut, P, F);
+    return launch_status();
+}
+
 template <int KS, bool TO_CHANNEL>
 static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
                          int nBlocks, int K, int Ko, int P, int F, cudaStream_t st) {
@@ -303,5 +612,13 @@ extern "C" int aerial_chest_interp(aerial_cf32* H, const aerial_ch2* Yp, const a
                                    int nAnt, int nBlocks, int nPilot, int nOut, int nPorts, int occLen, void* stream) {
     if (!srs_args_ok(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, kChestMaxK, nOut, nPorts, occLen))
         return AERIAL_ERR_INVALID_ARG;
+    if (chest_umma_ok(Yp, nPilot)) {
+        float2* h = reinterpret_cast<float2*>(H);
+        switch (nPilot / 32) {
+            case 1: return launch_chest_umma<1>(h, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
+            case 2: return launch_chest_umma<2>(h, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
+            default: return launch_chest_umma<3>(h, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
+        }
+    }
     return launch_srs_chan(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
 }

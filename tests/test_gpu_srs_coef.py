@@ -55,7 +55,9 @@ def test_srs_to_channel_layout(aeq, orc, cuda):
 
 # DMRS interpolation filter: (nPilot, nOut, ports, OCC length, antennas).  96 pilots x 4 ports over 64
 # antennas is the [64 x 96] x [96 x 4] product of the reference's README.md:200.
-CHEST_CFGS = [(96, 96, 4, 4, 64), (48, 96, 2, 2, 64), (96, 48, 4, 2, 33), (24, 12, 1, 1, 16), (56, 40, 3, 5, 48)]
+# Pilot counts that are multiples of 32 (up to 96) run the tcgen05 kernel, the others the mma.sync kernel.
+CHEST_CFGS = [(96, 96, 4, 4, 64), (48, 96, 2, 2, 64), (96, 48, 4, 2, 33), (24, 12, 1, 1, 16), (56, 40, 3, 5, 48),
+              (64, 64, 2, 2, 64), (32, 20, 3, 3, 40)]
 
 
 @pytest.mark.parametrize("nPilot,nOut,P,F,nAnt", CHEST_CFGS)
@@ -69,6 +71,23 @@ def test_chest_interp_vs_fp64(aeq, orc, cuda, nPilot, nOut, P, F, nAnt):
     ref = orc.chest_f64(s, w, f, nAnt, nBlk, nPilot, nOut, P, F).reshape(nBlk * nOut, nAnt, P)
     # taps split into two FP16 parts, FP32 accumulation: the error of an FP32 sum
     assert evm_db(H.cpu().numpy(), ref) < -120
+
+
+def test_chest_interp_many_tiles_per_cta(aeq, orc, cuda):
+    """200 blocks x 64 antennas: every CTA of the tcgen05 kernel walks several M tiles, so both operand stages
+    and both TMEM accumulators are reused across phases."""
+    nPilot, nOut, P, F, nAnt, nBlk = 96, 96, 4, 2, 64, 200
+    s, w, f = orc.ref_srs_inputs(12, nBlk * nAnt * nPilot, nOut * nPilot, P * F)
+    H = torch.empty(nBlk * nOut, nAnt, P, dtype=torch.complex64, device=cuda)
+    args = (_d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda))
+    aeq.chest_interp(H, *args, nAnt, nBlk, nPilot, nOut, P, F)
+    torch.cuda.synchronize()
+    first = H.clone()
+    ref = orc.chest_f64(s, w, f, nAnt, nBlk, nPilot, nOut, P, F).reshape(nBlk * nOut, nAnt, P)
+    assert evm_db(H.cpu().numpy(), ref) < -120
+    aeq.chest_interp(H, *args, nAnt, nBlk, nPilot, nOut, P, F)        # deterministic across calls
+    torch.cuda.synchronize()
+    assert torch.equal(H, first)
 
 
 def test_chest_interp_square_filter_equals_srs_to_channel(aeq, orc, cuda):
