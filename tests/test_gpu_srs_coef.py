@@ -90,6 +90,29 @@ def test_chest_interp_many_tiles_per_cta(aeq, orc, cuda):
     assert torch.equal(H, first)
 
 
+def test_chest_interp_and_srs_to_channel_on_offset_channel_pointers(aeq, orc, cuda):
+    """A channel array that starts one complex into an allocation (8-byte aligned only) takes the per-element
+    stores: same values as the aligned launch, and the element before the array is left alone."""
+    for nPilot, K in ((96, None), (None, 24)):
+        P, F, nAnt, nBlk = 4, 2, 64, 5
+        kin = nPilot or K
+        nOut = nPilot or K
+        s, w, f = orc.ref_srs_inputs(13, nBlk * nAnt * kin, nOut * kin, P * F)
+        args = (_d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda))
+        n = nBlk * nOut * nAnt * P
+        base = torch.full((n + 1,), 7 + 7j, dtype=torch.complex64, device=cuda)
+        ref = torch.empty(n, dtype=torch.complex64, device=cuda)
+        if nPilot:
+            aeq.chest_interp(base[1:], *args, nAnt, nBlk, nPilot, nOut, P, F)
+            aeq.chest_interp(ref, *args, nAnt, nBlk, nPilot, nOut, P, F)
+        else:
+            aeq.srs_to_channel(base[1:], *args, nAnt, nBlk, K, P, F)
+            aeq.srs_to_channel(ref, *args, nAnt, nBlk, K, P, F)
+        torch.cuda.synchronize()
+        assert torch.equal(base[1:], ref)
+        assert base[0].item() == 7 + 7j
+
+
 def test_chest_interp_square_filter_equals_srs_to_channel(aeq, orc, cuda):
     K, P, F, nBlk, nAnt = 24, 4, 8, 66, 64
     s, w, f = orc.ref_srs_inputs(43, nBlk * nAnt * K, K * K, P * F)
