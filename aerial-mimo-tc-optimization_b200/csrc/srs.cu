@@ -295,11 +295,13 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
     return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) ^ r) & 7) << 4) + (k & 7) * 2);
 }
 
-template <int KB>
+// KB: 64-element K atoms (2 nPilot <= 64 KB); OUT16: write the SRS filter's
+// FP16 H_est[blk][ant][k_out][p] layout instead of the complex64 channel.
+template <int KB, bool OUT16>
 __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                                       const __half2* __restrict__ Wf,
                                                                       const __half2* __restrict__ occ,
-                                                                      float2* __restrict__ H, int nAnt, int nBlocks,
+                                                                      void* __restrict__ out, int nAnt, int nBlocks,
                                                                       int nPilot, int nOut, int P, int F) {
     extern __shared__ __align__(1024) uint8_t usm_raw[];
     // 128-byte swizzle atoms must start on 1024-byte boundaries of the shared window
@@ -328,6 +330,10 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;\n" ::"r"(smem_u32(tslot)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
     }
+    // B's K columns past 2 nPilot inside the last atom must read as zero
+    for (int e = threadIdx.x; e < 2 * KB * kUmmaAtomBytes / 16; e += blockDim.x)
+        reinterpret_cast<uint4*>(sB)[e] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
     // B tile: rows r = 2 j + (re/im output) for complex output n = 64 nt + j,
     // K columns 2 kc + (re/im input); (Re T, -Im T) / (Im T, Re T) pairs.
     for (int e = threadIdx.x; e < 64 * nPilot; e += blockDim.x) {
@@ -350,7 +356,6 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
         *reinterpret_cast<uint32_t*>(bh + sw128_off(2 * j + 1, kin)) = hi1;
         *reinterpret_cast<uint32_t*>(bl + sw128_off(2 * j + 1, kin)) = lo1;
     }
-    // rows 128..: none (64 outputs x 2 = 128 rows exactly); K beyond 2 nPilot inside the last atom is never read
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
@@ -398,6 +403,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
                     for (int kb = 0; kb < KB; kb++) {
 #pragma unroll
                         for (int kk = 0; kk < kUmmaKB / 16; kk++) {
+                            if (kb * kUmmaKB + kk * 16 >= 2 * nPilot) break;   // K steps past the pilots
                             const uint64_t ad = umma_desc_sw128(a0 + kb * kUmmaAtomBytes + kk * 32);
                             const uint64_t bd = umma_desc_sw128(b0 + (part * KB + kb) * kUmmaAtomBytes + kk * 32);
                             const uint32_t acc = (part | kb | kk) ? 1u : 0u;
@@ -448,6 +454,28 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
                 asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
                 if (!mv) continue;
                 const int nb = 64 * nt + 16 * c;  // complex outputs nb .. nb + 15 of this row
+                if constexpr (OUT16) {
+                    // H_est[blk][ant][n]: the row's 16 outputs are 64 contiguous bytes of half2
+                    uint32_t h[16];
+#pragma unroll
+                    for (int jj = 0; jj < 16; jj++)
+                        h[jj] = h2bits(__floats2half2_rn(__uint_as_float(v[2 * jj]), __uint_as_float(v[2 * jj + 1])));
+                    uint32_t* dst = reinterpret_cast<uint32_t*>(out) + m * N + nb;
+                    if (nb + 16 <= N && (N & 7) == 0 && (reinterpret_cast<uintptr_t>(out) & 31) == 0) {
+#pragma unroll
+                        for (int hh = 0; hh < 2; hh++)
+                            asm volatile("st.global.cs.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"l"(dst + 8 * hh),
+                                         "r"(h[8 * hh]), "r"(h[8 * hh + 1]), "r"(h[8 * hh + 2]), "r"(h[8 * hh + 3]),
+                                         "r"(h[8 * hh + 4]), "r"(h[8 * hh + 5]), "r"(h[8 * hh + 6]), "r"(h[8 * hh + 7])
+                                         : "memory");
+                    } else {
+#pragma unroll
+                        for (int jj = 0; jj < 16; jj++)
+                            if (nb + jj < N) __stcs(dst + jj, h[jj]);
+                    }
+                    continue;
+                }
+                float2* H = reinterpret_cast<float2*>(out);
                 if (P == 4 && (reinterpret_cast<uintptr_t>(H) & 31) == 0) {
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
@@ -493,19 +521,22 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// Shapes the tcgen05 kernel takes: whole 64-element K atoms (nPilot a
-// multiple of 32, up to 96) and a 16-byte aligned pilot array.
+// Shapes the tcgen05 kernel takes: pilot rows whose byte stride (4 nPilot)
+// is a multiple of 16, up to 96 pilots, from a 16-byte aligned array.  The
+// tensor map is encoded per call; a shape it rejects falls back to the
+// mma.sync kernel.
 static bool chest_umma_ok(const aerial_ch2* Yp, int nPilot) {
-    return nPilot % 32 == 0 && nPilot <= 96 && (reinterpret_cast<uintptr_t>(Yp) & 15) == 0;
+    return nPilot % 4 == 0 && nPilot <= 96 && (reinterpret_cast<uintptr_t>(Yp) & 15) == 0;
 }
 
-template <int KB>
-static int launch_chest_umma(float2* H, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
+template <int KB, bool OUT16>
+static int launch_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
                              int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
     auto enc = tensor_map_encoder();
     if (!enc) return AERIAL_ERR_UNSUPPORTED;
     const long M = (long)nBlocks * nAnt;
     CUtensorMap tm;
+    // K extent 2 nPilot; a 64-element box past it (nPilot < 32 KB) reads zeros
     const cuuint64_t dims[2] = {(cuuint64_t)(2 * nPilot), (cuuint64_t)M};
     const cuuint64_t strides[1] = {(cuuint64_t)(4 * nPilot)};
     const cuuint32_t box[2] = {(cuuint32_t)kUmmaKB, (cuuint32_t)kUmmaM};
@@ -514,7 +545,7 @@ static int launch_chest_umma(float2* H, const aerial_ch2* Yp, const aerial_ch2* 
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return AERIAL_ERR_UNSUPPORTED;
-    const int s = allow_max_smem<chest_umma_kernel<KB>>();
+    const int s = allow_max_smem<chest_umma_kernel<KB, OUT16>>();
     if (s != AERIAL_OK) return s;
     // + barriers, TMEM slot, abort flag and the 1024-byte alignment slack; at
     // least 120 KB so one CTA (256 TMEM columns) runs per SM
@@ -525,9 +556,22 @@ static int launch_chest_umma(float2* H, const aerial_ch2* Yp, const aerial_ch2* 
     long gx = std::max(1L, (long)sm_count() / nNT);
     gx = std::min(gx, nMT);
     dim3 grid((unsigned)gx, (unsigned)nNT);
-    chest_umma_kernel<KB><<<grid, kUmmaThreads, smem, st>>>(tm, (const __half2*)Wf, (const __half2*)OCC, H, nAnt,
-                                                            nBlocks, nPilot, nOut, P, F);
+    chest_umma_kernel<KB, OUT16><<<grid, kUmmaThreads, smem, st>>>(tm, (const __half2*)Wf, (const __half2*)OCC, out,
+                                                                   nAnt, nBlocks, nPilot, nOut, P, F);
     return launch_status();
+}
+
+// The filter on tcgen05 when the shape allows it; AERIAL_ERR_UNSUPPORTED
+// (nothing launched) otherwise, and the caller takes the mma.sync kernel.
+template <bool OUT16>
+static int try_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
+                          int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
+    if (!chest_umma_ok(Yp, nPilot)) return AERIAL_ERR_UNSUPPORTED;
+    switch ((nPilot + 31) / 32) {
+        case 1: return launch_chest_umma<1, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+        case 2: return launch_chest_umma<2, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+        default: return launch_chest_umma<3, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+    }
 }
 
 template <int KS, bool TO_CHANNEL>
@@ -601,6 +645,8 @@ using namespace aeq;
 extern "C" int aerial_srs_filter(aerial_ch2* H_est, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC,
                                  int nAnt, int nBlocks, int K, int nPorts, int foccLen, void* stream) {
     if (!srs_args_ok(H_est, SRS, W, FOCC, nAnt, nBlocks, K, kSrsMaxK, K, nPorts, foccLen)) return AERIAL_ERR_INVALID_ARG;
+    const int r = try_chest_umma<true>(H_est, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
+    if (r != AERIAL_ERR_UNSUPPORTED) return r;
     return launch_srs_est(H_est, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, to_stream(stream));
 }
 
@@ -608,6 +654,8 @@ extern "C" int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, cons
                                      const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts, int foccLen,
                                      void* stream) {
     if (!srs_args_ok(H, SRS, W, FOCC, nAnt, nBlocks, K, kSrsMaxK, K, nPorts, foccLen)) return AERIAL_ERR_INVALID_ARG;
+    const int r = try_chest_umma<false>(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
+    if (r != AERIAL_ERR_UNSUPPORTED) return r;
     return launch_srs_chan(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
 }
 
@@ -615,13 +663,7 @@ extern "C" int aerial_chest_interp(aerial_cf32* H, const aerial_ch2* Yp, const a
                                    int nAnt, int nBlocks, int nPilot, int nOut, int nPorts, int occLen, void* stream) {
     if (!srs_args_ok(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, kChestMaxK, nOut, nPorts, occLen))
         return AERIAL_ERR_INVALID_ARG;
-    if (chest_umma_ok(Yp, nPilot)) {
-        float2* h = reinterpret_cast<float2*>(H);
-        switch (nPilot / 32) {
-            case 1: return launch_chest_umma<1>(h, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
-            case 2: return launch_chest_umma<2>(h, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
-            default: return launch_chest_umma<3>(h, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
-        }
-    }
+    const int r = try_chest_umma<false>(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
+    if (r != AERIAL_ERR_UNSUPPORTED) return r;
     return launch_srs_chan(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
 }

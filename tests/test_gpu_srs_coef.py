@@ -14,7 +14,8 @@ def _d(x, dev):
     return torch.from_numpy(np.ascontiguousarray(x)).to(dev)
 
 
-SRS_CFGS = [(24, 4, 8), (24, 2, 8), (12, 4, 12), (12, 2, 12), (8, 1, 4)]
+# K a multiple of 4 runs the tcgen05 kernel (rows of 16-byte multiples for TMA), the others the mma.sync kernel.
+SRS_CFGS = [(24, 4, 8), (24, 2, 8), (12, 4, 12), (12, 2, 12), (8, 1, 4), (10, 2, 5), (6, 3, 3)]
 
 
 @pytest.mark.parametrize("K,P,F", SRS_CFGS)
@@ -41,8 +42,9 @@ def test_srs_filter_vs_fp64(aeq, orc, cuda, K, P, F):
     assert cosine(v1f.view(np.complex64), g) > 0.9999
 
 
-def test_srs_to_channel_layout(aeq, orc, cuda):
-    K, P, F, nBlk, nAnt = 24, 4, 8, 66, 64
+@pytest.mark.parametrize("K,P,F", [(24, 4, 8), (10, 2, 5)])
+def test_srs_to_channel_layout(aeq, orc, cuda, K, P, F):
+    nBlk, nAnt = 66, 64
     s, w, f = orc.ref_srs_inputs(43, nBlk * nAnt * K, K * K, P * F)
     H = torch.empty(nBlk * K, nAnt, P, dtype=torch.complex64, device=cuda)
     aeq.srs_to_channel(H, _d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda),
@@ -55,9 +57,9 @@ def test_srs_to_channel_layout(aeq, orc, cuda):
 
 # DMRS interpolation filter: (nPilot, nOut, ports, OCC length, antennas).  96 pilots x 4 ports over 64
 # antennas is the [64 x 96] x [96 x 4] product of the reference's README.md:200.
-# Pilot counts that are multiples of 32 (up to 96) run the tcgen05 kernel, the others the mma.sync kernel.
+# Pilot counts that are multiples of 4 (up to 96) run the tcgen05 kernel, the others the mma.sync kernel.
 CHEST_CFGS = [(96, 96, 4, 4, 64), (48, 96, 2, 2, 64), (96, 48, 4, 2, 33), (24, 12, 1, 1, 16), (56, 40, 3, 5, 48),
-              (64, 64, 2, 2, 64), (32, 20, 3, 3, 40)]
+              (64, 64, 2, 2, 64), (32, 20, 3, 3, 40), (45, 30, 2, 3, 40), (90, 90, 4, 2, 64), (20, 24, 4, 4, 64)]
 
 
 @pytest.mark.parametrize("nPilot,nOut,P,F,nAnt", CHEST_CFGS)
