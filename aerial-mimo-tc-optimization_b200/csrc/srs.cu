@@ -234,10 +234,11 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
 //   - B (taps, real-embedded as in the mma.sync kernel, split hi/lo) is built
 //     once per CTA in shared memory in the same swizzled layout, for the
 //     CTA's tile of 128 real output columns (64 complex outputs).
-//   - One elected thread issues tcgen05.mma (M = 128, N = 128, K = 16, FP16
-//     operands, FP32 accumulate in TMEM): the hi products then the lo
-//     products into one accumulator.  Two TMEM accumulators (256 columns) let
-//     the epilogue of one M tile overlap the MMAs of the next.
+//   - One elected thread issues tcgen05.mma (M = 128, N = NTL = 128 or 192
+//     real columns, K = 16, FP16 operands, FP32 accumulate in TMEM): the hi
+//     products then the lo products into one accumulator.  Two TMEM
+//     accumulators let the epilogue of one M tile overlap the MMAs of the
+//     next.
 //   - Warps 2-5 read the accumulator rows with tcgen05.ld (one TMEM lane =
 //     one (block, antenna) row per thread) and store the channel layout;
 //     for 4 ports a thread's 4 consecutive outputs are one 256-bit store and
@@ -251,7 +252,7 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
 // (counted in g_umma_timeouts).
 // ---------------------------------------------------------------------------
 constexpr int kUmmaM = 128;                  // rows per M tile (TMEM lanes)
-constexpr int kUmmaN = 128;                  // real output columns per CTA tile
+constexpr int kUmmaN = 128;                  // real output columns per CTA tile (192 where shared memory allows)
 constexpr int kUmmaKB = 64;                  // K elements per swizzle atom (128 bytes of FP16)
 constexpr int kUmmaAtomBytes = kUmmaM * 128; // one 128 x 64 FP16 atom column block: 16 KB
 constexpr int kUmmaEpiWarps = 4;            // one per TMEM sub-partition
@@ -286,8 +287,12 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
            ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 // Instruction descriptor, kind::f16: FP32 accumulator, FP16 A and B, both
-// K-major, N = 128, M = 128.
-constexpr uint32_t kUmmaIdesc = (1u << 4) | ((uint32_t)(kUmmaN >> 3) << 17) | ((uint32_t)(kUmmaM >> 4) << 24);
+// K-major, N = n, M = 128.
+__host__ __device__ constexpr uint32_t umma_idesc(int n) {
+    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kUmmaM >> 4) << 24);
+}
+// TMEM columns for two accumulators of n columns (a power of two >= 32).
+__host__ __device__ constexpr int umma_tmem_cols(int n) { return 2 * n <= 256 ? 256 : 512; }
 
 // Byte offset of FP16 element (row r, k) in a K-major 128-byte-swizzled atom
 // column block of 128-byte rows (k < 64): 16-byte chunk index XOR (r mod 8).
@@ -295,9 +300,10 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
     return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 3) ^ r) & 7) << 4) + (k & 7) * 2);
 }
 
-// KB: 64-element K atoms (2 nPilot <= 64 KB); OUT16: write the SRS filter's
-// FP16 H_est[blk][ant][k_out][p] layout instead of the complex64 channel.
-template <int KB, bool OUT16>
+// KB: 64-element K atoms (2 nPilot <= 64 KB); NTL: real output columns per
+// tile (NTL / 2 complex outputs); OUT16: write the SRS filter's FP16
+// H_est[blk][ant][k_out][p] layout instead of the complex64 channel.
+template <int KB, int NTL, bool OUT16>
 __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                                       const __half2* __restrict__ Wf,
                                                                       const __half2* __restrict__ occ,
@@ -306,16 +312,18 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
     extern __shared__ __align__(1024) uint8_t usm_raw[];
     // 128-byte swizzle atoms must start on 1024-byte boundaries of the shared window
     uint8_t* usm = usm_raw + ((1024u - (smem_u32(usm_raw) & 1023u)) & 1023u);
-    // layout: A stages [2][KB atoms] | B [hi, lo][KB atoms] | barriers | TMEM slot
+    // layout: A stages [2][KB atoms of 128 rows] | B [hi, lo][KB atoms of NTL rows] | barriers | TMEM slot
+    constexpr int kBAtom = NTL * 128;             // bytes of one B atom column block
+    constexpr int kTCols = umma_tmem_cols(NTL);
     uint8_t* sA = usm;
     uint8_t* sB = usm + 2 * KB * kUmmaAtomBytes;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + 2 * KB * kUmmaAtomBytes);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + 2 * KB * kBAtom);
     // bars: full[2], empty[2], tfull[2], tempty[2]
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 8);
     volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int N = nOut * P;                       // complex outputs per row
-    const int nt = blockIdx.y;                    // tile of 64 complex outputs
+    const int nt = blockIdx.y;                    // tile of NTL / 2 complex outputs
     const long M = (long)nBlocks * nAnt;
     const long nMT = (M + kUmmaM - 1) / kUmmaM;
 
@@ -327,18 +335,19 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;\n" ::"r"(smem_u32(tslot)));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                     "r"(kTCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n");
     }
     // B's K columns past 2 nPilot inside the last atom must read as zero
-    for (int e = threadIdx.x; e < 2 * KB * kUmmaAtomBytes / 16; e += blockDim.x)
+    for (int e = threadIdx.x; e < 2 * KB * kBAtom / 16; e += blockDim.x)
         reinterpret_cast<uint4*>(sB)[e] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
-    // B tile: rows r = 2 j + (re/im output) for complex output n = 64 nt + j,
+    // B tile: rows r = 2 j + (re/im output) for complex output n = NTL/2 nt + j,
     // K columns 2 kc + (re/im input); (Re T, -Im T) / (Im T, Re T) pairs.
-    for (int e = threadIdx.x; e < 64 * nPilot; e += blockDim.x) {
+    for (int e = threadIdx.x; e < (NTL / 2) * nPilot; e += blockDim.x) {
         const int j = e / nPilot, kc = e - j * nPilot;
-        const int n = 64 * nt + j;
+        const int n = (NTL / 2) * nt + j;
         float2 t = make_float2(0.f, 0.f);
         if (n < N) {
             const float2 w = __half22float2(Wf[(n / P) * nPilot + kc]);
@@ -349,8 +358,8 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
         split_h2(t.x, -t.y, hi0, lo0);           // row 2j: Re out
         split_h2(t.y, t.x, hi1, lo1);            // row 2j+1: Im out
         const int k = 2 * kc, kb = k >> 6, kin = k & 63;
-        uint8_t* bh = sB + kb * kUmmaAtomBytes;
-        uint8_t* bl = sB + (KB + kb) * kUmmaAtomBytes;
+        uint8_t* bh = sB + kb * kBAtom;
+        uint8_t* bl = sB + (KB + kb) * kBAtom;
         *reinterpret_cast<uint32_t*>(bh + sw128_off(2 * j, kin)) = hi0;
         *reinterpret_cast<uint32_t*>(bl + sw128_off(2 * j, kin)) = lo0;
         *reinterpret_cast<uint32_t*>(bh + sw128_off(2 * j + 1, kin)) = hi1;
@@ -394,7 +403,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
                 if (!mbar_wait(tempty0 + 8 * a, ph ^ 1, abort)) break;
                 if (!mbar_wait(full0 + 8 * s, ph, abort)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                const uint32_t dt = tbase + (uint32_t)(a * kUmmaN);
+                const uint32_t dt = tbase + (uint32_t)(a * NTL);
                 const uint32_t a0 = smem_u32(sA + s * KB * kUmmaAtomBytes);
                 const uint32_t b0 = smem_u32(sB);
 #pragma unroll
@@ -405,12 +414,12 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
                         for (int kk = 0; kk < kUmmaKB / 16; kk++) {
                             if (kb * kUmmaKB + kk * 16 >= 2 * nPilot) break;   // K steps past the pilots
                             const uint64_t ad = umma_desc_sw128(a0 + kb * kUmmaAtomBytes + kk * 32);
-                            const uint64_t bd = umma_desc_sw128(b0 + (part * KB + kb) * kUmmaAtomBytes + kk * 32);
+                            const uint64_t bd = umma_desc_sw128(b0 + (part * KB + kb) * kBAtom + kk * 32);
                             const uint32_t acc = (part | kb | kk) ? 1u : 0u;
                             asm volatile(
                                 "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dt),
-                                "l"(ad), "l"(bd), "r"(kUmmaIdesc), "r"(acc)
+                                "l"(ad), "l"(bd), "r"(umma_idesc(NTL)), "r"(acc)
                                 : "memory");
                         }
                     }
@@ -438,9 +447,9 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
             const int blk = mv ? (int)(m / nAnt) : 0;
             const int ant = mv ? (int)(m - (long)blk * nAnt) : 0;
 #pragma unroll 1
-            for (int c = 0; c < kUmmaN / 32; c++) {
+            for (int c = 0; c < NTL / 32; c++) {
                 uint32_t v[32];
-                const uint32_t ta = tbase + ((uint32_t)(sp * 32) << 16) + (uint32_t)(a * kUmmaN + c * 32);
+                const uint32_t ta = tbase + ((uint32_t)(sp * 32) << 16) + (uint32_t)(a * NTL + c * 32);
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
                     "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
@@ -453,7 +462,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
                     : "r"(ta));
                 asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
                 if (!mv) continue;
-                const int nb = 64 * nt + 16 * c;  // complex outputs nb .. nb + 15 of this row
+                const int nb = (NTL / 2) * nt + 16 * c;  // complex outputs nb .. nb + 15 of this row
                 if constexpr (OUT16) {
                     // H_est[blk][ant][n]: the row's 16 outputs are 64 contiguous bytes of half2
                     uint32_t h[16];
@@ -504,7 +513,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;\n" ::"r"(tbase));
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tbase), "r"(kTCols));
 }
 
 // cuTensorMapEncodeTiled from the driver, looked up once.
@@ -529,7 +538,7 @@ static bool chest_umma_ok(const aerial_ch2* Yp, int nPilot) {
     return nPilot % 4 == 0 && nPilot <= 96 && (reinterpret_cast<uintptr_t>(Yp) & 15) == 0;
 }
 
-template <int KB, bool OUT16>
+template <int KB, int NTL, bool OUT16>
 static int launch_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
                              int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
     auto enc = tensor_map_encoder();
@@ -545,18 +554,19 @@ static int launch_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* 
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return AERIAL_ERR_UNSUPPORTED;
-    const int s = allow_max_smem<chest_umma_kernel<KB, OUT16>>();
+    const int s = allow_max_smem<chest_umma_kernel<KB, NTL, OUT16>>();
     if (s != AERIAL_OK) return s;
-    // + barriers, TMEM slot, abort flag and the 1024-byte alignment slack; at
-    // least 120 KB so one CTA (256 TMEM columns) runs per SM
-    const size_t smem = std::max<size_t>((size_t)4 * KB * kUmmaAtomBytes + 8 * sizeof(uint64_t) + 16 + 1024,
+    // A stages + B + barriers, TMEM slot, abort flag and the 1024-byte
+    // alignment slack; at least 120 KB so one CTA (its TMEM columns) runs per SM
+    const size_t smem = std::max<size_t>((size_t)2 * KB * (kUmmaAtomBytes + NTL * 128) + 8 * sizeof(uint64_t) + 16 +
+                                             1024,
                                          120 * 1024);
-    const int nNT = (2 * nOut * P + kUmmaN - 1) / kUmmaN;
+    const int nNT = (2 * nOut * P + NTL - 1) / NTL;
     const long nMT = (M + kUmmaM - 1) / kUmmaM;
     long gx = std::max(1L, (long)sm_count() / nNT);
     gx = std::min(gx, nMT);
     dim3 grid((unsigned)gx, (unsigned)nNT);
-    chest_umma_kernel<KB, OUT16><<<grid, kUmmaThreads, smem, st>>>(tm, (const __half2*)Wf, (const __half2*)OCC, out,
+    chest_umma_kernel<KB, NTL, OUT16><<<grid, kUmmaThreads, smem, st>>>(tm, (const __half2*)Wf, (const __half2*)OCC, out,
                                                                    nAnt, nBlocks, nPilot, nOut, P, F);
     return launch_status();
 }
@@ -567,10 +577,17 @@ template <bool OUT16>
 static int try_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
                           int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
     if (!chest_umma_ok(Yp, nPilot)) return AERIAL_ERR_UNSUPPORTED;
+    // 192-column tiles where more than 128 real output columns exist and the
+    // operands fit (up to 64 pilots); 128 otherwise
+    const bool wide = 2 * nOut * P > kUmmaN && nPilot <= 64;
     switch ((nPilot + 31) / 32) {
-        case 1: return launch_chest_umma<1, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
-        case 2: return launch_chest_umma<2, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
-        default: return launch_chest_umma<3, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+        case 1:
+            return wide ? launch_chest_umma<1, 192, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st)
+                        : launch_chest_umma<1, 128, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+        case 2:
+            return wide ? launch_chest_umma<2, 192, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st)
+                        : launch_chest_umma<2, 128, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+        default: return launch_chest_umma<3, 128, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
     }
 }
 
