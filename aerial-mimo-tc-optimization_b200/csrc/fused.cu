@@ -173,12 +173,13 @@ __device__ __forceinline__ CellView view_of(const FusedCell& c) {
 // 16 received rows Y[s][a0..a0+15] of 128 bytes whose 16-byte pieces are
 // XOR-swizzled by (s & 1) * 4 (conflict-free 16-byte fragment reads).
 // ---------------------------------------------------------------------------
-// Stages per warp: four where the epilogue region is small (exact tiles up to
-// 8 layers), three for the generic kernel and two for the 16-layer tile, whose
-// larger shared-memory footprint would otherwise cost resident warps (the
-// 16-layer cell is compute-bound: two stages let 12 warps per SM run instead
-// of 8, 3 % faster).
-__host__ __device__ constexpr int stages_of(int exactTile) { return exactTile == 16 ? 2 : exactTile == 0 ? 3 : 4; }
+// Stages per warp: three for exact tiles up to 8 layers, two for the generic
+// kernel and the 16-layer tile, whose larger epilogue regions would otherwise
+// cost resident warps.  Measured same-box A/B (sustained): the 8-layer cell
+// 250 -> 244 us with three stages instead of four (12 resident warps instead
+// of 10), the uneven 16-cell batch 57.0 -> 54.6 us and the 16-layer cell
+// 411 -> 398 us with two instead of three.
+__host__ __device__ constexpr int stages_of(int exactTile) { return exactTile == 0 || exactTile == 16 ? 2 : 3; }
 constexpr int CHUNK = 16;       // antennas per stage (two k-steps)
 
 __host__ __device__ constexpr int hrs_of(int L) {
