@@ -129,6 +129,7 @@ SIGNATURES = {
     "aerial_srs_filter": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
     "aerial_srs_to_channel": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
     "aerial_chest_interp": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
+    "aerial_kernel_timeouts": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "aerial_pusch_eq_fused": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), _P]),
     "aerial_pusch_eq_plain_workspace": (_Z, [ctypes.POINTER(CellDesc), _I]),
     "aerial_pusch_eq_plain": (_I, [ctypes.POINTER(CellDesc), _I, _P, _Z, _P]),
@@ -254,6 +255,13 @@ def srs_to_channel(H, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, stream=No
     """SRS filter multiply written as the PUSCH channel H[blk*K+k_out][ant][port] (complex64)."""
     _check(lib().aerial_srs_to_channel(_ptr(H), _ptr(SRS), _ptr(W), _ptr(FOCC), nAnt, nBlocks, K, nPorts, foccLen,
                                        _stream(stream)), "srs_to_channel")
+
+
+def kernel_timeouts() -> int:
+    """Bounded waits of the tcgen05 kernels that gave up on the current device (0 in correct operation)."""
+    n = ctypes.c_uint(0)
+    _check(lib().aerial_kernel_timeouts(ctypes.byref(n)), "kernel_timeouts")
+    return int(n.value)
 
 
 def chest_interp(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, stream=None):

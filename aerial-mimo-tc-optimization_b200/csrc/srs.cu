@@ -659,6 +659,14 @@ static bool srs_args_ok(const void* out, const aerial_ch2* SRS, const aerial_ch2
 
 using namespace aeq;
 
+// Bounded waits of the tcgen05 filter kernel that gave up on the current
+// device (the kernel then leaves its loops, frees its TMEM and returns).
+extern "C" int aerial_kernel_timeouts(unsigned int* count) {
+    if (!count) return AERIAL_ERR_INVALID_ARG;
+    const cudaError_t e = cudaMemcpyFromSymbol(count, g_umma_timeouts, sizeof(unsigned int));
+    return e == cudaSuccess ? AERIAL_OK : (int)e;
+}
+
 extern "C" int aerial_srs_filter(aerial_ch2* H_est, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC,
                                  int nAnt, int nBlocks, int K, int nPorts, int foccLen, void* stream) {
     if (!srs_args_ok(H_est, SRS, W, FOCC, nAnt, nBlocks, K, kSrsMaxK, K, nPorts, foccLen)) return AERIAL_ERR_INVALID_ARG;

@@ -72,6 +72,14 @@ enum {
 const char* aerial_error_string(int status);
 int aerial_version(void);
 
+/* Diagnostic with no counterpart in the reference: the number of mbarrier
+ * waits in this library's tcgen05 kernels (the SRS / DMRS filter multiply)
+ * that ran out of their iteration limit on the current device since the
+ * library was loaded.  0 in correct operation; a kernel whose wait gives up
+ * leaves its loops, frees its tensor memory and returns (its output is then
+ * not valid).  Synchronizes with the device (a device-to-host copy). */
+int aerial_kernel_timeouts(unsigned int* count);
+
 /* Load every kernel of the library on the current device and set its launch
  * attributes.  Optional: without it the first launch of each kernel variant
  * pays the driver's lazy module loading (milliseconds), which a latency-

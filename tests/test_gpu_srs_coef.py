@@ -115,6 +115,17 @@ def test_chest_interp_and_srs_to_channel_on_offset_channel_pointers(aeq, orc, cu
         assert base[0].item() == 7 + 7j
 
 
+def test_tcgen05_kernel_waits_never_gave_up(aeq, orc, cuda):
+    """After the filter launches of this module (tcgen05 kernel included), no bounded wait ran out."""
+    nPilot, nOut, P, F, nAnt, nBlk = 96, 96, 4, 2, 64, 40
+    s, w, f = orc.ref_srs_inputs(14, nBlk * nAnt * nPilot, nOut * nPilot, P * F)
+    H = torch.empty(nBlk * nOut, nAnt, P, dtype=torch.complex64, device=cuda)
+    aeq.chest_interp(H, _d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda),
+                     nAnt, nBlk, nPilot, nOut, P, F)
+    torch.cuda.synchronize()
+    assert aeq.kernel_timeouts() == 0
+
+
 def test_chest_interp_square_filter_equals_srs_to_channel(aeq, orc, cuda):
     K, P, F, nBlk, nAnt = 24, 4, 8, 66, 64
     s, w, f = orc.ref_srs_inputs(43, nBlk * nAnt * K, K * K, P * F)
