@@ -46,3 +46,17 @@ extern "C" float ref_coef_time(int which, const cf32* C, const cf32* Y, cf32* O,
     free(t); cudaEventDestroy(s); cudaEventDestroy(e);
     return m;
 }
+
+// Launch only (no synchronization), for event timing by the caller on the
+// default stream: which = 1 (V1 scalar), 2 (V2 WMMA), 3 (V3 WMMA 4 warps).
+extern "C" int ref_coef_launch(int which, const cf32* C, const cf32* Y, cf32* O, int nSC, int nSym) {
+    if (which == 1) {
+        dim3 blk(N_SC_PRB, nSym), grd((nSC + N_SC_PRB - 1) / N_SC_PRB, N_LAYERS);
+        coef_apply_v1_scalar<<<grd, blk>>>(C, Y, O, nSC, nSym);
+    } else if (which == 2) {
+        coef_apply_v2_wmma<<<nSC, 32>>>(C, Y, O, nSC, nSym);
+    } else {
+        coef_apply_v3_wmma_multiw<<<(nSC + SC_PER_BLK - 1) / SC_PER_BLK, SC_PER_BLK * 32>>>(C, Y, O, nSC, nSym);
+    }
+    return (int)cudaGetLastError();
+}

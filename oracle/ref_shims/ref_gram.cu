@@ -17,3 +17,10 @@ extern "C" int ref_gram_coef_apply(const cf32* C, const cf32* Y, cf32* O, int nS
     coef_apply_scalar<<<grd, blk>>>(C, Y, O, nSC, nSym);
     return (int)cudaDeviceSynchronize();
 }
+
+// Launch only (no synchronization), for event timing by the caller.
+extern "C" int ref_gram_launch(const cf32* M, const cf32* H, cf32* G, int nSC) {
+    dim3 blk(N_LAYERS, N_LAYERS), grd(N_SC_PRB, (nSC + N_SC_PRB - 1) / N_SC_PRB);
+    gram_scalar<<<grd, blk>>>(M, H, G, nSC);
+    return (int)cudaGetLastError();
+}

@@ -26,3 +26,16 @@ extern "C" int ref_llr_v3_v3(const half2c* d_in, const float* d_ni, __half* d_ou
     else return -1;
     return (int)cudaDeviceSynchronize();
 }
+
+// Launch only (no synchronization), for event timing by the caller:
+// which = 1 (llr_v1_baseline) or 3 (llr_v3_reg_template, nPamBits 2..4).
+extern "C" int ref_llr_v3_launch(int which, const half2c* d_in, const float* d_ni, __half* d_out, int N,
+                                 int nPamBits) {
+    dim3 b(512), g((N + 511) / 512);
+    if (which == 1) llr_v1_baseline<<<g, b>>>(d_in, d_ni, d_out, N, nPamBits);
+    else if (nPamBits == 2) llr_v3_reg_template<2><<<g, b>>>(d_in, d_ni, d_out, N);
+    else if (nPamBits == 3) llr_v3_reg_template<3><<<g, b>>>(d_in, d_ni, d_out, N);
+    else if (nPamBits == 4) llr_v3_reg_template<4><<<g, b>>>(d_in, d_ni, d_out, N);
+    else return -1;
+    return (int)cudaGetLastError();
+}

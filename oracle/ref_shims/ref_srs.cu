@@ -23,3 +23,17 @@ extern "C" int ref_srs(int version, void* out, const void* srs, const void* W, c
     if (K == 12 && P == 2 && F == 12) return run_srs<12, 2, 12>(version, o, s, w, f, nAnt, nBlocks);
     return -1;
 }
+
+// Launch only (no synchronization), for event timing by the caller; the
+// reference's main() configuration K = 24, 4 ports, FOCC length 8.
+extern "C" int ref_srs_launch(int version, void* out, const void* srs, const void* W, const void* focc, int nAnt,
+                              int nBlocks) {
+    dim3 blk(256), grd(1, 1, nBlocks);
+    if (version == 1)
+        srs_filter_v1_scalar<24, 4, 8><<<grd, blk>>>((ch2*)out, (const ch2*)srs, (const ch2*)W, (const ch2*)focc,
+                                                     nAnt, nBlocks);
+    else
+        srs_filter_v2_wmma<24, 4, 8><<<grd, blk>>>((ch2*)out, (const ch2*)srs, (const ch2*)W, (const ch2*)focc,
+                                                   nAnt, nBlocks);
+    return (int)cudaGetLastError();
+}
