@@ -42,6 +42,33 @@ def test_srs_filter_vs_fp64(aeq, orc, cuda, K, P, F):
     assert cosine(v1f.view(np.complex64), g) > 0.9999
 
 
+def test_srs_many_tiles_per_cta_both_layouts(aeq, orc, cuda):
+    """1000 SRS blocks x 64 antennas: each CTA of the tcgen05 kernel walks several M tiles (operand stages and
+    TMEM accumulators reused across phases), for the FP16 H_est layout and the channel layout, twice."""
+    K, P, F, nBlk, nAnt = 24, 4, 8, 1000, 64
+    s, w, f = orc.ref_srs_inputs(21, nBlk * nAnt * K, K * K, P * F)
+    args = (_d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda))
+    ref = orc.srs_f64(s, w, f, nAnt, nBlk, K, P, F)
+    est = torch.empty(nBlk * nAnt * K * P * 2, dtype=torch.int16, device=cuda)
+    H = torch.empty(nBlk * K, nAnt, P, dtype=torch.complex64, device=cuda)
+    for rep in range(2):
+        est.fill_(0)
+        H.fill_(0)
+        aeq.srs_filter(est, *args, nAnt, nBlk, K, P, F)
+        aeq.srs_to_channel(H, *args, nAnt, nBlk, K, P, F)
+        torch.cuda.synchronize()
+        got16 = est.cpu().numpy().view(np.uint16)
+        got = np.empty(got16.size, np.float32)
+        orc.lib().orc_f16_to_f32(got16, got, got.size)
+        g = got.view(np.complex64).astype(np.complex128)
+        tol = np.maximum(np.abs(ref.real), np.abs(ref.imag)) * 2.0 ** -11 + 2.0 ** -24
+        assert np.all(np.abs(g.real - ref.real) <= tol + 1e-6 * np.abs(ref).max())
+        assert np.all(np.abs(g.imag - ref.imag) <= tol + 1e-6 * np.abs(ref).max())
+        ch = ref.reshape(nBlk, nAnt, K, P).transpose(0, 2, 1, 3).reshape(nBlk * K, nAnt, P)
+        assert evm_db(H.cpu().numpy(), ch) < -120
+    assert aeq.kernel_timeouts() == 0
+
+
 @pytest.mark.parametrize("K,P,F", [(24, 4, 8), (10, 2, 5)])
 def test_srs_to_channel_layout(aeq, orc, cuda, K, P, F):
     nBlk, nAnt = 66, 64
