@@ -15,7 +15,8 @@ def _d(x, dev):
 
 
 # K a multiple of 4 runs the tcgen05 kernel (rows of 16-byte multiples for TMA), the others the mma.sync kernel.
-SRS_CFGS = [(24, 4, 8), (24, 2, 8), (12, 4, 12), (12, 2, 12), (8, 1, 4), (10, 2, 5), (6, 3, 3)]
+SRS_CFGS = [(24, 4, 8), (24, 2, 8), (12, 4, 12), (12, 2, 12), (8, 1, 4), (10, 2, 5), (6, 3, 3),
+            (48, 4, 8), (32, 16, 4), (44, 5, 4)]   # two K atoms; six 192-column tiles, the last partial; 48 max
 
 
 @pytest.mark.parametrize("K,P,F", SRS_CFGS)
