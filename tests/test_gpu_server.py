@@ -134,3 +134,33 @@ def test_server_srs_update_rewrites_resident_channel(aeq, orc, wl, cuda):
         assert srv.stats()["srs_updates"] == 1
     np.testing.assert_array_equal(before.cpu().numpy(), _alone(aeq, c, c.H.to(cuda), Y, cuda))
     np.testing.assert_array_equal(after.cpu().numpy(), _alone(aeq, c, Hsrs, Y, cuda))
+
+
+def test_server_deadline_misses_counted_for_late_producer(aeq, wl, cuda):
+    """Fault injected on the host: a producer that hands slots over late (arrival stamped 200 ms before the
+    submit, on the same steady clock) makes every such slot miss a 20 ms deadline, and the statistics count
+    them; slots handed over on time do not miss.  Malformed submissions return codes and queue nothing."""
+    c = wl.make_cell(4, 16, 2, 11, 4, 15.0, seed=131)
+    with aeq.Server(streams=1, deadline_us=20000.0) as srv:
+        k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
+        srv.set_channel(k, c.H.to(cuda), c.sigma2)
+        Y = c.Y.to(cuda)
+        outs = [torch.empty(c.llr_numel, dtype=torch.float32, device=cuda) for _ in range(8)]
+        for o in outs[:4]:
+            srv.submit(k, Y, o, arrival_ns=time.monotonic_ns() - 200_000_000)
+        srv.drain()
+        st = srv.stats()
+        assert st["slots_done"] == 4 and st["deadline_misses"] == 4
+        srv.reset_stats()
+        for o in outs[4:]:
+            srv.submit(k, Y, o)
+        srv.drain()
+        st = srv.stats()
+        assert st["slots_done"] == 4 and st["deadline_misses"] == 0
+        assert srv.submit_status(k + 100, Y, outs[0]) == 1007     # unknown cell
+        assert srv.submit_status(k, None, outs[0]) == 1001        # null received samples
+        assert srv.submit_status(k, Y, None) == 1001              # null LLR buffer
+        assert srv.stats()["pending"] == 0
+        torch.cuda.synchronize()
+        for o in outs[1:]:
+            assert torch.equal(o, outs[0])                        # same slot, same LLRs, late or not
