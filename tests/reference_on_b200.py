@@ -13,7 +13,8 @@ Shapes are the reference's own benchmark shapes:
   llr             139,392 symbols, 256-QAM (src/llr/aerial_llr_v3.cu:258-307)
   srs filter      66 blocks x 64 antennas, K = 24, 4 ports, FOCC length 8 (src/srs/srs_wmma_bench.cu:347)
   chain           gram_scalar -> coef_apply_v2_wmma -> llr_v3 on one 1584-subcarrier cell, against
-                  this library's fused launch of the same cell (Gram + MMSE solve + apply + LLR)
+                  this library's fused launch of the same cell (Gram + MMSE solve + apply + LLR);
+                  and the same over 64 cell-slots (101,376 subcarriers, inputs larger than L2)
 Timing follows the reference's own method (src/aerial_coef_wmma.cu:443-462): CUDA events around each
 launch on the default stream (the checker libraries' *_launch entry points do not synchronize, like this
 library's calls), median of 50 after 10 warm-ups, the inputs left in place between launches (L2-warm:
@@ -147,6 +148,40 @@ def main():
         "reference_gram_coefv2_llrv3_us (three launches, no solve)": timed(ref_chain),
         "aerial_pusch_eq_fused_us (Gram + MMSE solve + apply + LLR, one launch)":
             timed(lambda: aeq.pusch_eq_fused([desc], tun)),
+    }
+    # the headline scale: 64 cell-slots (101,376 subcarriers, 1.3 GB of inputs: larger than L2), the
+    # reference's three stages over all of them against one fused launch of this library
+    del Mc, Gc, Cc, Oc, M, H, C, Y
+    torch.cuda.empty_cache()
+    slots = 64
+    cells = [wl.config_cell(2, seed=17 * i + 1, device=dev) for i in range(slots)]
+    nS = nSC * slots
+    Hs = torch.cat([x.H for x in cells])
+    Ys = torch.cat([x.Y for x in cells])
+    Ms = Hs.conj().transpose(1, 2).contiguous()
+    Gs = torch.empty(nS, L, L, dtype=torch.complex64, device=dev)
+    Cs = crand((nS, L, A), dev)
+    Os = torch.empty(nS, L, S, dtype=torch.complex64, device=dev)
+    Ns = nS * L * S
+    soft_s = ((torch.rand(2 * Ns, device=dev) - 0.5) * 1.4).half()
+    ni_s = torch.rand(Ns, device=dev) * 10 + 1
+    lo_s = torch.empty(Ns * 2 * nb, dtype=torch.float16, device=dev)
+    llrs = [torch.empty(x.llr_numel, dtype=torch.float32, device=dev) for x in cells]
+    descs = [aeq.cell_desc(x.H, x.Y, l, x.sigma2, x.nPRB, x.nAnt, x.nLayers, x.nSym, x.nPamBits)
+             for x, l in zip(cells, llrs)]
+
+    def ref_chain_64():
+        lg.ref_gram_launch(Ms.data_ptr(), Hs.data_ptr(), Gs.data_ptr(), nS)
+        lc.ref_coef_launch(2, Cs.data_ptr(), Ys.data_ptr(), Os.data_ptr(), nS, S)
+        ll.ref_llr_v3_launch(3, soft_s.data_ptr(), ni_s.data_ptr(), lo_s.data_ptr(), Ns, nb)
+
+    t_ref = timed(ref_chain_64, warm=3, iters=20)
+    t_fused = timed(lambda: aeq.pusch_eq_fused(descs, tun), warm=3, iters=20)
+    rows["64_slot_chain"] = {
+        "reference_gram_coefv2_llrv3_us (three launches, no solve)": t_ref,
+        "reference_res_per_s": nS * S / (t_ref * 1e-6),
+        "aerial_pusch_eq_fused_us (Gram + MMSE solve + apply + LLR, one launch)": t_fused,
+        "aerial_res_per_s": nS * S / (t_fused * 1e-6),
     }
     print(json.dumps({"gpu": torch.cuda.get_device_name(0), "method": "median of 50 event-timed launches after 10 "
                       "warm-ups, inputs L2-warm (the reference's own method), the GPU kept busy across the host's "
