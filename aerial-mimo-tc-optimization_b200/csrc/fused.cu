@@ -1195,7 +1195,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_a(const __grid_constan
 // (16 antennas) whose 8-byte antenna-pair granules are XOR-swizzled by
 // (sym & 2) << 1; both make every fragment read of a warp conflict-free.
 // ---------------------------------------------------------------------------
-__host__ __device__ constexpr int hrs16_of(int L) { return L == 8 ? 48 : 16; }
+__host__ __device__ constexpr int hrs16_of(int L) { return L == 16 ? 80 : L == 8 ? 48 : 16; }
 
 struct ScPtrH {
     const char* h;   // the lane's channel piece of the subcarrier's first chunk
@@ -1209,6 +1209,8 @@ __device__ __forceinline__ void stage_chunk_h(uint32_t st, uint32_t hLaneS, uint
     constexpr int NP = CHUNK * LF / 4;                 // 16-byte channel pieces per chunk
     constexpr int A = CHUNK * NCH;
     if (NP >= 32 || lane < NP) cp_async16(st + hLaneS, s.h + j * CHUNK * LF * 4);
+    // 16 layers: 64 pieces, the second 32 are antenna rows 8-15
+    if (NP > 32) cp_async16(st + hLaneS + 8 * hrs16_of(LF), s.h + j * CHUNK * LF * 4 + 512);
     if (s.yk > 0) cp_async16(st + yLaneS, s.y + j * 64);
     if (s.yk > 1) cp_async16(st + yLaneS + 512, s.y + j * 64 + 8 * A * 4);
 }
@@ -1226,6 +1228,9 @@ __device__ __forceinline__ uint2 lds64u(uint32_t a) {
 
 // One full chunk: hb = stage + the lane's channel offset (antenna 2c, layer g),
 // yo[kk][nt] = its received-pair offsets.
+// 16 layers: two m-tiles (layers g and g + 8, 32 bytes apart in a row), the
+// Gram blocks (0,0), (1,0), (1,1) and both matched-filter m-tiles, each
+// accumulator fed in the complex64 kernel's order (mma_stage).
 template <int LT>
 __device__ __forceinline__ void mma_stage_h(uint32_t st, uint32_t hb, const uint32_t (&yo)[2][2],
                                             float (*gacc)[4], float (*zacc)[2][4], bool z2) {
@@ -1240,6 +1245,15 @@ __device__ __forceinline__ void mma_stage_h(uint32_t st, uint32_t hb, const uint
         mma16816<AERIAL_PREC_FP16>(gacc[0], h0, r0, h1, r1, h0, h1);
         mma16816<AERIAL_PREC_FP16>(zacc[0][0], h0, r0, h1, r1, y0.x, y0.y);
         if (z2) mma16816<AERIAL_PREC_FP16>(zacc[0][1], h0, r0, h1, r1, y1.x, y1.y);
+        if constexpr (LT == 16) {
+            const uint32_t u0 = lds32(hb + 8 * kk * HRS + 32);
+            const uint32_t u1 = lds32(hb + (8 * kk + 1) * HRS + 32);
+            const uint32_t q0 = jrot(u0), q1 = jrot(u1);
+            mma16816<AERIAL_PREC_FP16>(gacc[1], u0, q0, u1, q1, h0, h1);
+            mma16816<AERIAL_PREC_FP16>(gacc[2], u0, q0, u1, q1, u0, u1);
+            mma16816<AERIAL_PREC_FP16>(zacc[1][0], u0, q0, u1, q1, y0.x, y0.y);
+            if (z2) mma16816<AERIAL_PREC_FP16>(zacc[1][1], u0, q0, u1, q1, y1.x, y1.y);
+        }
     }
 }
 
@@ -1265,7 +1279,9 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_h(const __grid_constan
     if (gw >= total) return;
 
     const int s0 = lane >> 2, q4 = lane & 3;
-    const uint32_t hLaneS = LTF == 8 ? (lane >> 1) * HRS + (lane & 1) * 16 : lane * HRS;
+    const uint32_t hLaneS = LTF == 16 ? (lane >> 2) * HRS + (lane & 3) * 16
+                          : LTF == 8  ? (lane >> 1) * HRS + (lane & 1) * 16
+                                      : lane * HRS;
     const uint32_t yLaneS = CHUNK * HRS + s0 * 64 + ((q4 ^ (((s0 >> 1) & 1) << 1)) << 4);
     const long yLaneB = (long)(s0 * A + 4 * q4) * 4;
 
@@ -1328,12 +1344,17 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_h(const __grid_constan
                 nxt = first_sc(nc, ng);
             }
         }
+        constexpr int NMT = LTF > 8 ? 2 : 1;
 #pragma unroll
-        for (int e = 0; e < 4; e++) gacc[0][e] = 0.f;
+        for (int b = 0; b < (NMT == 2 ? 3 : 1); b++)
 #pragma unroll
-        for (int nt = 0; nt < 2; nt++)
+            for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
 #pragma unroll
-            for (int e = 0; e < 4; e++) zacc[0][nt][e] = 0.f;
+        for (int mt = 0; mt < NMT; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
 #pragma unroll
         for (int k = 0; k < NCH; k++) {
             __syncwarp();                              // every lane is done with the slot refilled now
@@ -1450,9 +1471,16 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
         if (same) p.exactChunks = a / CHUNK;
     }
     if (p.fmt == AERIAL_FMT_CF16) {
-        // half-format cells run the FP16 I/O kernel: exact 4- or 8-layer
+        // half-format cells run the FP16 I/O kernel: exact 4-, 8- or 16-layer
         // tile, 32 / 64 / 128 antennas, 16-byte aligned H and Y_rx
-        if ((p.exactTile != 4 && p.exactTile != 8) || !p.exactChunks) return AERIAL_ERR_UNSUPPORTED;
+        if (p.exactTile == 16) {
+            const int a = p.cell[0].A;
+            bool same = a == 32 || a == 64 || a == 128;
+            for (int i = 1; i < nCells && same; i++) same = p.cell[i].A == a;
+            p.exactChunks = same ? a / CHUNK : 0;
+        }
+        if ((p.exactTile != 4 && p.exactTile != 8 && p.exactTile != 16) || !p.exactChunks)
+            return AERIAL_ERR_UNSUPPORTED;
         int b = 0;
         for (int i = 0; i < nCells; i++) {
             const int v = CHUNK * hrs16_of(p.cell[i].L) + 64 * p.cell[i].nSym;
@@ -1561,7 +1589,9 @@ template <int P>
 static int plan_p(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
     if (p.fmt == AERIAL_FMT_CF16) {
         if (P != AERIAL_PREC_FP16) return AERIAL_ERR_UNSUPPORTED;
-        return p.exactTile == 4 ? plan_hn<4>(p, warpBytes, sh, out) : plan_hn<8>(p, warpBytes, sh, out);
+        return p.exactTile == 4   ? plan_hn<4>(p, warpBytes, sh, out)
+             : p.exactTile == 8   ? plan_hn<8>(p, warpBytes, sh, out)
+                                  : plan_hn<16>(p, warpBytes, sh, out);
     }
     if (p.exactChunks) {
         switch (p.exactTile) {
@@ -1863,6 +1893,9 @@ int prepare_fused_kernels() {
     if (!s) s = prepare_h<8, 2>();
     if (!s) s = prepare_h<8, 4>();
     if (!s) s = prepare_h<8, 8>();
+    if (!s) s = prepare_h<16, 2>();
+    if (!s) s = prepare_h<16, 4>();
+    if (!s) s = prepare_h<16, 8>();
     if (!s) s = prepare_p<AERIAL_PREC_BF16>();
     if (!s) s = prepare_p<AERIAL_PREC_BF16X3>();
     return s;

@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--precision", default="", choices=["", "fp16", "bf16", "bf16x3"])
     ap.add_argument("--io", default="cf32", choices=["cf32", "fp16"],
                     help="storage of H / Y_rx / LLRs: cf32 = the drop-in complex64 layout (default); fp16 = complex "
-                         "half in, __half LLRs out (configs 1 and 2, FP16 operands), reported as its own line")
+                         "half in, __half LLRs out (configs 1, 2 and 3 with FP16 operands), reported as its own line")
     ap.add_argument("--duration", type=float, default=1.0, help="serving run length in seconds (config 5)")
     ap.add_argument("--window-us", type=float, default=0.0, help="serving batching window (config 5; 0 = launch at once)")
     ap.add_argument("--min-batch", type=int, default=0, help="serving minimum batch before the window ends")
@@ -292,8 +292,9 @@ def main():
     cells = build_cells(wl, a.config, S, rank, dev)
     half = a.io == "fp16"
     if half:
-        if a.config not in (1, 2) or a.precision != "fp16":
-            raise SystemExit("--io fp16 runs configurations 1 and 2 with fp16 operands")
+        if a.config not in (1, 2, 3) or a.precision != "fp16":
+            raise SystemExit("--io fp16 runs configurations 1, 2 and 3 with fp16 operands "
+                             "(configuration 3: --precision fp16)")
         a.no_extras = True          # the extras run the complex64 plain chain
         # the same slots stored as complex half; the complex64 copies are dropped
         for c in cells:

@@ -173,8 +173,9 @@ int aerial_chest_interp(aerial_cf32* H, const aerial_ch2* Yp, const aerial_ch2* 
  *  AERIAL_FMT_CF16: H, Y_rx, Y_eq complex half (aerial_ch2), LLRs __half --
  *                   half the bytes; the LLR storage of the reference's
  *                   demapper (src/llr/aerial_llr_v3.cu:84-108).  Supported for
- *                   launches whose cells all have nLayers 4 or 8, nAnt 32, 64
- *                   or 128, with FP16 operands (else AERIAL_ERR_UNSUPPORTED). */
+ *                   launches whose cells all have the same nLayers of 4, 8 or
+ *                   16 and nAnt 32, 64 or 128, with FP16 operands (else
+ *                   AERIAL_ERR_UNSUPPORTED). */
 enum { AERIAL_FMT_CF32 = 0, AERIAL_FMT_CF16 = 1 };
 
 /* One cell-slot.  nSC = 12 * nPRB.  Y_eq may be NULL.  Pointer types name

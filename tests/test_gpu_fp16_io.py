@@ -45,7 +45,7 @@ def run_pair(aeq, cells, cuda, want_yeq=True):
     return out32, out16
 
 
-@pytest.mark.parametrize("L", [4, 8])
+@pytest.mark.parametrize("L", [4, 8, 16])
 @pytest.mark.parametrize("A", [32, 64, 128])
 def test_fp16_io_equals_complex64_path_rounded(aeq, wl, cuda, L, A):
     cells = [wl.make_cell(2, A, L, 11, 256, 25.0, seed=600 + A + L),
