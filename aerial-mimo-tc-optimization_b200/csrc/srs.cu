@@ -239,14 +239,16 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
 //     products then the lo products into one accumulator.  Two TMEM
 //     accumulators let the epilogue of one M tile overlap the MMAs of the
 //     next.
-//   - Warps 2-5 read the accumulator rows with tcgen05.ld (one TMEM lane =
-//     one (block, antenna) row per thread) and store the channel layout;
-//     for 4 ports a thread's 4 consecutive outputs are one 256-bit store and
-//     a warp's 32 antennas are 1 KB contiguous per instruction.  (Two 16-byte
+//   - Warps 2-9 read the accumulator rows with tcgen05.ld (one TMEM lane =
+//     one (block, antenna) row per thread; two warps per TMEM sub-partition,
+//     each half of the tile's columns) and store the channel layout; for 4
+//     ports a thread's 4 consecutive outputs are one 256-bit store and a
+//     warp's 32 antennas are 1 KB contiguous per instruction.  (Two 16-byte
 //     stores per thread left every 32-byte sector of a request half written:
-//     ncu showed 32 sectors per request and L1 at 76 %.  Eight epilogue warps
-//     instead of four measured slower, 188 against 140 us.)
-// Warp roles: 0 = TMA producer, 1 = TMEM owner + MMA issuer, 2-5 = epilogue.
+//     ncu showed 32 sectors per request and L1 at 76 %.  Staging the outputs
+//     in shared memory for TMA tensor stores measured slower than these
+//     direct stores, with 64-byte, 32-byte or 1 KB box rows.)
+// Warp roles: 0 = TMA producer, 1 = TMEM owner + MMA issuer, 2-9 = epilogue.
 // Every wait is bounded: on a timeout the CTA raises an abort flag, every
 // role leaves its loop, and the kernel still frees its TMEM and returns
 // (counted in g_umma_timeouts).
@@ -255,7 +257,7 @@ constexpr int kUmmaM = 128;                  // rows per M tile (TMEM lanes)
 constexpr int kUmmaN = 128;                  // real output columns per CTA tile (192 where shared memory allows)
 constexpr int kUmmaKB = 64;                  // K elements per swizzle atom (128 bytes of FP16)
 constexpr int kUmmaAtomBytes = kUmmaM * 128; // one 128 x 64 FP16 atom column block: 16 KB
-constexpr int kUmmaEpiWarps = 4;            // one per TMEM sub-partition
+constexpr int kUmmaEpiWarps = 8;            // two per TMEM sub-partition, each half of the columns
 constexpr int kUmmaThreads = 64 + 32 * kUmmaEpiWarps;
 constexpr long kUmmaWaitLimit = 1L << 22;    // mbarrier polls before a wait gives up
 
@@ -447,7 +449,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
             const int blk = mv ? (int)(m / nAnt) : 0;
             const int ant = mv ? (int)(m - (long)blk * nAnt) : 0;
 #pragma unroll 1
-            for (int c = 0; c < NTL / 32; c++) {
+            for (int c = ((warp - 2) >> 2) * (NTL / 64); c < (((warp - 2) >> 2) + 1) * (NTL / 64); c++) {
                 uint32_t v[32];
                 const uint32_t ta = tbase + ((uint32_t)(sp * 32) << 16) + (uint32_t)(a * NTL + c * 32);
                 asm volatile(

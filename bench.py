@@ -407,6 +407,7 @@ def main():
         if a.config == 4:
             extras["tiles"] = compare_tiles(aeq, descs, tun, stream, a, flush)
             extras["per_cell_streams_vs_batched"] = compare_streams(aeq, descs, tun, a, flush)
+            extras["sm_partition_strategies"] = sm_partition_strategies(aeq, wl, aeq.make_tuning("fp16"), dev)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         from oracle import oracle as orc
 
@@ -582,7 +583,8 @@ def compare_streams(aeq, descs, tuned, a, flush):
     (src/multicell_contention.cu:205-235) restated for this path: the 16 cells
     as one launch per cell on 16 concurrent streams (per-cell latency and
     makespan, against each cell alone) versus all cells in one persistent
-    batched launch."""
+    batched launch.  A device sleep ahead of each start event keeps host-side
+    call overhead out of every interval."""
     import torch
 
     n = len(descs)
@@ -600,6 +602,7 @@ def compare_streams(aeq, descs, tuned, a, flush):
         for r in range(reps):
             if flush is not None:
                 flush.fill_(float(r))
+            torch.cuda._sleep(2_000_000)     # the launch is enqueued before e0 fires
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(main)
             aeq.pusch_eq_fused([d], tuned, main)
@@ -612,6 +615,7 @@ def compare_streams(aeq, descs, tuned, a, flush):
         if flush is not None:
             flush.fill_(float(r))
         torch.cuda.synchronize()
+        torch.cuda._sleep(2_000_000)         # every launch is enqueued before g0 fires
         g0 = torch.cuda.Event(enable_timing=True)
         g0.record(main)
         ev = []
@@ -630,6 +634,7 @@ def compare_streams(aeq, descs, tuned, a, flush):
     for r in range(reps):
         if flush is not None:
             flush.fill_(float(r))
+        torch.cuda._sleep(2_000_000)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(main)
         aeq.pusch_eq_fused(descs, tuned, main)
@@ -642,6 +647,125 @@ def compare_streams(aeq, descs, tuned, a, flush):
             "streams_mean_degradation_vs_alone": sum(l / al for l, al in zip(lat, alone)) / n,
             "streams_makespan_us": med(span), "batched_launch_us": med(batched),
             "makespan_ratio_streams_over_batched": med(span) / med(batched)}
+
+
+def prb_range_desc(aeq, cell, llr, prb0, nprb):
+    """Subcarriers [12 prb0, 12 (prb0 + nprb)) of a device cell as a cell of
+    its own: the same buffers at an offset (H[nSC][A][L], Y_rx[nSC][nSym][A],
+    LLRs per subcarrier in the Y_eq order)."""
+    sc0 = 12 * prb0
+    return aeq.cell_desc(cell.H[sc0:], cell.Y[sc0:], llr[sc0 * (cell.llr_numel // cell.nSC):], cell.sigma2, nprb,
+                         cell.nAnt, cell.nLayers, cell.nSym, cell.nPamBits)
+
+
+def sm_partition_strategies(aeq, wl, tuned, dev, max_cells=8, reps=20):
+    """The reference's SM-partitioning study (src/adaptive_smpartition.cu:165-436)
+    restated with the fused launch, on cells of the 100 MHz shape (132 PRB x 64
+    antennas x 8 layers x 11 symbols, 256-QAM), for N = 1..8 cells:
+      A  one launch per cell on N concurrent streams;
+      B  the N launches back to back on one stream;
+      C  as A, even cells on a high-priority stream, odd cells on a low one;
+      D  ONE cell's PRB range split into N chunks, one launch per chunk on N
+         streams (the same total work as one cell);
+      E  launches two at a time on two streams, each pair after the previous;
+      F  all N cells in one persistent batched launch (this library's method).
+    Per-cell latency is event-timed on each cell's stream; the makespan runs
+    from a start event that every stream waits on to the last cell's end, with
+    every launch enqueued before the start fires.  L2
+    is flushed before every repetition (the N cells of 19.9 MB each fit in
+    L2 otherwise).  Medians over `reps` repetitions; degradation is the per-cell
+    latency over the cell alone."""
+    import torch
+
+    cells = [wl.config_cell(2, seed=300 + i, device=dev) for i in range(max_cells)]
+    llrs = [torch.empty(c.llr_numel, dtype=torch.float32, device=dev) for c in cells]
+    descs = [aeq.cell_desc(c.H, c.Y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+             for c, l in zip(cells, llrs)]
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    main = torch.cuda.current_stream()
+    plain = [torch.cuda.Stream() for _ in range(max_cells)]
+    lo_p, hi_p = torch.cuda.Stream.priority_range()
+    prio = [torch.cuda.Stream(priority=hi_p if i % 2 == 0 else lo_p) for i in range(max_cells)]
+
+    def med(v):
+        v = sorted(v)
+        return v[len(v) // 2]
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def run(plan):
+        """plan: list of (stream, [descs], after) launches; `after` = indices of
+        the launches whose ends this one waits for, or None for the start event.
+        Returns per-launch latencies and the makespan over `reps` repetitions."""
+        lat, span = [[] for _ in plan], []
+        for r in range(reps + 3):
+            flush.fill_(float(r))
+            # ~1 ms of device sleep ahead of the start event: every launch is
+            # enqueued before the start fires, so no interval holds host-side
+            # call overhead
+            torch.cuda._sleep(2_000_000)
+            g0 = ev()
+            g0.record(main)
+            ends = []
+            for k, (st, ds, after) in enumerate(plan):
+                for w in ([g0] if after is None else [ends[j][1] for j in after]):
+                    st.wait_event(w)
+                e0, e1 = ev(), ev()
+                e0.record(st)
+                aeq.pusch_eq_fused(ds, tuned, st)
+                e1.record(st)
+                ends.append((e0, e1))
+            for st, _, _ in plan:
+                main.wait_stream(st)
+            torch.cuda.synchronize()
+            if r < 3:
+                continue
+            for k, (e0, e1) in enumerate(ends):
+                lat[k].append(1e3 * e0.elapsed_time(e1))
+            span.append(max(1e3 * g0.elapsed_time(e1) for _, e1 in ends))
+        return [med(v) for v in lat], med(span)
+
+    iso, _ = run([(plain[0], [descs[0]], None)])
+    iso = iso[0]
+    out = {"cell": "132 PRB x 64 antennas x 8 layers x 11 symbols, 256-QAM, complex64 in, float32 LLRs",
+           "alone_us": iso, "reps": reps, "l2": "flushed before every repetition",
+           "strategies": {}}
+    rows = {k: [] for k in "ABCDEF"}
+    for n in range(1, max_cells + 1):
+        def row(lat, span):
+            pc = sum(lat) / len(lat)
+            return {"n": n, "per_cell_us": pc, "makespan_us": span, "degradation": pc / iso,
+                    "cells_per_s": n / (span * 1e-6)}
+        lat, span = run([(plain[i], [descs[i]], None) for i in range(n)])
+        rows["A"].append(row(lat, span))
+        lat, span = run([(plain[0], [descs[i]], None if i == 0 else [i - 1]) for i in range(n)])
+        rows["B"].append(row(lat, span))
+        lat, span = run([(prio[i], [descs[i]], None) for i in range(n)])
+        r = row(lat, span)
+        r["high_priority_us"] = sum(lat[0::2]) / len(lat[0::2])
+        r["low_priority_us"] = sum(lat[1::2]) / len(lat[1::2]) if n > 1 else None
+        rows["C"].append(r)
+        per = -(-cells[0].nPRB // n)
+        chunks = [(p0, min(per, cells[0].nPRB - p0)) for p0 in range(0, cells[0].nPRB, per)]
+        lat, span = run([(plain[i], [prb_range_desc(aeq, cells[0], llrs[0], p0, m)], None)
+                         for i, (p0, m) in enumerate(chunks)])
+        rows["D"].append({"n": n, "chunks": len(chunks), "per_chunk_us": sum(lat) / len(lat),
+                          "makespan_us": span, "speedup_vs_alone": iso / span})
+        if n >= 2:
+            plan = [(plain[i % 2], [descs[i]], None if i < 2 else [2 * (i // 2) - 2, 2 * (i // 2) - 1])
+                    for i in range(n)]
+            lat, span = run(plan)
+            rows["E"].append(row(lat, span))
+        lat, span = run([(main, descs[:n], None)])   # every cell's results land at the launch's end
+        rows["F"].append(row(lat * n, span))
+    names = {"A": "unrestricted concurrent streams", "B": "serial on one stream",
+             "C": "stream priority, alternating high/low", "D": "one cell split by PRB range over N streams",
+             "E": "pairs of streams, serial between pairs", "F": "one persistent batched launch"}
+    for k in "ABCDEF":
+        out["strategies"][k] = {"name": names[k], "rows": rows[k]}
+    del flush
+    return out
 
 
 def bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a):
@@ -722,6 +846,16 @@ def _time_launches(fn, stream, k=50):
     return e0.elapsed_time(e1) * 1e3 / k
 
 
+def write_fill_gbs(buf, stream):
+    """Write-only HBM rate on this GPU: torch's fill of `buf`'s bytes as 4-byte
+    words (no reads; torch's FP16 fill is slower than its 4-byte fill), GB/s.
+    Context for the filter kernels, whose traffic is 80-89 % writes."""
+    import torch
+
+    words = (torch.view_as_real(buf) if buf.is_complex() else buf).reshape(-1).view(torch.int32)
+    return words.numel() * 4 / (_time_launches(lambda: words.fill_(0), stream) * 1e-6) / 1e9
+
+
 def bench_chest(aeq, dev, stream):
     """DMRS frequency-interpolation filter: the [64 x 96] x [96 x 4] product per output subcarrier named by the
     reference (README.md:200) -- 64 antennas, 96 pilot REs and 96 output subcarriers per 8-PRB block, 4 ports,
@@ -744,6 +878,7 @@ def bench_chest(aeq, dev, stream):
     gbs = nbytes / (us * 1e-6) / 1e9
     return {"us_per_launch": us, "blocks_per_launch": nBlk, "bytes_per_launch": nbytes,
             "achieved_gbs": gbs, "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": kind,
+            "write_share": 8 * H.numel() / nbytes, "write_fill_gbs": write_fill_gbs(H, stream),
             "gflops": flops / (us * 1e-6) / 1e9, "tensor_gflops": 2 * flops / (us * 1e-6) / 1e9,
             "shape": f"{nBlk} blocks x {nAnt} antennas, {nPilot} pilots -> {nOut} subcarriers x {P} ports, "
                      f"OCC length {F}; FP16 in, complex64 channel out; tensor cores (FP16 operands, taps split "
@@ -789,6 +924,7 @@ def bench_srs(aeq, dev, stream):
     return {"us_per_launch": us, "blocks_per_launch": nBlk, "blocks_per_s": nBlk / (us * 1e-6),
             "bytes_per_launch": nbytes,
             "achieved_gbs": gbs, "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": kind,
+            "write_share": 2 * out.numel() / nbytes, "write_fill_gbs": write_fill_gbs(out, stream),
             "gflops": flops / (us * 1e-6) / 1e9,
             "shape": f"{nBlk} blocks x {nAnt} antennas, K={K}, P={P}, FOCC length {F}, FP16 in/out, "
                      "tensor cores (FP16 operands, taps split hi/lo), FP32 accumulate"}

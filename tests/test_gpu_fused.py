@@ -111,6 +111,35 @@ def test_multicell_same_alone_and_in_mix(aeq, wl, cuda):
         np.testing.assert_array_equal(alone[1], mixed[i][1])
 
 
+@pytest.mark.parametrize("cfg,n", [(2, 3), (2, 8), (1, 5)])
+def test_prb_range_split_equals_whole_cell(aeq, wl, cuda, cfg, n):
+    """A cell split into PRB ranges (the same buffers at offsets, fewer PRBs)
+    gives the whole cell's LLRs and Y_eq bit for bit, whether the ranges run as
+    cells of one launch or as separate launches on separate streams."""
+    c = wl.config_cell(cfg, seed=61)
+    whole = run_fused(aeq, [c], cuda, "fp16")[0]
+    H, Y = c.H.to(cuda), c.Y.to(cuda)
+    per_llr, per_y = c.llr_numel // c.nSC, c.nLayers * c.nSym
+    step = -(-c.nPRB // n)
+    ranges = [(p0, min(step, c.nPRB - p0)) for p0 in range(0, c.nPRB, step)]
+
+    def descs(llr, yeq):
+        return [aeq.cell_desc(H[12 * p0:], Y[12 * p0:], llr[12 * p0 * per_llr:], c.sigma2, m, c.nAnt, c.nLayers,
+                              c.nSym, c.nPamBits, Y_eq=yeq[12 * p0 * per_y:]) for p0, m in ranges]
+    t = aeq.make_tuning("fp16")
+    llr = torch.full((c.llr_numel,), float("nan"), dtype=torch.float32, device=cuda)
+    yeq = torch.full((c.nSC * per_y,), float("nan"), dtype=torch.complex64, device=cuda)
+    aeq.pusch_eq_fused(descs(llr, yeq), t)
+    llr2, yeq2 = torch.full_like(llr, float("nan")), torch.full_like(yeq, float("nan"))
+    streams = [torch.cuda.Stream() for _ in ranges]
+    for d, s in zip(descs(llr2, yeq2), streams):
+        aeq.pusch_eq_fused([d], t, s)
+    torch.cuda.synchronize()
+    for l_, y_ in ((llr, yeq), (llr2, yeq2)):
+        np.testing.assert_array_equal(l_.cpu().numpy(), whole[0])
+        np.testing.assert_array_equal(y_.cpu().numpy(), whole[1])
+
+
 def test_multicell_vs_fp64(aeq, wl, orc, cuda):
     cells = wl.multicell(16, seed=29)
     res = run_fused(aeq, cells, cuda, "fp16")

@@ -19,9 +19,9 @@ SRS_CFGS = [(24, 4, 8), (24, 2, 8), (12, 4, 12), (12, 2, 12), (8, 1, 4), (10, 2,
             (48, 4, 8), (32, 16, 4), (44, 5, 4)]   # two K atoms; six 192-column tiles, the last partial; 48 max
 
 
-@pytest.mark.parametrize("K,P,F", SRS_CFGS)
-def test_srs_filter_vs_fp64(aeq, orc, cuda, K, P, F):
-    nBlk, nAnt = 66, 64
+@pytest.mark.parametrize("K,P,F,nBlk,nAnt", [c + (66, 64) for c in SRS_CFGS] +
+                         [(24, 4, 8, 5, 33), (44, 5, 4, 3, 7), (32, 16, 4, 2, 100)])   # rows not in 32s: clipped
+def test_srs_filter_vs_fp64(aeq, orc, cuda, K, P, F, nBlk, nAnt):
     s, w, f = orc.ref_srs_inputs(42, nBlk * nAnt * K, K * K, P * F)
     out = torch.empty(nBlk * nAnt * K * P * 2, dtype=torch.int16, device=cuda)
     aeq.srs_filter(out, _d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda),
@@ -87,7 +87,8 @@ def test_srs_to_channel_layout(aeq, orc, cuda, K, P, F):
 # antennas is the [64 x 96] x [96 x 4] product of the reference's README.md:200.
 # Pilot counts that are multiples of 4 (up to 96) run the tcgen05 kernel, the others the mma.sync kernel.
 CHEST_CFGS = [(96, 96, 4, 4, 64), (48, 96, 2, 2, 64), (96, 48, 4, 2, 33), (24, 12, 1, 1, 16), (56, 40, 3, 5, 48),
-              (64, 64, 2, 2, 64), (32, 20, 3, 3, 40), (45, 30, 2, 3, 40), (90, 90, 4, 2, 64), (20, 24, 4, 4, 64)]
+              (64, 64, 2, 2, 64), (32, 20, 3, 3, 40), (45, 30, 2, 3, 40), (90, 90, 4, 2, 64), (20, 24, 4, 4, 64),
+              (32, 30, 4, 2, 32)]   # 4 ports, 32 antennas, 30 outputs: the TMA store clips the last subcarriers
 
 
 @pytest.mark.parametrize("nPilot,nOut,P,F,nAnt", CHEST_CFGS)
