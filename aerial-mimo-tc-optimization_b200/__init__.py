@@ -129,6 +129,7 @@ SIGNATURES = {
     "aerial_srs_filter": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
     "aerial_srs_to_channel": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
     "aerial_chest_interp": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
+    "aerial_chest_interp_h": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
     "aerial_kernel_timeouts": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "aerial_pusch_eq_fused": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), _P]),
     "aerial_pusch_eq_plain_workspace": (_Z, [ctypes.POINTER(CellDesc), _I]),
@@ -268,6 +269,12 @@ def chest_interp(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, st
     """DMRS frequency-interpolation filter written as the PUSCH channel H[blk*nOut+o][ant][port] (complex64)."""
     _check(lib().aerial_chest_interp(_ptr(H), _ptr(Yp), _ptr(Wf), _ptr(OCC), nAnt, nBlocks, nPilot, nOut, nPorts,
                                      occLen, _stream(stream)), "chest_interp")
+
+
+def chest_interp_h(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, stream=None):
+    """The same filter written as complex half (float16 (re, im) pairs): the H of an FMT_CF16 cell."""
+    _check(lib().aerial_chest_interp_h(_ptr(H), _ptr(Yp), _ptr(Wf), _ptr(OCC), nAnt, nBlocks, nPilot, nOut, nPorts,
+                                       occLen, _stream(stream)), "chest_interp_h")
 
 
 # ---------------------------------------------------------------------------

@@ -53,6 +53,12 @@ constexpr int kChestMaxK = 96;               // pilots of the interpolation filt
 constexpr int kSrsSliceBytes = 96 * 1024;    // taps of one slice of output groups
 constexpr int kSrsGroupBytes = 4 * 32 * 16;  // one k-step of a group: 4 tiles x 32 lanes x 16 B
 
+// Output layouts of the filter kernels: the SRS filter's FP16
+// H_est[blk][ant][k_out][p]; the PUSCH channel H[blk*Ko + k_out][ant][p] as
+// complex64 (the equalizer's drop-in format) or as complex half (its FP16 I/O
+// format).
+enum OutLayout : int { kOutEst16 = 0, kOutChan32 = 1, kOutChan16 = 2 };
+
 __device__ __forceinline__ void mma_f16(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
                                         uint32_t b1) {
     asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -76,7 +82,7 @@ __device__ __forceinline__ void split_h2(float x, float y, uint32_t& hi, uint32_
 // taps per antenna, Ko filter outputs per block (Ko = K for the SRS filter).
 // Grid: x = CTAs walking the (block, 16 MT-antenna) items, y = slices of NQ
 // output groups (16 complex outputs per group).
-template <int KS, int MT, bool TO_CHANNEL>
+template <int KS, int MT, int OUTL>
 __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const __half2* __restrict__ srs,
                                                                           const __half2* __restrict__ W,
                                                                           const __half2* __restrict__ focc,
@@ -182,7 +188,24 @@ __global__ void __launch_bounds__(kSrsWarps * 32, 2) srs_filter_tc_kernel(const 
                 for (int rr = 0; rr < 2; rr++) {
                     const int ant = ant0 + 16 * mt + g + 8 * rr;
                     if (ant >= nAnt) continue;
-                    if constexpr (TO_CHANNEL) {
+                    if constexpr (OUTL == kOutChan16) {
+                        // H[sc = blk*Ko + ko][ant][layer = p] as complex half
+                        uint32_t* H = reinterpret_cast<uint32_t*>(out);
+                        uint32_t v[4];
+#pragma unroll
+                        for (int jj = 0; jj < 4; jj++)
+                            v[jj] = h2bits(__floats2half2_rn(d[jj][mt][2 * rr], d[jj][mt][2 * rr + 1]));
+                        if (P == 4 && full && (reinterpret_cast<uintptr_t>(H) & 15) == 0) {
+                            __stcs(reinterpret_cast<uint4*>(H + (((long)blk * Ko + n0 / 4) * nAnt + ant) * 4),
+                                   make_uint4(v[0], v[1], v[2], v[3]));
+                        } else {
+#pragma unroll
+                            for (int jj = 0; jj < 4; jj++) {
+                                const int n = n0 + jj;
+                                if (n < N) __stcs(H + (((long)blk * Ko + n / P) * nAnt + ant) * P + n % P, v[jj]);
+                            }
+                        }
+                    } else if constexpr (OUTL == kOutChan32) {
                         // H[sc = blk*Ko + ko][ant][layer = p], nLayers = P
                         float2* H = reinterpret_cast<float2*>(out);
                         if (P == 4 && full && (reinterpret_cast<uintptr_t>(H) & 15) == 0) {
@@ -303,9 +326,8 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
 }
 
 // KB: 64-element K atoms (2 nPilot <= 64 KB); NTL: real output columns per
-// tile (NTL / 2 complex outputs); OUT16: write the SRS filter's FP16
-// H_est[blk][ant][k_out][p] layout instead of the complex64 channel.
-template <int KB, int NTL, bool OUT16>
+// tile (NTL / 2 complex outputs); OUTL: the output layout (OutLayout).
+template <int KB, int NTL, int OUTL>
 __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                                       const __half2* __restrict__ Wf,
                                                                       const __half2* __restrict__ occ,
@@ -463,9 +485,34 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
                       "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(ta));
                 asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-                if (!mv) continue;
                 const int nb = (NTL / 2) * nt + 16 * c;  // complex outputs nb .. nb + 15 of this row
-                if constexpr (OUT16) {
+                if (!mv) continue;
+                if constexpr (OUTL == kOutChan16) {
+                    // channel as complex half: a subcarrier's 4 ports are one 16-byte
+                    // store, a warp's 32 antennas 512 contiguous bytes.  (Pairing
+                    // lanes by a shuffle into 256-bit stores measured no faster.)
+                    uint32_t h[16];
+#pragma unroll
+                    for (int jj = 0; jj < 16; jj++)
+                        h[jj] = h2bits(__floats2half2_rn(__uint_as_float(v[2 * jj]), __uint_as_float(v[2 * jj + 1])));
+                    uint32_t* H = reinterpret_cast<uint32_t*>(out);
+                    if (P == 4 && (reinterpret_cast<uintptr_t>(H) & 15) == 0) {
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            if (nb + 4 * q >= N) break;
+                            __stcs(reinterpret_cast<uint4*>(H + (((long)blk * nOut + (nb >> 2) + q) * nAnt + ant) * 4),
+                                   make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2], h[4 * q + 3]));
+                        }
+                    } else {
+#pragma unroll
+                        for (int jj = 0; jj < 16; jj++) {
+                            const int n = nb + jj;
+                            if (n < N) __stcs(H + (((long)blk * nOut + n / P) * nAnt + ant) * P + n % P, h[jj]);
+                        }
+                    }
+                    continue;
+                }
+                if constexpr (OUTL == kOutEst16) {
                     // H_est[blk][ant][n]: the row's 16 outputs are 64 contiguous bytes of half2
                     uint32_t h[16];
 #pragma unroll
@@ -540,7 +587,7 @@ static bool chest_umma_ok(const aerial_ch2* Yp, int nPilot) {
     return nPilot % 4 == 0 && nPilot <= 96 && (reinterpret_cast<uintptr_t>(Yp) & 15) == 0;
 }
 
-template <int KB, int NTL, bool OUT16>
+template <int KB, int NTL, int OUTL>
 static int launch_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
                              int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
     auto enc = tensor_map_encoder();
@@ -556,7 +603,7 @@ static int launch_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* 
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return AERIAL_ERR_UNSUPPORTED;
-    const int s = allow_max_smem<chest_umma_kernel<KB, NTL, OUT16>>();
+    const int s = allow_max_smem<chest_umma_kernel<KB, NTL, OUTL>>();
     if (s != AERIAL_OK) return s;
     // A stages + B + barriers, TMEM slot, abort flag and the 1024-byte
     // alignment slack; at least 120 KB so one CTA (its TMEM columns) runs per SM
@@ -568,14 +615,14 @@ static int launch_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* 
     long gx = std::max(1L, (long)sm_count() / nNT);
     gx = std::min(gx, nMT);
     dim3 grid((unsigned)gx, (unsigned)nNT);
-    chest_umma_kernel<KB, NTL, OUT16><<<grid, kUmmaThreads, smem, st>>>(tm, (const __half2*)Wf, (const __half2*)OCC, out,
+    chest_umma_kernel<KB, NTL, OUTL><<<grid, kUmmaThreads, smem, st>>>(tm, (const __half2*)Wf, (const __half2*)OCC, out,
                                                                    nAnt, nBlocks, nPilot, nOut, P, F);
     return launch_status();
 }
 
 // The filter on tcgen05 when the shape allows it; AERIAL_ERR_UNSUPPORTED
 // (nothing launched) otherwise, and the caller takes the mma.sync kernel.
-template <bool OUT16>
+template <int OUTL>
 static int try_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
                           int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
     if (!chest_umma_ok(Yp, nPilot)) return AERIAL_ERR_UNSUPPORTED;
@@ -584,21 +631,21 @@ static int try_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf,
     const bool wide = 2 * nOut * P > kUmmaN && nPilot <= 64;
     switch ((nPilot + 31) / 32) {
         case 1:
-            return wide ? launch_chest_umma<1, 192, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st)
-                        : launch_chest_umma<1, 128, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+            return wide ? launch_chest_umma<1, 192, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st)
+                        : launch_chest_umma<1, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
         case 2:
-            return wide ? launch_chest_umma<2, 192, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st)
-                        : launch_chest_umma<2, 128, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
-        default: return launch_chest_umma<3, 128, OUT16>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+            return wide ? launch_chest_umma<2, 192, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st)
+                        : launch_chest_umma<2, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+        default: return launch_chest_umma<3, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
     }
 }
 
-template <int KS, bool TO_CHANNEL>
+template <int KS, int OUTL>
 static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
                          int nBlocks, int K, int Ko, int P, int F, cudaStream_t st) {
     constexpr int MT = KS <= 6 ? 2 : 1;
-    auto kern = srs_filter_tc_kernel<KS, MT, TO_CHANNEL>;
-    const int s = allow_max_smem<srs_filter_tc_kernel<KS, MT, TO_CHANNEL>>();
+    auto kern = srs_filter_tc_kernel<KS, MT, OUTL>;
+    const int s = allow_max_smem<srs_filter_tc_kernel<KS, MT, OUTL>>();
     if (s != AERIAL_OK) return s;
     const int nGroups = (Ko * P + 15) / 16;
     const int groupBytes = KS * kSrsGroupBytes;
@@ -623,31 +670,33 @@ static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, 
 static int launch_srs_est(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
                           int nBlocks, int K, int P, int F, cudaStream_t st) {
     switch ((K + 7) / 8) {
-        case 1: return launch_srs_tc<1, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
-        case 2: return launch_srs_tc<2, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
-        case 3: return launch_srs_tc<3, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
-        case 4: return launch_srs_tc<4, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
-        case 5: return launch_srs_tc<5, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
-        default: return launch_srs_tc<6, false>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 1: return launch_srs_tc<1, kOutEst16>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 2: return launch_srs_tc<2, kOutEst16>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 3: return launch_srs_tc<3, kOutEst16>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 4: return launch_srs_tc<4, kOutEst16>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        case 5: return launch_srs_tc<5, kOutEst16>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
+        default: return launch_srs_tc<6, kOutEst16>(out, SRS, W, FOCC, nAnt, nBlocks, K, K, P, F, st);
     }
 }
 
-// Channel layout H[blk*Ko + ko][ant][p]: up to 96 input taps.
+// Channel layout H[blk*Ko + ko][ant][p] (OUTL: complex64 or complex half): up
+// to 96 input taps.
+template <int OUTL>
 static int launch_srs_chan(void* out, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC, int nAnt,
                            int nBlocks, int K, int Ko, int P, int F, cudaStream_t st) {
     switch ((K + 7) / 8) {
-        case 1: return launch_srs_tc<1, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 2: return launch_srs_tc<2, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 3: return launch_srs_tc<3, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 4: return launch_srs_tc<4, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 5: return launch_srs_tc<5, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 6: return launch_srs_tc<6, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 7: return launch_srs_tc<7, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 8: return launch_srs_tc<8, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 9: return launch_srs_tc<9, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 10: return launch_srs_tc<10, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        case 11: return launch_srs_tc<11, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
-        default: return launch_srs_tc<12, true>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 1: return launch_srs_tc<1, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 2: return launch_srs_tc<2, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 3: return launch_srs_tc<3, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 4: return launch_srs_tc<4, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 5: return launch_srs_tc<5, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 6: return launch_srs_tc<6, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 7: return launch_srs_tc<7, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 8: return launch_srs_tc<8, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 9: return launch_srs_tc<9, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 10: return launch_srs_tc<10, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        case 11: return launch_srs_tc<11, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
+        default: return launch_srs_tc<12, OUTL>(out, SRS, W, FOCC, nAnt, nBlocks, K, Ko, P, F, st);
     }
 }
 
@@ -672,7 +721,7 @@ extern "C" int aerial_kernel_timeouts(unsigned int* count) {
 extern "C" int aerial_srs_filter(aerial_ch2* H_est, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC,
                                  int nAnt, int nBlocks, int K, int nPorts, int foccLen, void* stream) {
     if (!srs_args_ok(H_est, SRS, W, FOCC, nAnt, nBlocks, K, kSrsMaxK, K, nPorts, foccLen)) return AERIAL_ERR_INVALID_ARG;
-    const int r = try_chest_umma<true>(H_est, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
+    const int r = try_chest_umma<kOutEst16>(H_est, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
     if (r != AERIAL_ERR_UNSUPPORTED) return r;
     return launch_srs_est(H_est, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, to_stream(stream));
 }
@@ -681,16 +730,28 @@ extern "C" int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, cons
                                      const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts, int foccLen,
                                      void* stream) {
     if (!srs_args_ok(H, SRS, W, FOCC, nAnt, nBlocks, K, kSrsMaxK, K, nPorts, foccLen)) return AERIAL_ERR_INVALID_ARG;
-    const int r = try_chest_umma<false>(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
+    const int r = try_chest_umma<kOutChan32>(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
     if (r != AERIAL_ERR_UNSUPPORTED) return r;
-    return launch_srs_chan(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
+    return launch_srs_chan<kOutChan32>(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
 }
 
 extern "C" int aerial_chest_interp(aerial_cf32* H, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC,
                                    int nAnt, int nBlocks, int nPilot, int nOut, int nPorts, int occLen, void* stream) {
     if (!srs_args_ok(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, kChestMaxK, nOut, nPorts, occLen))
         return AERIAL_ERR_INVALID_ARG;
-    const int r = try_chest_umma<false>(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
+    const int r = try_chest_umma<kOutChan32>(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen,
+                                             to_stream(stream));
     if (r != AERIAL_ERR_UNSUPPORTED) return r;
-    return launch_srs_chan(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
+    return launch_srs_chan<kOutChan32>(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
+}
+
+extern "C" int aerial_chest_interp_h(aerial_ch2* H, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC,
+                                     int nAnt, int nBlocks, int nPilot, int nOut, int nPorts, int occLen,
+                                     void* stream) {
+    if (!srs_args_ok(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, kChestMaxK, nOut, nPorts, occLen))
+        return AERIAL_ERR_INVALID_ARG;
+    const int r = try_chest_umma<kOutChan16>(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen,
+                                             to_stream(stream));
+    if (r != AERIAL_ERR_UNSUPPORTED) return r;
+    return launch_srs_chan<kOutChan16>(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
 }

@@ -876,9 +876,16 @@ def bench_chest(aeq, dev, stream):
     flops = 8.0 * nBlk * nAnt * nPilot * nOut * P
     peak, kind = measured_peaks()
     gbs = nbytes / (us * 1e-6) / 1e9
+    # the same filter writing the channel as complex half (the H of an FP16 I/O cell)
+    H16 = torch.empty(H.numel(), 2, dtype=torch.float16, device=dev)
+    us16 = _time_launches(lambda: aeq.chest_interp_h(H16, yp, wf, occ, nAnt, nBlk, nPilot, nOut, P, F, stream), stream)
+    nbytes16 = 2 * (yp.numel() + wf.numel() + occ.numel()) + 4 * H.numel()
+    fp16 = {"us_per_launch": us16, "bytes_per_launch": nbytes16, "achieved_gbs": nbytes16 / (us16 * 1e-6) / 1e9,
+            "hbm_frac": nbytes16 / (us16 * 1e-6) / 1e9 / peak}
     return {"us_per_launch": us, "blocks_per_launch": nBlk, "bytes_per_launch": nbytes,
             "achieved_gbs": gbs, "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": kind,
             "write_share": 8 * H.numel() / nbytes, "write_fill_gbs": write_fill_gbs(H, stream),
+            "fp16_channel": fp16,
             "gflops": flops / (us * 1e-6) / 1e9, "tensor_gflops": 2 * flops / (us * 1e-6) / 1e9,
             "shape": f"{nBlk} blocks x {nAnt} antennas, {nPilot} pilots -> {nOut} subcarriers x {P} ports, "
                      f"OCC length {F}; FP16 in, complex64 channel out; tensor cores (FP16 operands, taps split "

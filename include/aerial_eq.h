@@ -162,6 +162,14 @@ int aerial_chest_interp(aerial_cf32* H, const aerial_ch2* Yp, const aerial_ch2* 
                         const aerial_ch2* OCC, int nAnt, int nBlocks, int nPilot, int nOut,
                         int nPorts, int occLen, void* stream);
 
+/* The same filter writing the channel as complex half (H[blk*nOut + o][ant][p]
+ * in aerial_ch2): the H input of an AERIAL_FMT_CF16 cell.  Each value is
+ * aerial_chest_interp's FP32 sum rounded once to half (round to nearest
+ * even), bit for bit.  New: the reference has no FP16 channel producer. */
+int aerial_chest_interp_h(aerial_ch2* H, const aerial_ch2* Yp, const aerial_ch2* Wf,
+                          const aerial_ch2* OCC, int nAnt, int nBlocks, int nPilot, int nOut,
+                          int nPorts, int occLen, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Fused chain: Gram -> FP32 MMSE solve -> apply -> LLR in one kernel; G, C */
 /* and Y_eq stay on chip, only LLRs (and optionally Y_eq) are written.       */

@@ -88,7 +88,7 @@ def test_srs_to_channel_layout(aeq, orc, cuda, K, P, F):
 # Pilot counts that are multiples of 4 (up to 96) run the tcgen05 kernel, the others the mma.sync kernel.
 CHEST_CFGS = [(96, 96, 4, 4, 64), (48, 96, 2, 2, 64), (96, 48, 4, 2, 33), (24, 12, 1, 1, 16), (56, 40, 3, 5, 48),
               (64, 64, 2, 2, 64), (32, 20, 3, 3, 40), (45, 30, 2, 3, 40), (90, 90, 4, 2, 64), (20, 24, 4, 4, 64),
-              (32, 30, 4, 2, 32)]   # 4 ports, 32 antennas, 30 outputs: the TMA store clips the last subcarriers
+              (32, 30, 4, 2, 32), (48, 45, 4, 2, 34)]   # 4 ports, even antenna counts, ragged outputs
 
 
 @pytest.mark.parametrize("nPilot,nOut,P,F,nAnt", CHEST_CFGS)
@@ -102,6 +102,53 @@ def test_chest_interp_vs_fp64(aeq, orc, cuda, nPilot, nOut, P, F, nAnt):
     ref = orc.chest_f64(s, w, f, nAnt, nBlk, nPilot, nOut, P, F).reshape(nBlk * nOut, nAnt, P)
     # taps split into two FP16 parts, FP32 accumulation: the error of an FP32 sum
     assert evm_db(H.cpu().numpy(), ref) < -120
+
+
+@pytest.mark.parametrize("nPilot,nOut,P,F,nAnt", CHEST_CFGS)
+@pytest.mark.parametrize("offset", [0, 1])
+def test_chest_interp_h_equals_complex64_rounded(aeq, orc, cuda, nPilot, nOut, P, F, nAnt, offset):
+    """The complex-half channel is the complex64 channel rounded once to half,
+    bit for bit: the same FP32 sums on both kernels (tcgen05 and mma.sync),
+    at a 16-byte aligned and at a 4-byte aligned (offset one complex) start."""
+    nBlk = 7
+    s, w, f = orc.ref_srs_inputs(13, nBlk * nAnt * nPilot, nOut * nPilot, P * F)
+    args = (_d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda))
+    H32 = torch.empty(nBlk * nOut, nAnt, P, dtype=torch.complex64, device=cuda)
+    aeq.chest_interp(H32, *args, nAnt, nBlk, nPilot, nOut, P, F)
+    n = nBlk * nOut * nAnt * P
+    buf = torch.full((n + offset, 2), float("nan"), dtype=torch.float16, device=cuda)
+    H16 = buf[offset:]
+    aeq.chest_interp_h(H16, *args, nAnt, nBlk, nPilot, nOut, P, F)
+    torch.cuda.synchronize()
+    assert torch.equal(H16, torch.view_as_real(H32).reshape(n, 2).to(torch.float16))
+    if offset:
+        assert torch.isnan(buf[0]).all()                                 # nothing written before the start
+
+
+def test_chest_interp_h_feeds_fp16_io_cell(aeq, wl, orc, cuda):
+    """The FP16 channel straight from the pilots into an FP16 I/O cell (4
+    layers = 4 ports, 64 antennas, 33 blocks x 96 subcarriers = 264 PRB): the
+    LLRs equal those of the same cell built from the complex64 channel rounded
+    to half."""
+    nPilot, nOut, P, F, nAnt, nBlk = 96, 96, 4, 2, 64, 33
+    s, w, f = orc.ref_srs_inputs(14, nBlk * nAnt * nPilot, nOut * nPilot, P * F)
+    args = (_d(s.view(np.int16), cuda), _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda))
+    nSC = nBlk * nOut
+    H16 = torch.empty(nSC * nAnt * P, 2, dtype=torch.float16, device=cuda)
+    H32 = torch.empty(nSC, nAnt, P, dtype=torch.complex64, device=cuda)
+    aeq.chest_interp_h(H16, *args, nAnt, nBlk, nPilot, nOut, P, F)
+    aeq.chest_interp(H32, *args, nAnt, nBlk, nPilot, nOut, P, F)
+    c = wl.make_cell(nSC // 12, nAnt, P, 11, 64, 25.0, seed=15)
+    Y16 = torch.view_as_real(c.Y).to(torch.float16).contiguous().to(cuda)
+    outs = []
+    for H in (H16, torch.view_as_real(H32).reshape(-1, 2).to(torch.float16).contiguous()):
+        llr = torch.full((c.llr_numel,), float("nan"), dtype=torch.float16, device=cuda)
+        d = aeq.cell_desc(H, Y16, llr, c.sigma2, c.nPRB, nAnt, P, 11, c.nPamBits, fmt=aeq.FMT_CF16)
+        aeq.pusch_eq_fused([d], aeq.make_tuning("fp16"))
+        outs.append(llr)
+    torch.cuda.synchronize()
+    assert torch.isfinite(outs[0].float()).all()
+    assert torch.equal(outs[0], outs[1])
 
 
 def test_chest_interp_many_tiles_per_cta(aeq, orc, cuda):
