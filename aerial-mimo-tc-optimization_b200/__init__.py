@@ -154,6 +154,7 @@ SIGNATURES = {
     "aerial_server_pause": (_I, [_P, _I]),
     "aerial_server_stats": (_I, [_P, ctypes.POINTER(ServerStats)]),
     "aerial_server_reset_stats": (_I, [_P]),
+    "aerial_server_inject_alloc_failure": (_I, [_P, _I]),
 }
 
 
@@ -489,6 +490,10 @@ class Server:
 
     def reset_stats(self):
         _check(lib().aerial_server_reset_stats(self._h), "server_reset_stats")
+
+    def inject_alloc_failure(self, nth):
+        """Fault injection for tests: the nth device allocation from now on fails (0 disarms)."""
+        _check(lib().aerial_server_inject_alloc_failure(self._h, int(nth)), "server_inject_alloc_failure")
 
     def close(self):
         if self._h:

@@ -96,7 +96,24 @@ struct aerial_server {
     long resDone = 0, batchesLaunched = 0, slotsLaunched = 0, srsDone = 0, misses = 0;
     int launchError = 0;
     int inflightBatches = 0;           // batches launched and not finished (under mu)
+    int failAllocIn = 0;               // fault injection: the n-th next device allocation fails (0 = off)
 };
+
+// A device allocation of the server.  A failed cudaMalloc leaves its error in
+// the runtime's last-error state, which a later launch check would read as
+// its own, so it is cleared here.  With fault injection armed the n-th
+// allocation fails with cudaErrorMemoryAllocation without calling the
+// runtime (host side only).  Lock held.
+static cudaError_t srv_malloc(aerial_server* s, void** p, size_t bytes) {
+    *p = nullptr;
+    if (s->failAllocIn > 0 && --s->failAllocIn == 0) return cudaErrorMemoryAllocation;
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        *p = nullptr;
+    }
+    return e;
+}
 
 static void finish_batch(aerial_server* s, SrvBatch& b, int status) {
     const int64_t t = now_ns();
@@ -133,6 +150,8 @@ struct Formed {
     aerial_cf32* H = nullptr;
     const aerial_ch2 *S = nullptr, *W = nullptr, *F = nullptr;
     int nAnt = 0, nBlocks = 0, K = 0, P = 0, foccLen = 0;
+    void* ws = nullptr;                 // the plain chain's workspace of this stream
+    size_t wsBytes = 0;
 };
 
 // Form one batch for stream i from the pending queue; lock held.
@@ -212,7 +231,7 @@ static int launch_formed(aerial_server* s, int i, const Formed& f) {
     } else if (s->cfg.mode == AERIAL_SERVER_PLAIN) {
         // the plain FP32 chain, request by request (comparison mode)
         for (int k = 0; k < f.n && !status; k++)
-            status = aerial_pusch_eq_plain(&f.descs[k], 1, s->plainWs[i], s->plainWsBytes, st);
+            status = aerial_pusch_eq_plain(&f.descs[k], 1, f.ws, f.wsBytes, st);
     } else {
         aerial_tuning t{s->cfg.precision, 0, 0, 0};
         status = aerial_pusch_eq_fused(f.descs, f.n, &t, st);
@@ -256,6 +275,10 @@ static void dispatcher(aerial_server* s) {
             f.n = 0;
             f.srs = false;
             if (!s->paused && !s->pending.empty() && batch_ready(s)) form_batch(s, (int)i, f);
+            if (s->cfg.mode == AERIAL_SERVER_PLAIN) {
+                f.ws = s->plainWs.empty() ? nullptr : s->plainWs[i];
+                f.wsBytes = s->plainWsBytes;
+            }
             const bool formed = f.n > 0 || f.srs;
             if (formed) {
                 b.busy = true;
@@ -356,42 +379,62 @@ extern "C" int aerial_server_add_cell(aerial_server* s, int nPRB, int nAnt, int 
     c.hBytes = sizeof(aerial_cf32) * nSC * nAnt * nLayers;
     c.reqBytes = (int64_t)(sizeof(aerial_cf32) * nSC * nSym * nAnt + sizeof(float) * nSC * nLayers * nSym * 2 * nPamBits);
     c.res = nSC * nSym;
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (s->used + (int64_t)c.hBytes + c.reqBytes > s->cfg.memory_budget_bytes) return AERIAL_ERR_BUDGET;
-    cudaError_t e = cudaMalloc(&c.H, c.hBytes);
-    if (e != cudaSuccess) return (int)e;
-    cudaMemset(c.H, 0, c.hBytes);
-    c.shape.H = c.H;
     c.shape.sigma2 = sigma2;
     c.shape.nPRB = nPRB;
     c.shape.nAnt = nAnt;
     c.shape.nLayers = nLayers;
     c.shape.nSym = nSym;
     c.shape.nPamBits = nPamBits;
-    s->used += (int64_t)c.hBytes;
+    std::unique_lock<std::mutex> lk(s->mu);
+    // plain mode: the per-stream workspaces grow to the largest cell
+    size_t need = 0;
+    int64_t extra = 0;
     if (s->cfg.mode == AERIAL_SERVER_PLAIN) {
-        // the plain chain's intermediates, one workspace per stream, sized for the largest cell
-        const size_t need = aerial_pusch_eq_plain_workspace(&c.shape, 1);
-        if (need > s->plainWsBytes) {
-            const int64_t extra = (int64_t)(need - s->plainWsBytes) * (int64_t)s->streams.size();
-            if (s->used + extra + c.reqBytes > s->cfg.memory_budget_bytes) {
-                s->used -= (int64_t)c.hBytes;
-                cudaFree(c.H);
-                return AERIAL_ERR_BUDGET;
-            }
-            s->plainWs.resize(s->streams.size(), nullptr);
-            for (void*& w : s->plainWs) {
-                cudaFree(w);
-                w = nullptr;
-                e = cudaMalloc(&w, need);
-                if (e != cudaSuccess) return (int)e;
-            }
-            s->used += extra;
-            s->plainWsBytes = need;
-        }
+        need = aerial_pusch_eq_plain_workspace(&c.shape, 1);
+        if (need > s->plainWsBytes) extra = (int64_t)(need - s->plainWsBytes) * (int64_t)s->streams.size();
+        else need = 0;
+    }
+    if (s->used + (int64_t)c.hBytes + extra + c.reqBytes > s->cfg.memory_budget_bytes) return AERIAL_ERR_BUDGET;
+    // Everything is allocated before anything is committed: a failed
+    // allocation leaves the server as it was.
+    void* h = nullptr;
+    int status = (int)srv_malloc(s, &h, c.hBytes);
+    if (status) return status;
+    std::vector<void*> fresh(need ? s->streams.size() : 0, nullptr);
+    for (void*& w : fresh)
+        if (!status) status = (int)srv_malloc(s, &w, need);
+    if (!status && need) {
+        // the old workspaces may be in use: wait (bounded) until no batch is in
+        // flight; none can form while the lock is held afterwards
+        const auto limit = std::chrono::steady_clock::now() + std::chrono::seconds(10);
+        while (s->inflightBatches > 0 && !status)
+            if (s->doneCv.wait_until(lk, limit) == std::cv_status::timeout && s->inflightBatches > 0)
+                status = AERIAL_ERR_TIMEOUT;
+    }
+    if (status) {
+        for (void* w : fresh) cudaFree(w);
+        cudaFree(h);
+        return status;
+    }
+    c.H = static_cast<aerial_cf32*>(h);
+    cudaMemset(c.H, 0, c.hBytes);
+    c.shape.H = c.H;
+    s->used += (int64_t)c.hBytes;
+    if (need) {
+        for (void* w : s->plainWs) cudaFree(w);
+        s->plainWs = std::move(fresh);
+        s->plainWsBytes = need;
+        s->used += extra;
     }
     s->cells.push_back(c);
     *cellId = (int)s->cells.size() - 1;
+    return AERIAL_OK;
+}
+
+extern "C" int aerial_server_inject_alloc_failure(aerial_server* s, int nth) {
+    if (!s || nth < 0) return AERIAL_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->failAllocIn = nth;
     return AERIAL_OK;
 }
 

@@ -361,6 +361,13 @@ int aerial_server_pause(aerial_server* server, int paused);
 int aerial_server_stats(aerial_server* server, aerial_server_statistics* out);
 /* Forget the latency samples and counters gathered so far (e.g. after warm-up). */
 int aerial_server_reset_stats(aerial_server* server);
+/* Fault injection for tests: the nth device allocation the server makes from
+ * now on (nth >= 1; aerial_server_add_cell makes one for the resident channel
+ * and, in AERIAL_SERVER_PLAIN mode, one workspace per stream when the cell is
+ * the largest so far) fails with cudaErrorMemoryAllocation without calling
+ * the CUDA runtime; 0 disarms.  Host side only.  A failed allocation leaves
+ * the server as it was. */
+int aerial_server_inject_alloc_failure(aerial_server* server, int nth);
 
 /* ------------------------------------------------------------------------ */
 /* Autotuner                                                                  */

@@ -78,6 +78,7 @@ def test_server_rejects_bad_config_without_gpu():
     cfg = pkg.ServerConfig(1 << 30, 0, 64, 0, 0, 0, 0, 500.0, 0.0, 0)   # no stream
     assert lib.aerial_server_create(ctypes.byref(cfg), ctypes.byref(h)) == 1001
     assert lib.aerial_server_destroy(None) == 1001
+    assert lib.aerial_server_inject_alloc_failure(None, 1) == 1001
     n = ctypes.c_int()
     assert lib.aerial_server_poll(None, None, 0, ctypes.byref(n)) == 1001
 

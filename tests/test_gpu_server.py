@@ -164,3 +164,65 @@ def test_server_deadline_misses_counted_for_late_producer(aeq, wl, cuda):
         torch.cuda.synchronize()
         for o in outs[1:]:
             assert torch.equal(o, outs[0])                        # same slot, same LLRs, late or not
+
+
+@pytest.mark.parametrize("mode,nth", [("fused", 1), ("plain", 1), ("plain", 3)])
+def test_server_allocation_failure_leaves_server_usable(aeq, wl, cuda, mode, nth):
+    """A device allocation that fails inside add_cell (injected on the host:
+    the runtime is not called) leaves the server as it was: no cell added, the
+    budget unchanged, and the cell already there serves bit-identical results.
+    nth = 1 fails the channel's allocation; in the plain mode with two streams
+    nth = 3 fails the second workspace of the regrowth, after the channel and
+    the first workspace were allocated.  The same cell then adds cleanly."""
+    plain = mode == "plain"
+    small = wl.make_cell(4, 16, 2, 11, 4, 15.0, seed=131)
+    big = wl.make_cell(24, 32, 4, 11, 16, 20.0, seed=132)
+    with aeq.Server(streams=2, mode=aeq.SERVER_PLAIN if plain else aeq.SERVER_FUSED) as srv:
+        Hs = small.H.to(cuda)
+        k0 = srv.add_cell(small.nPRB, small.nAnt, small.nLayers, small.nSym, small.nPamBits, small.sigma2)
+        srv.set_channel(k0, Hs, small.sigma2)
+        used = srv.stats()["budget_used_bytes"]
+        srv.inject_alloc_failure(nth)
+        with pytest.raises(aeq.AerialError) as err:
+            srv.add_cell(big.nPRB, big.nAnt, big.nLayers, big.nSym, big.nPamBits, big.sigma2)
+        assert err.value.status == 2                                   # cudaErrorMemoryAllocation
+        assert srv.stats()["budget_used_bytes"] == used
+        Ys = small.Y.to(cuda)
+        out = torch.full((small.llr_numel,), float("nan"), dtype=torch.float32, device=cuda)
+        assert srv.wait(srv.submit(k0, Ys, out)) == 0
+        np.testing.assert_array_equal(out.cpu().numpy(), _alone(aeq, small, Hs, Ys, cuda, plain))
+        k1 = srv.add_cell(big.nPRB, big.nAnt, big.nLayers, big.nSym, big.nPamBits, big.sigma2)
+        assert k1 == k0 + 1
+        Hb, Yb = big.H.to(cuda), big.Y.to(cuda)
+        srv.set_channel(k1, Hb, big.sigma2)
+        outs = [torch.full((c.llr_numel,), float("nan"), dtype=torch.float32, device=cuda) for c in (small, big)]
+        ids = [srv.submit(k0, Ys, outs[0]), srv.submit(k1, Yb, outs[1])]
+        assert all(srv.wait(i) == 0 for i in ids)
+    np.testing.assert_array_equal(outs[0].cpu().numpy(), _alone(aeq, small, Hs, Ys, cuda, plain))
+    np.testing.assert_array_equal(outs[1].cpu().numpy(), _alone(aeq, big, Hb, Yb, cuda, plain))
+
+
+def test_server_plain_workspace_regrowth_while_slots_in_flight(aeq, wl, cuda):
+    """In the plain mode a larger cell regrows every stream's workspace.  Added
+    while slots of a smaller cell are queued and running, it waits until no
+    batch holds the old workspaces, so every slot's LLRs stay bit-identical."""
+    small = wl.make_cell(24, 32, 2, 11, 16, 20.0, seed=141)
+    big = wl.make_cell(51, 64, 8, 11, 64, 25.0, seed=142)
+    with aeq.Server(streams=3, mode=aeq.SERVER_PLAIN) as srv:
+        Hs, Ys = small.H.to(cuda), small.Y.to(cuda)
+        k0 = srv.add_cell(small.nPRB, small.nAnt, small.nLayers, small.nSym, small.nPamBits, small.sigma2)
+        srv.set_channel(k0, Hs, small.sigma2)
+        outs = [torch.full((small.llr_numel,), float("nan"), dtype=torch.float32, device=cuda) for _ in range(24)]
+        ids = [srv.submit(k0, Ys, o) for o in outs]
+        k1 = srv.add_cell(big.nPRB, big.nAnt, big.nLayers, big.nSym, big.nPamBits, big.sigma2)
+        Hb, Yb = big.H.to(cuda), big.Y.to(cuda)
+        srv.set_channel(k1, Hb, big.sigma2)
+        ob = torch.full((big.llr_numel,), float("nan"), dtype=torch.float32, device=cuda)
+        ids.append(srv.submit(k1, Yb, ob))
+        outs += [torch.full_like(outs[0], float("nan")) for _ in range(4)]
+        ids += [srv.submit(k0, Ys, o) for o in outs[-4:]]
+        assert all(srv.wait(i) == 0 for i in ids)
+    ref = _alone(aeq, small, Hs, Ys, cuda, plain=True)
+    for o in outs:
+        np.testing.assert_array_equal(o.cpu().numpy(), ref)
+    np.testing.assert_array_equal(ob.cpu().numpy(), _alone(aeq, big, Hb, Yb, cuda, plain=True))
