@@ -20,6 +20,17 @@ inline int launch_status() {
     return e == cudaSuccess ? AERIAL_OK : (int)e;
 }
 
+// Status of a runtime call.  A failed call also leaves its error in the
+// calling thread's last-error state, where the next launch check
+// (launch_status) would read it as that launch's own; once returned here it
+// is cleared.  Sticky errors (a faulted context) stay, as the runtime keeps
+// them.
+inline int rt_status(cudaError_t e) {
+    if (e == cudaSuccess) return AERIAL_OK;
+    (void)cudaGetLastError();
+    return (int)e;
+}
+
 inline cudaStream_t to_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 constexpr int kMaxDevices = 64;                 // devices with cached per-device state
@@ -48,11 +59,11 @@ int allow_max_smem() {
     static bool done[kMaxDevices] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return (int)e;
+    if (e != cudaSuccess) return rt_status(e);
     std::lock_guard<std::mutex> lock(mu);
     if (dev >= 0 && dev < kMaxDevices && done[dev]) return AERIAL_OK;
     e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmemPerCta);
-    if (e != cudaSuccess) return (int)e;
+    if (e != cudaSuccess) return rt_status(e);
     if (dev >= 0 && dev < kMaxDevices) done[dev] = true;
     return AERIAL_OK;
 }

@@ -1628,7 +1628,7 @@ int launch_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, 
     if (s) return s;
     void* args[] = {const_cast<FusedParams*>(&p)};
     cudaError_t e = cudaLaunchKernel(pl.func, pl.grid, pl.block, args, (size_t)pl.smem, st);
-    return e == cudaSuccess ? AERIAL_OK : (int)e;
+    return rt_status(e);
 }
 
 // Resolve precision and launch shape from an optional tuning struct.
@@ -1711,7 +1711,7 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
             if (s) break;
             cudaError_t e = cudaEventSynchronize(e1);
             if (e != cudaSuccess) {
-                s = (int)e;
+                s = rt_status(e);
                 break;
             }
             float ms = 0.f;
@@ -1791,7 +1791,7 @@ extern "C" int aerial_eq_graph_create(const aerial_cell_desc* cells, int nCells,
         e = cudaGraphAddKernelNode(&g->node, g->graph, nullptr, 0, &kp);
     }
     if (!s && e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
-    if (!s && e != cudaSuccess) s = (int)e;
+    if (!s && e != cudaSuccess) s = rt_status(e);
     if (s) {
         if (g->exec) cudaGraphExecDestroy(g->exec);
         if (g->graph) cudaGraphDestroy(g->graph);
@@ -1818,13 +1818,13 @@ extern "C" int aerial_eq_graph_update(aerial_eq_graph* g, const aerial_cell_desc
     void* args[] = {&g->params};
     cudaKernelNodeParams kp = node_params(g, args);
     cudaError_t e = cudaGraphExecKernelNodeSetParams(g->exec, g->node, &kp);
-    return e == cudaSuccess ? AERIAL_OK : (int)e;
+    return rt_status(e);
 }
 
 extern "C" int aerial_eq_graph_launch(aerial_eq_graph* g, void* stream) {
     if (!g) return AERIAL_ERR_INVALID_ARG;
     cudaError_t e = cudaGraphLaunch(g->exec, to_stream(stream));
-    return e == cudaSuccess ? AERIAL_OK : (int)e;
+    return rt_status(e);
 }
 
 extern "C" int aerial_eq_graph_destroy(aerial_eq_graph* g) {
@@ -1832,7 +1832,8 @@ extern "C" int aerial_eq_graph_destroy(aerial_eq_graph* g) {
     cudaError_t e1 = g->exec ? cudaGraphExecDestroy(g->exec) : cudaSuccess;
     cudaError_t e2 = g->graph ? cudaGraphDestroy(g->graph) : cudaSuccess;
     delete g;
-    return e1 != cudaSuccess ? (int)e1 : (e2 != cudaSuccess ? (int)e2 : AERIAL_OK);
+    const int s1 = rt_status(e1), s2 = rt_status(e2);
+    return s1 ? s1 : s2;
 }
 
 namespace aeq {
@@ -1846,14 +1847,14 @@ template <int P, int LTF>
 static int prepare_v() {
     cudaFuncAttributes at;
     const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel<P, LTF>);
-    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel<P, LTF>>() : (int)e;
+    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel<P, LTF>>() : rt_status(e);
 }
 
 template <int P, int LTF, int NCH>
 static int prepare_a() {
     cudaFuncAttributes at;
     const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_a<P, LTF, NCH>);
-    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_a<P, LTF, NCH>>() : (int)e;
+    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_a<P, LTF, NCH>>() : rt_status(e);
 }
 
 template <int P, int LTF>
@@ -1868,7 +1869,7 @@ template <int LTF, int NCH>
 static int prepare_h() {
     cudaFuncAttributes at;
     const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_h<LTF, NCH>);
-    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_h<LTF, NCH>>() : (int)e;
+    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_h<LTF, NCH>>() : rt_status(e);
 }
 
 template <int P>

@@ -93,7 +93,7 @@ static size_t slot_bytes(const aerial_cell_desc* cells, int nCells, int bs) {
 static int host_pipe(HostPipe** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return (int)e;
+    if (e != cudaSuccess) return rt_status(e);
     if (dev < 0 || dev >= 64) return AERIAL_ERR_UNSUPPORTED;
     if (!g_pipes[dev]) {
         HostPipe* p = new HostPipe();
@@ -104,7 +104,7 @@ static int host_pipe(HostPipe** out) {
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->start, cudaEventDisableTiming);
         if (e != cudaSuccess) {
             delete p;  // the handles made so far stay with the context
-            return (int)e;
+            return rt_status(e);
         }
         g_pipes[dev] = p;
     }
@@ -147,7 +147,7 @@ extern "C" int aerial_pusch_eq_host(const aerial_cell_desc* cells, int nCells, c
     const cudaStream_t caller = to_stream(stream);
     cudaError_t e = cudaEventRecord(hp->start, caller);
     for (int k = 0; k < slots && e == cudaSuccess; k++) e = cudaStreamWaitEvent(hp->s[k], hp->start, 0);
-    if (e != cudaSuccess) return (int)e;
+    if (e != cudaSuccess) return rt_status(e);
 
     // Batch b runs on stream b % slots with workspace slot b % slots: the
     // stream order keeps a slot's next batch behind its previous copies out.
@@ -193,6 +193,6 @@ extern "C" int aerial_pusch_eq_host(const aerial_cell_desc* cells, int nCells, c
         if (r != cudaSuccess && je == cudaSuccess) je = r;
     }
     if (st) return st;
-    if (e != cudaSuccess) return (int)e;
+    if (e != cudaSuccess) return rt_status(e);
     return je == cudaSuccess ? AERIAL_OK : (int)je;
 }

@@ -348,13 +348,13 @@ static int static_scratch_address(void** out) {
     static void* addr[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return (int)e;
+    if (e != cudaSuccess) return rt_status(e);
     if (dev < 0 || dev >= 64) return AERIAL_ERR_NO_DEVICE;
     std::lock_guard<std::mutex> lock(mu);
     if (!addr[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_plain_static_scratch);
-        if (e != cudaSuccess) return (int)e;
+        if (e != cudaSuccess) return rt_status(e);
         addr[dev] = p;
     }
     *out = addr[dev];

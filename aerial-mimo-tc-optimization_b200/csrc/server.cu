@@ -99,20 +99,16 @@ struct aerial_server {
     int failAllocIn = 0;               // fault injection: the n-th next device allocation fails (0 = off)
 };
 
-// A device allocation of the server.  A failed cudaMalloc leaves its error in
-// the runtime's last-error state, which a later launch check would read as
-// its own, so it is cleared here.  With fault injection armed the n-th
-// allocation fails with cudaErrorMemoryAllocation without calling the
-// runtime (host side only).  Lock held.
-static cudaError_t srv_malloc(aerial_server* s, void** p, size_t bytes) {
+// A device allocation of the server, as a status (rt_status clears a failed
+// cudaMalloc's error from the thread's last-error state).  With fault
+// injection armed the n-th allocation fails with cudaErrorMemoryAllocation
+// without calling the runtime (host side only).  Lock held.
+static int srv_malloc(aerial_server* s, void** p, size_t bytes) {
     *p = nullptr;
-    if (s->failAllocIn > 0 && --s->failAllocIn == 0) return cudaErrorMemoryAllocation;
-    const cudaError_t e = cudaMalloc(p, bytes);
-    if (e != cudaSuccess) {
-        (void)cudaGetLastError();
-        *p = nullptr;
-    }
-    return e;
+    if (s->failAllocIn > 0 && --s->failAllocIn == 0) return (int)cudaErrorMemoryAllocation;
+    const int status = rt_status(cudaMalloc(p, bytes));
+    if (status) *p = nullptr;
+    return status;
 }
 
 static void finish_batch(aerial_server* s, SrvBatch& b, int status) {
@@ -238,7 +234,7 @@ static int launch_formed(aerial_server* s, int i, const Formed& f) {
     }
     if (!status) {
         cudaError_t e = cudaEventRecord(s->batches[i].ev, st);
-        if (e != cudaSuccess) status = (int)e;
+        if (e != cudaSuccess) status = rt_status(e);
     }
     return status;
 }
@@ -257,7 +253,7 @@ static void dispatcher(aerial_server* s) {
             const cudaError_t e = cudaEventQuery(b.ev);
             if (e == cudaErrorNotReady) continue;
             lk.lock();
-            finish_batch(s, b, e == cudaSuccess ? AERIAL_OK : (int)e);
+            finish_batch(s, b, rt_status(e));
             s->inflightBatches--;
             lk.unlock();
             s->doneCv.notify_all();
@@ -340,7 +336,7 @@ extern "C" int aerial_server_create(const aerial_server_config* cfg, aerial_serv
                 if (s->batches[k].ev) cudaEventDestroy(s->batches[k].ev);
             }
             delete s;
-            return (int)e;
+            return rt_status(e);
         }
     }
     s->th = std::thread(dispatcher, s);
@@ -398,11 +394,11 @@ extern "C" int aerial_server_add_cell(aerial_server* s, int nPRB, int nAnt, int 
     // Everything is allocated before anything is committed: a failed
     // allocation leaves the server as it was.
     void* h = nullptr;
-    int status = (int)srv_malloc(s, &h, c.hBytes);
+    int status = srv_malloc(s, &h, c.hBytes);
     if (status) return status;
     std::vector<void*> fresh(need ? s->streams.size() : 0, nullptr);
     for (void*& w : fresh)
-        if (!status) status = (int)srv_malloc(s, &w, need);
+        if (!status) status = srv_malloc(s, &w, need);
     if (!status && need) {
         // the old workspaces may be in use: wait (bounded) until no batch is in
         // flight; none can form while the lock is held afterwards
@@ -450,7 +446,7 @@ extern "C" int aerial_server_set_channel(aerial_server* s, int cellId, const aer
     }
     cudaError_t e = cudaMemcpy(c.H, H, c.hBytes, cudaMemcpyDefault);
     c.shape.sigma2 = sigma2;
-    return e == cudaSuccess ? AERIAL_OK : (int)e;
+    return rt_status(e);
 }
 
 extern "C" int aerial_server_submit(aerial_server* s, int cellId, const aerial_cf32* Y_rx, float* llr,

@@ -654,7 +654,7 @@ static int launch_srs_tc(void* out, const aerial_ch2* SRS, const aerial_ch2* W, 
     const size_t smem = (size_t)NQ * groupBytes;
     int perSm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kern, kSrsWarps * 32, smem);
-    if (e != cudaSuccess) return (int)e;
+    if (e != cudaSuccess) return rt_status(e);
     const long items = (long)nBlocks * ((nAnt + 16 * MT - 1) / (16 * MT));
     const long ctasForItems = (items + kSrsWarps - 1) / kSrsWarps;
     // enough CTAs to fill the GPU once per slice; each walks its share of items
@@ -715,7 +715,7 @@ using namespace aeq;
 extern "C" int aerial_kernel_timeouts(unsigned int* count) {
     if (!count) return AERIAL_ERR_INVALID_ARG;
     const cudaError_t e = cudaMemcpyFromSymbol(count, g_umma_timeouts, sizeof(unsigned int));
-    return e == cudaSuccess ? AERIAL_OK : (int)e;
+    return rt_status(e);
 }
 
 extern "C" int aerial_srs_filter(aerial_ch2* H_est, const aerial_ch2* SRS, const aerial_ch2* W, const aerial_ch2* FOCC,

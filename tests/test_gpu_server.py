@@ -226,3 +226,18 @@ def test_server_plain_workspace_regrowth_while_slots_in_flight(aeq, wl, cuda):
     for o in outs:
         np.testing.assert_array_equal(o.cpu().numpy(), ref)
     np.testing.assert_array_equal(ob.cpu().numpy(), _alone(aeq, big, Hb, Yb, cuda, plain=True))
+
+
+def test_real_allocation_failure_does_not_leak_into_the_next_launch(aeq, wl, cuda):
+    """A real cudaMalloc failure (a 393 GB channel: the runtime refuses it and
+    touches no memory) is returned by add_cell and cleared from this thread's
+    last-error state, so the next launch on the thread reports its own
+    success rather than the old failure."""
+    with aeq.Server(memory_budget_bytes=1 << 50, streams=1) as srv:
+        with pytest.raises(aeq.AerialError) as err:
+            srv.add_cell(1_000_000, 256, 16, 14, 4, 0.01)     # 8 B x 12M subcarriers x 256 x 16
+        assert err.value.status == 2                          # cudaErrorMemoryAllocation
+        assert srv.stats()["budget_used_bytes"] == 0
+    c = wl.make_cell(4, 16, 2, 11, 4, 15.0, seed=151)
+    llr = _alone(aeq, c, c.H.to(cuda), c.Y.to(cuda), cuda)    # raises if its launch check saw the old error
+    assert np.isfinite(llr).all()
