@@ -29,6 +29,7 @@ PREC_FP16, PREC_BF16, PREC_BF16X3, PREC_FP32 = 0, 1, 2, 3
 PREC_NAMES = {"fp16": PREC_FP16, "bf16": PREC_BF16, "bf16x3": PREC_BF16X3, "fp32": PREC_FP32}
 FMT_CF32, FMT_CF16 = 0, 1          # cell storage formats (aerial_cell_desc.format)
 MAX_CELLS = 64
+MAX_PRB = 524288            # AERIAL_MAX_PRB: PRBs per cell descriptor
 
 
 class AerialError(RuntimeError):

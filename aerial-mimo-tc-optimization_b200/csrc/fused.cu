@@ -1418,8 +1418,9 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
     warpBytes = 0;
     for (int i = 0; i < nCells; i++) {
         const aerial_cell_desc& c = cells[i];
+        if (c.nPRB < 1 || c.nPRB > AERIAL_MAX_PRB) return AERIAL_ERR_INVALID_ARG;
         const int nSC = c.nPRB * 12;
-        if (!c.H || !c.Y_rx || !c.llr || c.nPRB < 1 || c.nAnt < 1 || c.nAnt > AERIAL_MAX_ANTS || c.nLayers < 1 ||
+        if (!c.H || !c.Y_rx || !c.llr || c.nAnt < 1 || c.nAnt > AERIAL_MAX_ANTS || c.nLayers < 1 ||
             c.nLayers > AERIAL_MAX_LAYERS || c.nSym < 1 || c.nSym > AERIAL_MAX_SYMS || c.nPamBits < 1 ||
             c.nPamBits > 4 || !(c.sigma2 >= 0.f))
             return AERIAL_ERR_INVALID_ARG;

@@ -55,7 +55,7 @@ static size_t cell_footprint(const aerial_cell_desc& c) {
 // Host-side envelope of one cell (the device-side checks run again on the
 // staged descriptors inside aerial_pusch_eq_fused).
 static bool host_cell_ok(const aerial_cell_desc& c) {
-    return c.H && c.Y_rx && c.llr && c.nPRB >= 1 && c.nAnt >= 1 && c.nAnt <= AERIAL_MAX_ANTS && c.nLayers >= 1 &&
+    return c.H && c.Y_rx && c.llr && c.nPRB >= 1 && c.nPRB <= AERIAL_MAX_PRB && c.nAnt >= 1 && c.nAnt <= AERIAL_MAX_ANTS && c.nLayers >= 1 &&
            c.nLayers <= AERIAL_MAX_LAYERS && c.nSym >= 1 && c.nSym <= AERIAL_MAX_SYMS && c.nPamBits >= 1 &&
            c.nPamBits <= 4 && c.sigma2 >= 0.f && (c.format == AERIAL_FMT_CF32 || c.format == AERIAL_FMT_CF16);
 }
@@ -194,5 +194,5 @@ extern "C" int aerial_pusch_eq_host(const aerial_cell_desc* cells, int nCells, c
     }
     if (st) return st;
     if (e != cudaSuccess) return rt_status(e);
-    return je == cudaSuccess ? AERIAL_OK : (int)je;
+    return rt_status(je);
 }

@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(512) llr_f32_kernel(const cf* __restrict__ in,
 // host launchers
 // ---------------------------------------------------------------------------
 static bool shape_ok(int nSC, int nSym, int L, int A) {
-    return nSC >= 1 && nSym >= 1 && nSym <= AERIAL_MAX_SYMS && L >= 1 && L <= AERIAL_MAX_LAYERS && A >= 1 &&
+    return nSC >= 1 && nSC <= 12 * AERIAL_MAX_PRB && nSym >= 1 && nSym <= AERIAL_MAX_SYMS && L >= 1 && L <= AERIAL_MAX_LAYERS && A >= 1 &&
            A <= AERIAL_MAX_ANTS;
 }
 
@@ -297,6 +297,7 @@ extern "C" int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, 
     cudaStream_t st = to_stream(stream);
     for (int i = 0; i < nCells; i++) {
         const aerial_cell_desc& c = cells[i];
+        if (c.nPRB < 1 || c.nPRB > AERIAL_MAX_PRB) return AERIAL_ERR_INVALID_ARG;
         int nSC = c.nPRB * 12;
         if (!c.H || !c.Y_rx || !c.llr || c.nPamBits < 1 || c.nPamBits > 4 || !shape_ok(nSC, c.nSym, c.nLayers, c.nAnt))
             return AERIAL_ERR_INVALID_ARG;

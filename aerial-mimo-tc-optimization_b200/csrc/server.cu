@@ -366,7 +366,7 @@ extern "C" int aerial_server_destroy(aerial_server* s) {
 
 extern "C" int aerial_server_add_cell(aerial_server* s, int nPRB, int nAnt, int nLayers, int nSym, int nPamBits,
                                       float sigma2, int* cellId) {
-    if (!s || !cellId || nPRB < 1 || nAnt < 1 || nAnt > AERIAL_MAX_ANTS || nLayers < 1 ||
+    if (!s || !cellId || nPRB < 1 || nPRB > AERIAL_MAX_PRB || nAnt < 1 || nAnt > AERIAL_MAX_ANTS || nLayers < 1 ||
         nLayers > AERIAL_MAX_LAYERS || nSym < 1 || nSym > AERIAL_MAX_SYMS || nPamBits < 1 || nPamBits > 4 ||
         !(sigma2 >= 0.f))
         return AERIAL_ERR_INVALID_ARG;

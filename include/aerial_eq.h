@@ -63,7 +63,11 @@ enum {
 };
 
 /* Supported envelope: 1 <= nLayers <= 16, 1 <= nSym <= 16, 1 <= nAnt <= 256,
- * 1 <= nPamBits <= 4 (QPSK..256QAM), nSC >= 1. */
+ * 1 <= nPamBits <= 4 (QPSK..256QAM), 1 <= nPRB <= AERIAL_MAX_PRB per cell
+ * descriptor (nSC = 12 nPRB; the per-stage entry points take nSC up to
+ * 12 AERIAL_MAX_PRB).  The PRB bound keeps every symbol index of a cell
+ * (nSC x nLayers x nSym) inside 32 bits. */
+#define AERIAL_MAX_PRB 524288
 #define AERIAL_MAX_LAYERS 16
 #define AERIAL_MAX_SYMS 16
 #define AERIAL_MAX_ANTS 256

@@ -109,6 +109,10 @@ def test_host_pipeline_workspace_and_checks_without_gpu():
     assert lib.aerial_pusch_eq_host_workspace(None, 5, 0, ctypes.byref(b)) == 1001
     bad = (pkg.CellDesc * 1)(desc(132, 64, 17, 11, 4))
     assert lib.aerial_pusch_eq_host_workspace(bad, 1, 0, ctypes.byref(b)) == 1001
+    wide = (pkg.CellDesc * 1)(desc(pkg.MAX_PRB + 1, 16, 2, 11, 4))   # beyond AERIAL_MAX_PRB
+    assert lib.aerial_pusch_eq_host_workspace(wide, 1, 0, ctypes.byref(b)) == 1001
+    wide[0].nPRB = pkg.MAX_PRB
+    assert lib.aerial_pusch_eq_host_workspace(wide, 1, 0, ctypes.byref(b)) == 0
     ws = ctypes.c_void_p(0x200000)
     assert lib.aerial_pusch_eq_host(arr, 5, None, 2, ws, 1024, None) == 1001         # workspace too small
     assert lib.aerial_pusch_eq_host(arr, 5, None, 2, ctypes.c_void_p(0x200010), 1 << 40, None) == 1001  # misaligned

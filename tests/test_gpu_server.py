@@ -229,13 +229,17 @@ def test_server_plain_workspace_regrowth_while_slots_in_flight(aeq, wl, cuda):
 
 
 def test_real_allocation_failure_does_not_leak_into_the_next_launch(aeq, wl, cuda):
-    """A real cudaMalloc failure (a 393 GB channel: the runtime refuses it and
-    touches no memory) is returned by add_cell and cleared from this thread's
-    last-error state, so the next launch on the thread reports its own
-    success rather than the old failure."""
+    """A real cudaMalloc failure (a 206 GB channel at the largest cell the
+    envelope allows: the runtime refuses it and touches no memory) is returned
+    by add_cell and cleared from this thread's last-error state, so the next
+    launch on the thread reports its own success rather than the old
+    failure."""
     with aeq.Server(memory_budget_bytes=1 << 50, streams=1) as srv:
         with pytest.raises(aeq.AerialError) as err:
-            srv.add_cell(1_000_000, 256, 16, 14, 4, 0.01)     # 8 B x 12M subcarriers x 256 x 16
+            srv.add_cell(aeq.MAX_PRB + 1, 16, 2, 11, 4, 0.01)
+        assert err.value.status == 1001                       # beyond the envelope: checked on the host
+        with pytest.raises(aeq.AerialError) as err:
+            srv.add_cell(aeq.MAX_PRB, 256, 16, 14, 4, 0.01)  # 8 B x 6.3 M subcarriers x 256 x 16
         assert err.value.status == 2                          # cudaErrorMemoryAllocation
         assert srv.stats()["budget_used_bytes"] == 0
     c = wl.make_cell(4, 16, 2, 11, 4, 15.0, seed=151)
