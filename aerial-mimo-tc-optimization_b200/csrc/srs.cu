@@ -38,6 +38,7 @@
 // fragments (two 16-antenna m-tiles, the whole K) are loaded once from global
 // memory, then it sweeps the slice's groups.
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
 
 #include <cuda.h>
@@ -583,8 +584,10 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // is a multiple of 16, up to 96 pilots, from a 16-byte aligned array.  The
 // tensor map is encoded per call; a shape it rejects falls back to the
 // mma.sync kernel.
-static bool chest_umma_ok(const aerial_ch2* Yp, int nPilot) {
-    return nPilot % 4 == 0 && nPilot <= 96 && (reinterpret_cast<uintptr_t>(Yp) & 15) == 0;
+static bool chest_umma_ok(const aerial_ch2* Yp, int nPilot, long rows) {
+    // TMA row coordinates are 32-bit: more rows take the mma.sync kernel
+    return nPilot % 4 == 0 && nPilot <= 96 && (reinterpret_cast<uintptr_t>(Yp) & 15) == 0 &&
+           rows <= (long)INT32_MAX - kUmmaM;
 }
 
 template <int KB, int NTL, int OUTL>
@@ -625,7 +628,7 @@ static int launch_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* 
 template <int OUTL>
 static int try_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
                           int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
-    if (!chest_umma_ok(Yp, nPilot)) return AERIAL_ERR_UNSUPPORTED;
+    if (!chest_umma_ok(Yp, nPilot, (long)nBlocks * nAnt)) return AERIAL_ERR_UNSUPPORTED;
     // 192-column tiles where more than 128 real output columns exist and the
     // operands fit (up to 64 pilots); 128 otherwise
     const bool wide = 2 * nOut * P > kUmmaN && nPilot <= 64;
