@@ -823,27 +823,39 @@ def bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a):
 
 
 def accuracy_vs_fp64(orc, aeq, cells, llrs, descs, tun, stream):
-    """Checker: slot 0's fused result against the FP64 model of the oracle."""
+    """Checker: slot 0 against the FP64 model of the oracle, through the fused
+    launch at the bench's operand precision (the top-level keys), and under
+    `by_path` at every operand precision and through the plain FP32 chain
+    (the reference's method), so the precisions compare at the same EVM."""
     import numpy as np
     import torch
 
     c = cells[0]
-    H, Y = c.H.cpu().numpy(), c.Y.cpu().numpy()
-    yeq = torch.empty(c.nSC * c.nLayers * c.nSym, dtype=torch.complex64, device=c.H.device)
-    d = aeq.cell_desc(c.H, c.Y, llrs[0], c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, Y_eq=yeq)
-    aeq.pusch_eq_fused([d], tun, stream)
-    torch.cuda.synchronize()
-    y64, _, l64 = orc.chain_f64(H, Y, c.sigma2, c.nSC, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
-    y = yeq.cpu().numpy().astype(np.complex128)
-    l = llrs[0].cpu().numpy().astype(np.float64)
-    evm = 10 * np.log10(np.sum(np.abs(y - y64) ** 2) / np.sum(np.abs(y64) ** 2))
+    y64, _, l64 = orc.chain_f64(c.H.cpu().numpy(), c.Y.cpu().numpy(), c.sigma2, c.nSC, c.nAnt, c.nLayers, c.nSym,
+                                c.nPamBits)
     bits = c.bits.cpu().numpy().reshape(-1)
-    return {
-        "evm_db": float(evm), "llr_max_abs_err": float(np.abs(l - l64).max()),
-        "llr_scale": float(np.abs(l64).max()),
-        "hard_bit_mismatch": int(np.sum((l < 0) != (l64 < 0))), "bits": int(l.size),
-        "ber_vs_tx": float(np.mean((l < 0).astype(np.uint8) != bits)),
-    }
+
+    def run(fn):
+        llr = torch.empty(c.llr_numel, dtype=torch.float32, device=c.H.device)
+        yeq = torch.empty(c.nSC * c.nLayers * c.nSym, dtype=torch.complex64, device=c.H.device)
+        d = aeq.cell_desc(c.H, c.Y, llr, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, Y_eq=yeq)
+        fn(d)
+        torch.cuda.synchronize()
+        y = yeq.cpu().numpy().astype(np.complex128)
+        l = llr.cpu().numpy().astype(np.float64)
+        return {"evm_db": float(10 * np.log10(np.sum(np.abs(y - y64) ** 2) / np.sum(np.abs(y64) ** 2))),
+                "llr_max_abs_err": float(np.abs(l - l64).max()), "llr_scale": float(np.abs(l64).max()),
+                "hard_bit_mismatch": int(np.sum((l < 0) != (l64 < 0))), "bits": int(l.size),
+                "ber_vs_tx": float(np.mean((l < 0).astype(np.uint8) != bits))}
+
+    out = run(lambda d: aeq.pusch_eq_fused([d], tun, stream))
+    by = {}
+    for name in ("fp16", "bf16", "bf16x3"):
+        by["fused_" + name] = run(lambda d: aeq.pusch_eq_fused([d], aeq.make_tuning(name), stream))
+    ws = torch.empty(aeq.pusch_eq_plain_workspace(descs[:1]), dtype=torch.uint8, device=c.H.device)
+    by["plain_fp32_chain"] = run(lambda d: aeq.pusch_eq_plain([d], ws, stream))
+    out["by_path"] = by
+    return out
 
 
 def _time_launches(fn, stream, k=50):
