@@ -130,6 +130,7 @@ SIGNATURES = {
     "aerial_srs_filter": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
     "aerial_srs_to_channel": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P]),
     "aerial_chest_interp": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
+    "aerial_srs_to_channel_avg": (_I, [_P, _P, _I, _P, _P, _I, _I, _I, _I, _I, _P]),
     "aerial_chest_interp_h": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
     "aerial_kernel_timeouts": (_I, [ctypes.POINTER(ctypes.c_uint)]),
     "aerial_pusch_eq_fused": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), _P]),
@@ -148,6 +149,7 @@ SIGNATURES = {
     "aerial_server_add_cell": (_I, [_P, _I, _I, _I, _I, _I, _F, ctypes.POINTER(_I)]),
     "aerial_server_set_channel": (_I, [_P, _I, _P, _F]),
     "aerial_server_srs_update": (_I, [_P, _I, _P, _P, _P, _I, _I, ctypes.POINTER(ctypes.c_uint64)]),
+    "aerial_server_srs_update_n": (_I, [_P, _I, _P, _I, _P, _P, _I, _I, ctypes.POINTER(ctypes.c_uint64)]),
     "aerial_server_submit": (_I, [_P, _I, _P, _P, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64)]),
     "aerial_server_poll": (_I, [_P, ctypes.POINTER(ServerCompletion), _I, ctypes.POINTER(_I)]),
     "aerial_server_wait": (_I, [_P, ctypes.c_uint64, _I]),
@@ -258,6 +260,12 @@ def srs_to_channel(H, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, stream=No
     """SRS filter multiply written as the PUSCH channel H[blk*K+k_out][ant][port] (complex64)."""
     _check(lib().aerial_srs_to_channel(_ptr(H), _ptr(SRS), _ptr(W), _ptr(FOCC), nAnt, nBlocks, K, nPorts, foccLen,
                                        _stream(stream)), "srs_to_channel")
+
+
+def srs_to_channel_avg(H, SRS, nSrsSym, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, stream=None):
+    """srs_to_channel averaged over nSrsSym (1, 2 or 4) consecutive SRS symbols in SRS."""
+    _check(lib().aerial_srs_to_channel_avg(_ptr(H), _ptr(SRS), int(nSrsSym), _ptr(W), _ptr(FOCC), nAnt, nBlocks, K,
+                                           nPorts, foccLen, _stream(stream)), "srs_to_channel_avg")
 
 
 def kernel_timeouts() -> int:
@@ -452,10 +460,12 @@ class Server:
         _check(lib().aerial_server_set_channel(self._h, cell, ctypes.c_void_p(H.data_ptr()), float(sigma2)),
                "server_set_channel")
 
-    def srs_update(self, cell, SRS, W, FOCC, K, foccLen) -> int:
+    def srs_update(self, cell, SRS, W, FOCC, K, foccLen, n_symbols=1) -> int:
+        """Queue an SRS update of the cell's resident channel; n_symbols (1, 2
+        or 4) consecutive SRS symbols in SRS are averaged."""
         rid = ctypes.c_uint64()
-        _check(lib().aerial_server_srs_update(self._h, cell, _ptr(SRS), _ptr(W), _ptr(FOCC), K, foccLen,
-                                              ctypes.byref(rid)), "server_srs_update")
+        _check(lib().aerial_server_srs_update_n(self._h, cell, _ptr(SRS), int(n_symbols), _ptr(W), _ptr(FOCC), K,
+                                                foccLen, ctypes.byref(rid)), "server_srs_update")
         return rid.value
 
     def submit(self, cell, Y, llr_out, arrival_ns=0) -> int:

@@ -54,7 +54,7 @@ struct SrvReq {
     float* llr = nullptr;
     // SRS update operands
     const aerial_ch2 *srs = nullptr, *W = nullptr, *focc = nullptr;
-    int K = 0, P = 0, F = 0;
+    int K = 0, P = 0, F = 0, nSrs = 1;
     int64_t arrival = 0, launched = 0, done = 0;
     int status = AERIAL_OK;
     bool admitted = false, finished = false;
@@ -145,7 +145,7 @@ struct Formed {
     bool srs = false;                   // an SRS update instead
     aerial_cf32* H = nullptr;
     const aerial_ch2 *S = nullptr, *W = nullptr, *F = nullptr;
-    int nAnt = 0, nBlocks = 0, K = 0, P = 0, foccLen = 0;
+    int nAnt = 0, nBlocks = 0, K = 0, P = 0, foccLen = 0, nSrs = 1;
     void* ws = nullptr;                 // the plain chain's workspace of this stream
     size_t wsBytes = 0;
 };
@@ -182,6 +182,7 @@ static void form_batch(aerial_server* s, int i, Formed& f) {
                 f.K = r->K;
                 f.P = r->P;
                 f.foccLen = r->F;
+                f.nSrs = r->nSrs;
                 return;
             }
             blocked[r->cell] = 1;       // the cell's later slots wait behind its update
@@ -223,7 +224,7 @@ static int launch_formed(aerial_server* s, int i, const Formed& f) {
     cudaStream_t st = s->streams[i];
     int status = AERIAL_OK;
     if (f.srs) {
-        status = aerial_srs_to_channel(f.H, f.S, f.W, f.F, f.nAnt, f.nBlocks, f.K, f.P, f.foccLen, st);
+        status = aerial_srs_to_channel_avg(f.H, f.S, f.nSrs, f.W, f.F, f.nAnt, f.nBlocks, f.K, f.P, f.foccLen, st);
     } else if (s->cfg.mode == AERIAL_SERVER_PLAIN) {
         // the plain FP32 chain, request by request (comparison mode)
         for (int k = 0; k < f.n && !status; k++)
@@ -480,9 +481,17 @@ extern "C" int aerial_server_submit(aerial_server* s, int cellId, const aerial_c
 
 extern "C" int aerial_server_srs_update(aerial_server* s, int cellId, const aerial_ch2* SRS, const aerial_ch2* W,
                                         const aerial_ch2* FOCC, int K, int foccLen, uint64_t* requestId) {
-    if (!s || !SRS || !W || !FOCC || K < 1 || foccLen < 1) return AERIAL_ERR_INVALID_ARG;
+    return aerial_server_srs_update_n(s, cellId, SRS, 1, W, FOCC, K, foccLen, requestId);
+}
+
+extern "C" int aerial_server_srs_update_n(aerial_server* s, int cellId, const aerial_ch2* SRS, int nSrsSym,
+                                          const aerial_ch2* W, const aerial_ch2* FOCC, int K, int foccLen,
+                                          uint64_t* requestId) {
+    if (!s || !SRS || !W || !FOCC || K < 1 || foccLen < 1 || (nSrsSym != 1 && nSrsSym != 2 && nSrsSym != 4))
+        return AERIAL_ERR_INVALID_ARG;
     SrvReq* r = new SrvReq();
     r->kind = 1;
+    r->nSrs = nSrsSym;
     r->srs = SRS;
     r->W = W;
     r->focc = FOCC;

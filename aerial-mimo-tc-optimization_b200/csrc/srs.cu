@@ -328,20 +328,25 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
 
 // KB: 64-element K atoms (2 nPilot <= 64 KB); NTL: real output columns per
 // tile (NTL / 2 complex outputs); OUTL: the output layout (OutLayout).
+// nSrs input symbols (1, 2 or 4; tmA is [nSrs][rows][2 nPilot]) give the
+// average of their filter outputs: the K loop runs over every symbol's A
+// tile into one FP32 accumulator, with the taps scaled by 1/nSrs (exact for
+// these counts), so (1/S) sum_s f(in_s) is one GEMM with K extended over S.
 template <int KB, int NTL, int OUTL>
 __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                                       const __half2* __restrict__ Wf,
                                                                       const __half2* __restrict__ occ,
                                                                       void* __restrict__ out, int nAnt, int nBlocks,
-                                                                      int nPilot, int nOut, int P, int F) {
+                                                                      int nPilot, int nOut, int P, int F, int nSrs) {
     extern __shared__ __align__(1024) uint8_t usm_raw[];
     // 128-byte swizzle atoms must start on 1024-byte boundaries of the shared window
     uint8_t* usm = usm_raw + ((1024u - (smem_u32(usm_raw) & 1023u)) & 1023u);
-    // layout: A stages [2][KB atoms of 128 rows] | B [hi, lo][KB atoms of NTL rows] | barriers | TMEM slot
+    // layout: A stages [2][nSrs x KB atoms of 128 rows] | B [hi, lo][KB atoms of NTL rows] | barriers | TMEM slot
     constexpr int kBAtom = NTL * 128;             // bytes of one B atom column block
     constexpr int kTCols = umma_tmem_cols(NTL);
+    const uint32_t aStage = (uint32_t)nSrs * KB * kUmmaAtomBytes;
     uint8_t* sA = usm;
-    uint8_t* sB = usm + 2 * KB * kUmmaAtomBytes;
+    uint8_t* sB = usm + 2 * aStage;
     uint64_t* bars = reinterpret_cast<uint64_t*>(sB + 2 * KB * kBAtom);
     // bars: full[2], empty[2], tfull[2], tempty[2]
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 8);
@@ -378,6 +383,7 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
             const float2 w = __half22float2(Wf[(n / P) * nPilot + kc]);
             const float2 f = __half22float2(occ[(n % P) * F + (kc % F)]);
             t = make_float2(w.x * f.x - w.y * f.y, w.x * f.y + w.y * f.x);
+            if (nSrs > 1) t = make_float2(t.x * (1.f / nSrs), t.y * (1.f / nSrs));   // a power of two: exact
         }
         uint32_t hi0, lo0, hi1, lo1;
         split_h2(t.x, -t.y, hi0, lo0);           // row 2j: Re out
@@ -405,16 +411,18 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
                 const int s = (int)(i & 1);
                 if (!mbar_wait(empty0 + 8 * s, (uint32_t)(((i >> 1) & 1) ^ 1), abort)) break;
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(full0 + 8 * s),
-                             "r"(KB * kUmmaAtomBytes)
+                             "r"(aStage)
                              : "memory");
+                for (int q = 0; q < nSrs; q++)
 #pragma unroll
-                for (int kb = 0; kb < KB; kb++)
-                    asm volatile(
-                        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-                        "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(smem_u32(sA + (s * KB + kb) * kUmmaAtomBytes)),
-                        "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(kb * kUmmaKB), "r"((int)(mt * kUmmaM)),
-                        "r"(full0 + 8 * s)
-                        : "memory");
+                    for (int kb = 0; kb < KB; kb++)
+                        asm volatile(
+                            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                            "[%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+                                smem_u32(sA + s * aStage + (uint32_t)(q * KB + kb) * kUmmaAtomBytes)),
+                            "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(kb * kUmmaKB), "r"((int)(mt * kUmmaM)), "r"(q),
+                            "r"(full0 + 8 * s)
+                            : "memory");
             }
             // leave no copy in flight: the last two stages' loads have landed
             for (long d = (i > 2 ? i - 2 : 0); d < i; d++) mbar_wait(full0 + 8 * (d & 1), (uint32_t)((d >> 1) & 1), abort);
@@ -429,23 +437,26 @@ __global__ void __launch_bounds__(kUmmaThreads, 1) chest_umma_kernel(const __gri
                 if (!mbar_wait(full0 + 8 * s, ph, abort)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                 const uint32_t dt = tbase + (uint32_t)(a * NTL);
-                const uint32_t a0 = smem_u32(sA + s * KB * kUmmaAtomBytes);
+                const uint32_t a0 = smem_u32(sA + s * aStage);
                 const uint32_t b0 = smem_u32(sB);
 #pragma unroll
                 for (int part = 0; part < 2; part++) {
+                    for (int q = 0; q < nSrs; q++) {
 #pragma unroll
-                    for (int kb = 0; kb < KB; kb++) {
+                        for (int kb = 0; kb < KB; kb++) {
 #pragma unroll
-                        for (int kk = 0; kk < kUmmaKB / 16; kk++) {
-                            if (kb * kUmmaKB + kk * 16 >= 2 * nPilot) break;   // K steps past the pilots
-                            const uint64_t ad = umma_desc_sw128(a0 + kb * kUmmaAtomBytes + kk * 32);
-                            const uint64_t bd = umma_desc_sw128(b0 + (part * KB + kb) * kBAtom + kk * 32);
-                            const uint32_t acc = (part | kb | kk) ? 1u : 0u;
-                            asm volatile(
-                                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dt),
-                                "l"(ad), "l"(bd), "r"(umma_idesc(NTL)), "r"(acc)
-                                : "memory");
+                            for (int kk = 0; kk < kUmmaKB / 16; kk++) {
+                                if (kb * kUmmaKB + kk * 16 >= 2 * nPilot) break;   // K steps past the pilots
+                                const uint64_t ad =
+                                    umma_desc_sw128(a0 + (uint32_t)(q * KB + kb) * kUmmaAtomBytes + kk * 32);
+                                const uint64_t bd = umma_desc_sw128(b0 + (part * KB + kb) * kBAtom + kk * 32);
+                                const uint32_t acc = (part | q | kb | kk) ? 1u : 0u;
+                                asm volatile(
+                                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dt),
+                                    "l"(ad), "l"(bd), "r"(umma_idesc(NTL)), "r"(acc)
+                                    : "memory");
+                            }
                         }
                     }
                 }
@@ -592,54 +603,58 @@ static bool chest_umma_ok(const aerial_ch2* Yp, int nPilot, long rows) {
 
 template <int KB, int NTL, int OUTL>
 static int launch_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
-                             int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
+                             int nBlocks, int nPilot, int nOut, int P, int F, int nSrs, cudaStream_t st) {
     auto enc = tensor_map_encoder();
     if (!enc) return AERIAL_ERR_UNSUPPORTED;
     const long M = (long)nBlocks * nAnt;
+    // A stages (nSrs x KB atoms each) + B + barriers, TMEM slot, abort flag
+    // and the 1024-byte alignment slack; at least 120 KB so one CTA (its TMEM
+    // columns) runs per SM
+    const size_t smem = std::max<size_t>((size_t)2 * nSrs * KB * kUmmaAtomBytes + (size_t)2 * KB * NTL * 128 +
+                                             8 * sizeof(uint64_t) + 16 + 1024,
+                                         120 * 1024);
+    if (smem > (size_t)kMaxSmemPerCta) return AERIAL_ERR_UNSUPPORTED;
     CUtensorMap tm;
-    // K extent 2 nPilot; a 64-element box past it (nPilot < 32 KB) reads zeros
-    const cuuint64_t dims[2] = {(cuuint64_t)(2 * nPilot), (cuuint64_t)M};
-    const cuuint64_t strides[1] = {(cuuint64_t)(4 * nPilot)};
-    const cuuint32_t box[2] = {(cuuint32_t)kUmmaKB, (cuuint32_t)kUmmaM};
-    const cuuint32_t estr[2] = {1, 1};
-    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<aerial_ch2*>(Yp), dims, strides, box, estr,
+    // [nSrs][M rows][2 nPilot]: K extent 2 nPilot; a 64-element box past it
+    // (nPilot < 32 KB) reads zeros
+    const cuuint64_t dims[3] = {(cuuint64_t)(2 * nPilot), (cuuint64_t)M, (cuuint64_t)nSrs};
+    const cuuint64_t strides[2] = {(cuuint64_t)(4 * nPilot), (cuuint64_t)M * 4 * nPilot};
+    const cuuint32_t box[3] = {(cuuint32_t)kUmmaKB, (cuuint32_t)kUmmaM, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<aerial_ch2*>(Yp), dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return AERIAL_ERR_UNSUPPORTED;
     const int s = allow_max_smem<chest_umma_kernel<KB, NTL, OUTL>>();
     if (s != AERIAL_OK) return s;
-    // A stages + B + barriers, TMEM slot, abort flag and the 1024-byte
-    // alignment slack; at least 120 KB so one CTA (its TMEM columns) runs per SM
-    const size_t smem = std::max<size_t>((size_t)2 * KB * (kUmmaAtomBytes + NTL * 128) + 8 * sizeof(uint64_t) + 16 +
-                                             1024,
-                                         120 * 1024);
     const int nNT = (2 * nOut * P + NTL - 1) / NTL;
     const long nMT = (M + kUmmaM - 1) / kUmmaM;
     long gx = std::max(1L, (long)sm_count() / nNT);
     gx = std::min(gx, nMT);
     dim3 grid((unsigned)gx, (unsigned)nNT);
     chest_umma_kernel<KB, NTL, OUTL><<<grid, kUmmaThreads, smem, st>>>(tm, (const __half2*)Wf, (const __half2*)OCC, out,
-                                                                   nAnt, nBlocks, nPilot, nOut, P, F);
+                                                                   nAnt, nBlocks, nPilot, nOut, P, F, nSrs);
     return launch_status();
 }
 
 // The filter on tcgen05 when the shape allows it; AERIAL_ERR_UNSUPPORTED
 // (nothing launched) otherwise, and the caller takes the mma.sync kernel.
+// nSrs > 1 averages that many consecutive input symbols.
 template <int OUTL>
 static int try_chest_umma(void* out, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC, int nAnt,
-                          int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st) {
+                          int nBlocks, int nPilot, int nOut, int P, int F, cudaStream_t st, int nSrs = 1) {
     if (!chest_umma_ok(Yp, nPilot, (long)nBlocks * nAnt)) return AERIAL_ERR_UNSUPPORTED;
     // 192-column tiles where more than 128 real output columns exist and the
     // operands fit (up to 64 pilots); 128 otherwise
     const bool wide = 2 * nOut * P > kUmmaN && nPilot <= 64;
     switch ((nPilot + 31) / 32) {
         case 1:
-            return wide ? launch_chest_umma<1, 192, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st)
-                        : launch_chest_umma<1, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+            return wide ? launch_chest_umma<1, 192, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, nSrs, st)
+                        : launch_chest_umma<1, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, nSrs, st);
         case 2:
-            return wide ? launch_chest_umma<2, 192, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st)
-                        : launch_chest_umma<2, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
-        default: return launch_chest_umma<3, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, st);
+            return wide ? launch_chest_umma<2, 192, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, nSrs, st)
+                        : launch_chest_umma<2, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, nSrs, st);
+        default: return launch_chest_umma<3, 128, OUTL>(out, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, P, F, nSrs, st);
     }
 }
 
@@ -736,6 +751,17 @@ extern "C" int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, cons
     const int r = try_chest_umma<kOutChan32>(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
     if (r != AERIAL_ERR_UNSUPPORTED) return r;
     return launch_srs_chan<kOutChan32>(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream));
+}
+
+extern "C" int aerial_srs_to_channel_avg(aerial_cf32* H, const aerial_ch2* SRS, int nSrsSym, const aerial_ch2* W,
+                                         const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts, int foccLen,
+                                         void* stream) {
+    if (nSrsSym != 1 && nSrsSym != 2 && nSrsSym != 4) return AERIAL_ERR_INVALID_ARG;
+    if (nSrsSym == 1) return aerial_srs_to_channel(H, SRS, W, FOCC, nAnt, nBlocks, K, nPorts, foccLen, stream);
+    if (!srs_args_ok(H, SRS, W, FOCC, nAnt, nBlocks, K, kSrsMaxK, K, nPorts, foccLen)) return AERIAL_ERR_INVALID_ARG;
+    // the average runs inside the tcgen05 kernel's K loop only
+    return try_chest_umma<kOutChan32>(H, SRS, W, FOCC, nAnt, nBlocks, K, K, nPorts, foccLen, to_stream(stream),
+                                      nSrsSym);
 }
 
 extern "C" int aerial_chest_interp(aerial_cf32* H, const aerial_ch2* Yp, const aerial_ch2* Wf, const aerial_ch2* OCC,

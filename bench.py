@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--duration", type=float, default=1.0, help="serving run length in seconds (config 5)")
     ap.add_argument("--window-us", type=float, default=0.0, help="serving batching window (config 5; 0 = launch at once)")
     ap.add_argument("--min-batch", type=int, default=0, help="serving minimum batch before the window ends")
+    ap.add_argument("--srs-symbols", type=int, default=4, choices=[1, 2, 4],
+                    help="SRS symbols averaged by each serving SRS update (config 5)")
     ap.add_argument("--soak", type=float, default=1.5, help="seconds of untimed load before timing (clock steady state)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -478,12 +480,12 @@ def run_serving(a, aeq, wl, dev):
     """Configuration 5: 40 cells submit slots as Poisson arrivals (mean one
     slot per 500 us per cell) to the serving loop; every 20th slot of a cell
     is preceded by an SRS channel update (filter multiply, K = 12, one port per
-    layer).  The same arrival trace is served by the fused batched loop and by
-    the plain FP32 chain run request by request."""
+    layer, averaged over 4 SRS symbols).  The same arrival trace is served by
+    the fused batched loop and by the plain FP32 chain run request by request."""
     import numpy as np
     import torch
 
-    n_cells, per_slot_s, srs_every = 40, 500e-6, 20
+    n_cells, per_slot_s, srs_every, srs_syms = 40, 500e-6, 20, a.srs_symbols
     shapes = wl.multicell_shapes(n_cells, seed=5)
     cells, Ys, rings, srs_ops = [], [], [], []
     for i, (p, A, L, q, snr) in enumerate(shapes):
@@ -496,7 +498,7 @@ def run_serving(a, aeq, wl, dev):
         g.manual_seed(9000 + i)
         nblk = c.nSC // 12
         srs_ops.append([(torch.randn(n, generator=g, device=dev) * 0.5).half().view(torch.int16).contiguous()
-                        for n in (2 * nblk * A * 12, 2 * 12 * 12, 2 * L * 12)])
+                        for n in (2 * srs_syms * nblk * A * 12, 2 * 12 * 12, 2 * L * 12)])
     rng = np.random.default_rng(11)
     arrivals = []
     for ci in range(n_cells):
@@ -540,8 +542,8 @@ def run_serving(a, aeq, wl, dev):
             k = count[ci]
             count[ci] += 1
             if k and k % srs_every == 0:
-                errors += lib.aerial_server_srs_update(handle, ids[ci], sp[ci][0], sp[ci][1], sp[ci][2], 12, 12,
-                                                       None) != 0
+                errors += lib.aerial_server_srs_update_n(handle, ids[ci], sp[ci][0], srs_syms, sp[ci][1], sp[ci][2],
+                                                         12, 12, None) != 0
             errors += lib.aerial_server_submit(handle, ids[ci], yp[ci][k % 2], rp[ci][k % 16], target, None) != 0
         srv.drain(600000)
         st = srv.stats()
@@ -561,8 +563,9 @@ def run_serving(a, aeq, wl, dev):
         "metric": "serving: equalized REs/s with p99 slot latency (deadline 500 us)", "value": fused["res_per_s"],
         "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "benchmark_config": 5,
         "config": {"workload": (f"{n_cells} cells, Poisson slot arrivals (mean one per 500 us per cell) for "
-                                f"{a.duration:.1f} s, shapes drawn as the 16-cell batch, SRS update every "
-                                f"{srs_every} slots, 16 GB admission budget, 3 streams, up to 64 slots a launch"),
+                                f"{a.duration:.1f} s, shapes drawn as the 16-cell batch, SRS update (filter multiply "
+                                f"averaged over {srs_syms} SRS symbols) every {srs_every} slots, 16 GB admission "
+                                f"budget, 3 streams, up to 64 slots a launch"),
                    "slots_offered": len(arrivals), "precision": a.precision},
         "fused_batched": dict({k: fused[k] for k in keep}, batch_window_us=a.window_us, min_batch=a.min_batch),
         "plain_fp32_per_request": {k: plain[k] for k in keep},

@@ -150,6 +150,18 @@ int aerial_srs_to_channel(aerial_cf32* H, const aerial_ch2* SRS, const aerial_ch
                           const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts,
                           int foccLen, void* stream);
 
+/* aerial_srs_to_channel over nSrsSym (1, 2 or 4) SRS symbols, averaged:
+ *   H = (1 / nSrsSym) sum_s srs_to_channel(SRS_s),
+ * with SRS holding the symbols one after another ([sym][blk][ant][K]).  The
+ * average is one FP32 sum: the tcgen05 kernel's K loop runs over every
+ * symbol with the taps scaled by 1/nSrsSym (exact for these counts).
+ * nSrsSym > 1 needs the tcgen05 path (K a multiple of 4, SRS 16-byte
+ * aligned, and K <= 32 for 4 symbols, whose operand stages must fit in
+ * shared memory); other shapes return AERIAL_ERR_UNSUPPORTED. */
+int aerial_srs_to_channel_avg(aerial_cf32* H, const aerial_ch2* SRS, int nSrsSym, const aerial_ch2* W,
+                              const aerial_ch2* FOCC, int nAnt, int nBlocks, int K, int nPorts,
+                              int foccLen, void* stream);
+
 /* Frequency-interpolation filter of DMRS channel estimation, straight into
  * the PUSCH channel layout (complex64):
  *   H[blk*nOut + o][ant][p] = sum_k Wf[o][k] * OCC[p][k % occLen] * Yp[blk][ant][k]
@@ -354,6 +366,11 @@ int aerial_server_set_channel(aerial_server* server, int cellId, const aerial_cf
  * port per layer, K subcarriers per block); slots queued after it see it. */
 int aerial_server_srs_update(aerial_server* server, int cellId, const aerial_ch2* SRS, const aerial_ch2* W,
                              const aerial_ch2* FOCC, int K, int foccLen, uint64_t* requestId);
+/* The same over nSrsSym (1, 2 or 4) SRS symbols whose estimates are averaged
+ * (aerial_srs_to_channel_avg); aerial_server_srs_update is nSrsSym = 1. */
+int aerial_server_srs_update_n(aerial_server* server, int cellId, const aerial_ch2* SRS, int nSrsSym,
+                               const aerial_ch2* W, const aerial_ch2* FOCC, int K, int foccLen,
+                               uint64_t* requestId);
 /* Queue one slot: Y_rx [nSC][nSym][nAnt] in, LLRs out (device memory).
  * arrival_ns: steady-clock arrival time in ns (0 = now). */
 int aerial_server_submit(aerial_server* server, int cellId, const aerial_cf32* Y_rx, float* llr,

@@ -60,6 +60,9 @@ def test_invalid_arguments_rejected_before_any_launch():
     assert lib.aerial_chest_interp(None, fake, fake, fake, 64, 34, 96, 96, 4, 4, None) == 1001
     assert lib.aerial_chest_interp_h(fake, fake, fake, fake, 64, 34, 97, 96, 4, 4, None) == 1001
     assert lib.aerial_chest_interp_h(None, fake, fake, fake, 64, 34, 96, 96, 4, 4, None) == 1001
+    assert lib.aerial_srs_to_channel_avg(fake, fake, 3, fake, fake, 64, 66, 12, 4, 4, None) == 1001
+    assert lib.aerial_srs_to_channel_avg(None, fake, 4, fake, fake, 64, 66, 12, 4, 4, None) == 1001
+    assert lib.aerial_server_srs_update_n(None, 0, fake, 4, fake, fake, 12, 4, None) == 1001
     assert lib.aerial_kernel_timeouts(None) == 1001
     cells = (pkg.CellDesc * 1)()
     assert lib.aerial_pusch_eq_fused(cells, 1, None, None) == 1001     # null buffers

@@ -136,6 +136,33 @@ def test_server_srs_update_rewrites_resident_channel(aeq, orc, wl, cuda):
     np.testing.assert_array_equal(after.cpu().numpy(), _alone(aeq, c, Hsrs, Y, cuda))
 
 
+def test_server_srs_update_averages_four_symbols(aeq, orc, wl, cuda):
+    """An SRS update over 4 SRS symbols (the serving configuration's) leaves the
+    resident channel equal to srs_to_channel_avg of those symbols: the slot
+    queued after it equalizes bit for bit like a launch on that channel."""
+    K, F, S = 12, 4, 4
+    c = wl.make_cell(4, 64, 4, 11, 64, 25.0, seed=133)
+    nBlk = c.nSC // K
+    syms = [orc.ref_srs_inputs(70 + q, nBlk * c.nAnt * K, K * K, c.nLayers * F) for q in range(S)]
+    dS = torch.from_numpy(np.concatenate([x[0] for x in syms]).view(np.int16)).to(cuda)
+    dW = torch.from_numpy(syms[0][1].view(np.int16)).to(cuda)
+    dF = torch.from_numpy(syms[0][2].view(np.int16)).to(cuda)
+    Havg = torch.empty(c.nSC, c.nAnt, c.nLayers, dtype=torch.complex64, device=cuda)
+    aeq.srs_to_channel_avg(Havg, dS, S, dW, dF, c.nAnt, nBlk, K, c.nLayers, F)
+    Y = c.Y.to(cuda)
+    with aeq.Server(streams=2) as srv:
+        k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
+        srv.set_channel(k, c.H.to(cuda), c.sigma2)
+        after = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+        srv.srs_update(k, dS, dW, dF, K, F, n_symbols=S)
+        srv.submit(k, Y, after)
+        srv.drain()
+        assert srv.stats()["srs_updates"] == 1
+        with pytest.raises(aeq.AerialError):
+            srv.srs_update(k, dS, dW, dF, K, F, n_symbols=3)
+    np.testing.assert_array_equal(after.cpu().numpy(), _alone(aeq, c, Havg, Y, cuda))
+
+
 def test_server_deadline_misses_counted_for_late_producer(aeq, wl, cuda):
     """Fault injected on the host: a producer that hands slots over late (arrival stamped 200 ms before the
     submit, on the same steady clock) makes every such slot miss a 20 ms deadline, and the statistics count

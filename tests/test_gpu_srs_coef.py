@@ -83,6 +83,48 @@ def test_srs_to_channel_layout(aeq, orc, cuda, K, P, F):
     assert evm_db(H.cpu().numpy(), ref) < -120
 
 
+@pytest.mark.parametrize("K,P,F,S,nBlk,nAnt", [(12, 4, 4, 4, 9, 48), (12, 8, 2, 4, 6, 64), (24, 4, 8, 2, 9, 48),
+                                                (24, 2, 8, 4, 5, 64), (48, 4, 8, 2, 4, 64), (12, 2, 4, 1, 9, 48)])
+def test_srs_to_channel_avg_vs_fp64(aeq, orc, cuda, K, P, F, S, nBlk, nAnt):
+    """The channel averaged over S SRS symbols against the FP64 average of the
+    per-symbol estimates.  S = 1 is srs_to_channel, bit for bit."""
+    syms = [orc.ref_srs_inputs(50 + q, nBlk * nAnt * K, K * K, P * F) for q in range(S)]
+    w, f = syms[0][1], syms[0][2]
+    SRS = _d(np.concatenate([x[0] for x in syms]).view(np.int16), cuda)
+    Wd, Fd = _d(w.view(np.int16), cuda), _d(f.view(np.int16), cuda)
+    H = torch.full((nBlk * K, nAnt, P), float("nan"), dtype=torch.complex64, device=cuda)
+    aeq.srs_to_channel_avg(H, SRS, S, Wd, Fd, nAnt, nBlk, K, P, F)
+    torch.cuda.synchronize()
+    ref = np.mean([orc.srs_f64(x[0], w, f, nAnt, nBlk, K, P, F) for x in syms], axis=0)
+    ref = ref.reshape(nBlk, nAnt, K, P).transpose(0, 2, 1, 3).reshape(nBlk * K, nAnt, P)
+    assert evm_db(H.cpu().numpy(), ref) < -120
+    if S == 1:
+        H1 = torch.empty_like(H)
+        aeq.srs_to_channel(H1, SRS, Wd, Fd, nAnt, nBlk, K, P, F)
+        torch.cuda.synchronize()
+        assert torch.equal(H, H1)
+
+
+def test_srs_to_channel_avg_envelope(aeq, orc, cuda):
+    """Symbol counts other than 1, 2, 4 are invalid; shapes the tcgen05
+    kernel cannot average (taps not a multiple of 4, or 4 symbols of more than
+    32 taps) are unsupported, with nothing launched."""
+    K, P, F, nBlk, nAnt = 10, 2, 5, 4, 32
+    s, w, f = orc.ref_srs_inputs(60, 4 * nBlk * nAnt * 48, 48 * 48, 4 * 8)
+    SRS, Wd, Fd = (_d(x.view(np.int16), cuda) for x in (s, w, f))
+    H = torch.empty(nBlk * 48, nAnt, 4, dtype=torch.complex64, device=cuda)
+    for S in (0, 3, 8):
+        with pytest.raises(aeq.AerialError) as e:
+            aeq.srs_to_channel_avg(H, SRS, S, Wd, Fd, nAnt, nBlk, 12, 4, 8)
+        assert e.value.status == 1001
+    with pytest.raises(aeq.AerialError) as e:
+        aeq.srs_to_channel_avg(H, SRS, 2, Wd, Fd, nAnt, nBlk, K, P, F)
+    assert e.value.status == 1002
+    with pytest.raises(aeq.AerialError) as e:
+        aeq.srs_to_channel_avg(H, SRS, 4, Wd, Fd, nAnt, nBlk, 48, 4, 8)
+    assert e.value.status == 1002
+
+
 # DMRS interpolation filter: (nPilot, nOut, ports, OCC length, antennas).  96 pilots x 4 ports over 64
 # antennas is the [64 x 96] x [96 x 4] product of the reference's README.md:200.
 # Pilot counts that are multiples of 4 (up to 96) run the tcgen05 kernel, the others the mma.sync kernel.
