@@ -333,37 +333,101 @@ extern "C" int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, 
 // every GPU that loads this library holds it until the process exits.
 //
 // The array's host-side name is only a stand-in for the device symbol; the
-// device address comes from cudaGetSymbolAddress, done once per device with
-// that device current, on the first call made on it (which must therefore
-// happen before any stream capture).  All calls share the one array and it
-// keeps the last call's contents: every scratch byte a call reads is first
-// written by that same call, so nothing needs clearing, but calls that
-// overlap on the GPU (two streams, two threads) race on it.
+// device address comes from cudaGetSymbolAddress, made with the device
+// current.  The address belongs to the CUDA context that loaded the module:
+// a cudaDeviceReset, or a second context on the same device, gets its own
+// copy of the array.  The address is therefore cached per device together
+// with the unique ID of the context it was looked up in (cuCtxGetId, which a
+// new context never reuses even where its handle value is recycled), and
+// looked up again whenever a call runs in a different context.  The first
+// call in each context does that lookup, so make it before any stream
+// capture.  All calls share the one array and it keeps the last call's
+// contents: every scratch byte a call reads is first written by that same
+// call, so nothing needs clearing, but calls that overlap on the GPU (two
+// streams, two threads) race on it.
 // ---------------------------------------------------------------------------
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <mutex>
 
 static __device__ __align__(256) unsigned char g_plain_static_scratch[AERIAL_STATIC_SCRATCH_BYTES];
 
+// cuCtxGetCurrent / cuCtxGetId from the driver, looked up once.
+struct CtxQuery {
+    PFN_cuCtxGetCurrent_v4000 current = nullptr;
+    PFN_cuCtxGetId_v12000 id = nullptr;
+};
+static const CtxQuery& ctx_query() {
+    static std::once_flag once;
+    static CtxQuery q;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult r;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r) == cudaSuccess &&
+            r == cudaDriverEntryPointSuccess)
+            q.current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &r) == cudaSuccess &&
+            r == cudaDriverEntryPointSuccess)
+            q.id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+    });
+    return q;
+}
+
+// Unique ID of the calling thread's current context, 0 if there is none yet
+// or the driver cannot say.
+static unsigned long long current_ctx_id() {
+    const CtxQuery& q = ctx_query();
+    if (!q.current || !q.id) return 0;
+    CUcontext ctx = nullptr;
+    if (q.current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    unsigned long long id = 0;
+    return q.id(ctx, &id) == CUDA_SUCCESS ? id : 0;
+}
+
 static int static_scratch_address(void** out) {
     static std::mutex mu;
     static void* addr[64] = {};
+    static unsigned long long ctxOf[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return rt_status(e);
     if (dev < 0 || dev >= 64) return AERIAL_ERR_NO_DEVICE;
     std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_plain_static_scratch);
-        if (e != cudaSuccess) return rt_status(e);
-        addr[dev] = p;
+    const unsigned long long ctx = current_ctx_id();
+    if (ctx != 0 && addr[dev] && ctxOf[dev] == ctx) {
+        *out = addr[dev];
+        return AERIAL_OK;
     }
-    *out = addr[dev];
+    // no cached address for this context (or no context yet: the runtime
+    // makes the device's primary context current inside this call)
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_plain_static_scratch);
+    if (e != cudaSuccess) return rt_status(e);
+    addr[dev] = p;
+    ctxOf[dev] = current_ctx_id();    // 0 when unknown: looked up again next call
+    *out = p;
+    return AERIAL_OK;
+}
+
+// The checks aerial_pusch_eq_plain makes per cell, so a malformed cell gets
+// AERIAL_ERR_INVALID_ARG / AERIAL_ERR_UNSUPPORTED before the size comparison
+// (negative shapes would otherwise wrap in the workspace arithmetic).
+static int plain_cell_check(const aerial_cell_desc& c) {
+    if (c.nPRB < 1 || c.nPRB > AERIAL_MAX_PRB) return AERIAL_ERR_INVALID_ARG;
+    if (!c.H || !c.Y_rx || !c.llr || c.nPamBits < 1 || c.nPamBits > 4 ||
+        !shape_ok(c.nPRB * 12, c.nSym, c.nLayers, c.nAnt))
+        return AERIAL_ERR_INVALID_ARG;
+    if (c.format != AERIAL_FMT_CF32) return AERIAL_ERR_UNSUPPORTED;
     return AERIAL_OK;
 }
 
 extern "C" int aerial_pusch_eq_plain_static(const aerial_cell_desc* cells, int nCells, void* stream) {
     if (!cells || nCells < 1) return AERIAL_ERR_INVALID_ARG;
+    for (int i = 0; i < nCells; i++) {
+        const int s = plain_cell_check(cells[i]);
+        if (s != AERIAL_OK) return s;
+    }
     if (aerial_pusch_eq_plain_workspace(cells, nCells) > (size_t)AERIAL_STATIC_SCRATCH_BYTES)
         return AERIAL_ERR_SCRATCH_LIMIT;
     void* scratch = nullptr;
