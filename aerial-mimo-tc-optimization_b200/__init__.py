@@ -25,8 +25,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libaerial_eq.so")
 
 AERIAL_OK = 0
-PREC_FP16, PREC_BF16, PREC_BF16X3, PREC_FP32 = 0, 1, 2, 3
-PREC_NAMES = {"fp16": PREC_FP16, "bf16": PREC_BF16, "bf16x3": PREC_BF16X3, "fp32": PREC_FP32}
+PREC_FP16, PREC_BF16, PREC_BF16X3, PREC_FP32, PREC_FP16X3 = 0, 1, 2, 3, 4
+PREC_NAMES = {"fp16": PREC_FP16, "bf16": PREC_BF16, "bf16x3": PREC_BF16X3, "fp32": PREC_FP32,
+              "fp16x3": PREC_FP16X3}
 FMT_CF32, FMT_CF16 = 0, 1          # cell storage formats (aerial_cell_desc.format)
 MAX_CELLS = 64
 MAX_PRB = 524288            # AERIAL_MAX_PRB: PRBs per cell descriptor
@@ -108,6 +109,11 @@ class ServerStats(ctypes.Structure):
         ("srs_updates", ctypes.c_long),
         ("budget_used_bytes", ctypes.c_int64),
         ("pending", ctypes.c_long),
+        ("submit_lag_p99_us", ctypes.c_float),
+        ("submit_lag_max_us", ctypes.c_float),
+        ("dispatch_gap_max_us", ctypes.c_float),
+        ("launch_call_max_us", ctypes.c_float),
+        ("misses_late_submit", ctypes.c_long),
     ]
 
 
@@ -133,6 +139,7 @@ SIGNATURES = {
     "aerial_srs_to_channel_avg": (_I, [_P, _P, _I, _P, _P, _I, _I, _I, _I, _I, _P]),
     "aerial_chest_interp_h": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
     "aerial_kernel_timeouts": (_I, [ctypes.POINTER(ctypes.c_uint)]),
+    "aerial_fp16_operand_scale": (_F, [_F]),
     "aerial_pusch_eq_fused": (_I, [ctypes.POINTER(CellDesc), _I, ctypes.POINTER(Tuning), _P]),
     "aerial_pusch_eq_plain_workspace": (_Z, [ctypes.POINTER(CellDesc), _I]),
     "aerial_pusch_eq_plain": (_I, [ctypes.POINTER(CellDesc), _I, _P, _Z, _P]),
@@ -180,6 +187,12 @@ def _lib_handle():
 def lib():
     """The loaded ``libaerial_eq.so`` (ctypes handle)."""
     return _lib_handle()
+
+
+def fp16_operand_scale(sigma2: float) -> float:
+    """The power-of-two scale the FP16 path applies to a complex64 cell's H and
+    Y_rx for noise variance sigma2 (1 where raw FP16 operands are safe)."""
+    return float(lib().aerial_fp16_operand_scale(float(sigma2)))
 
 
 def prepare():

@@ -50,7 +50,8 @@ struct FusedCell {
     float* llr;
     float2* yeq;
     long group0;     // first global group index of this cell
-    float sigma2;
+    float sigma2;    // noise variance in the units the kernel sees (times scale^2)
+    float scale;     // power-of-two operand scale (FP16 operands), else 1
     int nSC, A, L, nSym, nPam, LT, vecY, vecH, lgHalfL;
     int GS;          // subcarriers per group = min(32 / LT, kMaxGroupSC)
     int nChunk;      // 16-antenna chunks per subcarrier
@@ -67,6 +68,7 @@ struct FusedParams {
     int nStages;     // operand stages per warp of that kernel
     int exactChunks; // with an exact tile: every cell has nAnt == 16 * exactChunks (2, 4, 8), else 0
     int fmt;         // AERIAL_FMT_* shared by every cell
+    int scaled;      // some cell's FP16 operands are scaled (selects the kernel)
     long totalGroups;
 };
 
@@ -94,11 +96,56 @@ __device__ __forceinline__ void split_bf16(float re, float im, uint32_t& hi, uin
     hi = *reinterpret_cast<uint32_t*>(&h);
     lo = *reinterpret_cast<uint32_t*>(&l);
 }
+// fp16 hi/lo split: x = hi + lo to ~22 significant bits, for operands the
+// host has normalized (set_operand_scale) so that lo stays a normal half.
+__device__ __forceinline__ void split_fp16(float re, float im, uint32_t& hi, uint32_t& lo) {
+    __half2 h = __floats2half2_rn(re, im);
+    float2 hf = __half22float2(h);
+    __half2 l = __floats2half2_rn(re - hf.x, im - hf.y);
+    hi = *reinterpret_cast<uint32_t*>(&h);
+    lo = *reinterpret_cast<uint32_t*>(&l);
+}
+template <int P>
+__device__ __forceinline__ void split2(float re, float im, uint32_t& hi, uint32_t& lo) {
+    if constexpr (P == AERIAL_PREC_FP16X3)
+        split_fp16(re, im, hi, lo);
+    else
+        split_bf16(re, im, hi, lo);
+}
+
+// Packed FP32 pairs (fma.rn.f32x2 and friends, two IEEE operations per
+// instruction on sm_100a).
+__device__ __forceinline__ unsigned long long pk2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+// Two complex samples times the (exact, power-of-two) operand scale ss = (s, s).
+__device__ __forceinline__ float4 scale4(float4 v, unsigned long long ss) {
+    const float2 a = upk2(mul2(pk2(v.x, v.y), ss));
+    const float2 b = upk2(mul2(pk2(v.z, v.w), ss));
+    return make_float4(a.x, a.y, b.x, b.y);
+}
 
 template <int P>
 __device__ __forceinline__ void mma16816(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
                                          uint32_t b1) {
-    if constexpr (P == AERIAL_PREC_FP16) {
+    if constexpr (P == AERIAL_PREC_FP16 || P == AERIAL_PREC_FP16X3) {
         asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
             "{%0,%1,%2,%3};\n"
             : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
@@ -219,9 +266,14 @@ __device__ __forceinline__ float4 lds128(uint32_t a) {
 // yo[kk][nt]: the lane's received-row fragment offsets in a stage (row
 // 8 nt + g, clamped to row 0 past nSym, antenna pair 8 kk + 2 c, swizzled),
 // fixed per cell.
-template <int LT, int P, bool LEXACT, bool FULL>
+// SC: FP16 operands of a cell whose noise level lies outside the range where
+// raw FP16 is safe are multiplied by the cell's power-of-two scale ss = (s, s)
+// before they are rounded (exact; the cell's sigma2 carries s^2, so G^-1 Z,
+// mu and the LLRs are unchanged).
+template <int LT, int P, bool LEXACT, bool FULL, bool SC = false>
 __device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L, const uint32_t (&yo)[2][2],
-                                          float (*gacc)[4], float (*zacc)[2][4], bool z2, int g, int c) {
+                                          float (*gacc)[4], float (*zacc)[2][4], bool z2, int g, int c,
+                                          unsigned long long ss = 0) {
     constexpr int NMT = LT > 8 ? 2 : 1;
 #pragma unroll
     for (int kk = 0; kk < 2; kk++) {
@@ -245,18 +297,24 @@ __device__ __forceinline__ void mma_stage(uint32_t st, int hrs, int nRows, int L
             const float4 y = lds128(st + yo[kk][nt]);
             yv[nt] = FULL ? y : make_float4(v0 ? y.x : 0.f, v0 ? y.y : 0.f, v1 ? y.z : 0.f, v1 ? y.w : 0.f);
         }
-        if constexpr (P == AERIAL_PREC_BF16X3) {
+        if constexpr (SC) {
+#pragma unroll
+            for (int mt = 0; mt < NMT; mt++) hv[mt] = scale4(hv[mt], ss);
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) yv[nt] = scale4(yv[nt], ss);
+        }
+        if constexpr (P == AERIAL_PREC_BF16X3 || P == AERIAL_PREC_FP16X3) {
             uint32_t ah[NMT][2], al[NMT][2];
 #pragma unroll
             for (int mt = 0; mt < NMT; mt++) {
-                split_bf16(hv[mt].x, hv[mt].y, ah[mt][0], al[mt][0]);
-                split_bf16(hv[mt].z, hv[mt].w, ah[mt][1], al[mt][1]);
+                split2<P>(hv[mt].x, hv[mt].y, ah[mt][0], al[mt][0]);
+                split2<P>(hv[mt].z, hv[mt].w, ah[mt][1], al[mt][1]);
             }
             uint32_t yh[2][2], yl[2][2];
 #pragma unroll
             for (int nt = 0; nt < 2; nt++) {
-                split_bf16(yv[nt].x, yv[nt].y, yh[nt][0], yl[nt][0]);
-                split_bf16(yv[nt].z, yv[nt].w, yh[nt][1], yl[nt][1]);
+                split2<P>(yv[nt].x, yv[nt].y, yh[nt][0], yl[nt][0]);
+                split2<P>(yv[nt].z, yv[nt].w, yh[nt][1], yl[nt][1]);
             }
 #pragma unroll
             for (int mt = 0; mt < NMT; mt++) {
@@ -420,30 +478,6 @@ __device__ __forceinline__ void emit1(char* lp, char* ye, float2 x, float invMu,
         write_llr<N>(reinterpret_cast<float*>(lp), o);
 }
 
-// X[i][s] = sum_m Ginv[i][m] Z[m][s] for symbol pairs (FP32 fma chains), then
-// unbias and demap; lp / ye walk the row's LLRs and equalized symbols.
-// Packed FP32 pairs (fma.rn.f32x2 and friends, two IEEE operations per
-// instruction on sm_100a).
-__device__ __forceinline__ unsigned long long pk2(float lo, float hi) {
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ float2 upk2(unsigned long long v) {
-    float2 r;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
-    return r;
-}
-__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
-    unsigned long long d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
 __device__ __forceinline__ void lds2x64(uint32_t a, unsigned long long& v0, unsigned long long& v1) {
     asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];\n" : "=l"(v0), "=l"(v1) : "r"(a));
 }
@@ -790,7 +824,8 @@ __device__ __forceinline__ int group_valid(const FusedCell& cl, long grp) {
 // LTF = 0: any mix of cells.  LTF in {2, 4, 8, 16}: every cell has
 // nLayers == LTF and 16-byte aligned H / Y_rx (the host checks), so the layer
 // tile, strides and masks are compile-time constants.
-template <int P, int LTF>
+// SC: the launch has cells whose FP16 operands are scaled (mma_stage).
+template <int P, int LTF, bool SC = false>
 __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant__ FusedParams p) {
     extern __shared__ float4 smem_raw[];
     const int lane = threadIdx.x & 31;
@@ -904,8 +939,10 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     bool cExact = false;                                  // generic kernel: L fills the tile, aligned rows
     bool z2;
     uint32_t yo[2][2];
+    unsigned long long ss = 0;                            // (scale, scale) of the cell's operands
     auto load_ccell = [&]() {
         const FusedCell& cl = p.cell[ci];
+        if constexpr (SC) ss = pk2(cl.scale, cl.scale);
         nValid = group_valid(cl, grp);
         cA = cl.A;
         cNChunk = cl.nChunk;
@@ -947,24 +984,25 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
         cslot = cslot == NST - 1 ? 0 : cslot + 1;
         if constexpr (LTF != 0) {
             if (ch < cNFull)
-                mma_stage<LTF, P, true, true>(st, hrs_of(LTF), CHUNK, LTF, yo, gacc, zacc, z2, g, c);
+                mma_stage<LTF, P, true, true, SC>(st, hrs_of(LTF), CHUNK, LTF, yo, gacc, zacc, z2, g, c, ss);
             else
-                mma_stage<LTF, P, true, false>(st, hrs_of(LTF), cA - CHUNK * ch, LTF, yo, gacc, zacc, z2, g, c);
+                mma_stage<LTF, P, true, false, SC>(st, hrs_of(LTF), cA - CHUNK * ch, LTF, yo, gacc, zacc, z2, g, c,
+                                                   ss);
         } else {
             const int nRows = min(CHUNK, cA - CHUNK * ch);
             if (cExact && nRows == CHUNK) {
                 switch (cLT) {
-                    case 2: mma_stage<2, P, true, true>(st, cHrs, CHUNK, 2, yo, gacc, zacc, z2, g, c); break;
-                    case 4: mma_stage<4, P, true, true>(st, cHrs, CHUNK, 4, yo, gacc, zacc, z2, g, c); break;
-                    case 8: mma_stage<8, P, true, true>(st, cHrs, CHUNK, 8, yo, gacc, zacc, z2, g, c); break;
-                    default: mma_stage<16, P, true, true>(st, cHrs, CHUNK, 16, yo, gacc, zacc, z2, g, c); break;
+                    case 2: mma_stage<2, P, true, true, SC>(st, cHrs, CHUNK, 2, yo, gacc, zacc, z2, g, c, ss); break;
+                    case 4: mma_stage<4, P, true, true, SC>(st, cHrs, CHUNK, 4, yo, gacc, zacc, z2, g, c, ss); break;
+                    case 8: mma_stage<8, P, true, true, SC>(st, cHrs, CHUNK, 8, yo, gacc, zacc, z2, g, c, ss); break;
+                    default: mma_stage<16, P, true, true, SC>(st, cHrs, CHUNK, 16, yo, gacc, zacc, z2, g, c, ss); break;
                 }
             } else switch (cLT) {
-                case 1: mma_stage<1, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
-                case 2: mma_stage<2, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
-                case 4: mma_stage<4, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
-                case 8: mma_stage<8, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
-                default: mma_stage<16, P, false, false>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c); break;
+                case 1: mma_stage<1, P, false, false, SC>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c, ss); break;
+                case 2: mma_stage<2, P, false, false, SC>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c, ss); break;
+                case 4: mma_stage<4, P, false, false, SC>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c, ss); break;
+                case 8: mma_stage<8, P, false, false, SC>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c, ss); break;
+                default: mma_stage<16, P, false, false, SC>(st, cHrs, nRows, cL, yo, gacc, zacc, z2, g, c, ss); break;
             }
         }
         if (++ch < cNChunk) continue;
@@ -1054,7 +1092,7 @@ __device__ __forceinline__ void stage_chunk(uint32_t st, uint32_t hLaneS, uint32
         if (k < s.yk) cp_async16(st + yLaneS + 512 * k, s.y + CHUNK * j + 4 * k * A);
 }
 
-template <int P, int LTF, int NCH>
+template <int P, int LTF, int NCH, bool SC = false>
 __global__ void __launch_bounds__(256, 2) fused_eq_kernel_a(const __grid_constant__ FusedParams p) {
     constexpr int NST = stages_of_a(LTF, NCH);
     constexpr int A = CHUNK * NCH;
@@ -1097,8 +1135,10 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_a(const __grid_constan
     int nValid, nSym;
     bool z2;
     uint32_t yo[2][2];
+    unsigned long long ss = 0;                           // (scale, scale) of the cell's operands
     auto load_cell = [&]() {
         const FusedCell& cl = p.cell[ci];
+        if constexpr (SC) ss = pk2(cl.scale, cl.scale);
         nValid = group_valid(cl, grp);
         nSym = cl.nSym;
         z2 = nSym > 8;
@@ -1162,8 +1202,8 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_a(const __grid_constan
             pslot = pslot == NST - 1 ? 0 : pslot + 1;
             cp_async_wait<NST - 1>();                  // this chunk's copies (own lane) have landed
             __syncwarp();                              // ... and every lane's
-            mma_stage<LTF, P, true, true>(stBase + cslot * p.stageBytes, HRS, CHUNK, LTF, yo, gacc, zacc, z2, g,
-                                          c);
+            mma_stage<LTF, P, true, true, SC>(stBase + cslot * p.stageBytes, HRS, CHUNK, LTF, yo, gacc, zacc, z2, g,
+                                              c, ss);
             cslot = cslot == NST - 1 ? 0 : cslot + 1;
         }
         store_acc<LTF>(sm, gacc, zacc, q, g, c);
@@ -1409,6 +1449,30 @@ static int exact_tile(const FusedParams& p) {
     return lt;
 }
 
+}  // namespace aeq
+
+// Power-of-two scale for a cell's FP16 operands, from its noise variance.
+// FP16 keeps 11 significant bits only between 2^-14 and 65504, so H and Y_rx
+// are rounded raw only while sigma2 lies in [2^-16, 2^7) (noise standard
+// deviation 2^-8 ... 11.3: received samples up to about 75 dB above the
+// noise stay below 65504, and channel taps 20 dB under it stay normal).
+// Outside that window the operands are multiplied by s = 2^k with
+// s^2 sigma2 in [2^-10, 2^-8) before rounding, and sigma2 by s^2: G, Z and
+// G^-1 then scale by exact powers of two, which X = G^-1 Z, mu and the LLRs
+// do not see.  sigma2 = 0 (zero forcing) or non-finite takes no scale.
+extern "C" float aerial_fp16_operand_scale(float sigma2) {
+    if (!(sigma2 > 0.f) || !(sigma2 < INFINITY)) return 1.f;
+    int e = 0;
+    (void)frexpf(sigma2, &e);             // sigma2 in [2^(e-1), 2^e)
+    const int E = e - 1;
+    if (E >= -16 && E <= 6) return 1.f;
+    int k = (-10 - E) >= 0 ? (-10 - E + 1) / 2 : -((E + 10) / 2);   // ceil((-10 - E) / 2)
+    k = k > 60 ? 60 : (k < -60 ? -60 : k);
+    return ldexpf(1.f, k);
+}
+
+namespace aeq {
+
 // warpBytes: the per-warp shared memory of the launch (epilogue region of the
 // largest layer-tile footprint present, which is not monotonic in the tile,
 // plus the kernel's operand stages).
@@ -1432,6 +1496,7 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
         f.llr = c.llr;
         f.yeq = (float2*)c.Y_eq;
         f.sigma2 = c.sigma2;
+        f.scale = 1.f;                  // set_operand_scale decides, once the precision is known
         f.nSC = nSC;
         f.A = c.nAnt;
         f.L = c.nLayers;
@@ -1454,6 +1519,7 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
         g0 += (nSC + f.GS - 1) / f.GS;
     }
     p.nCells = nCells;
+    p.scaled = 0;
     p.totalGroups = g0;
     p.fmt = cells[0].format;
     for (int i = 0; i < nCells; i++)
@@ -1492,6 +1558,44 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
     p.nStages = p.exactChunks ? stages_of_a(p.exactTile, p.exactChunks) : stages_of(p.exactTile);
     warpBytes = p.epiBytes + p.nStages * p.stageBytes;
     return AERIAL_OK;
+}
+
+// FP16 operands from complex64 cells: each cell's power-of-two scale
+// (aerial_fp16_operand_scale) and its sigma2 in the scaled units; p.scaled
+// selects the kernels that apply it.  Other precisions keep the FP32 range
+// and complex-half cells are read as stored: no scale.  Call once per
+// parameter block, after build_fused_params.
+//
+// FP16X3 operands are always normalized, to s^2 sigma2 in [1/4, 1): the low
+// half of each split then stays a normal half (22 significant bits in all)
+// for channel taps down to about 40 dB under the noise, and received samples
+// up to about 90 dB above it stay below 65504.  Its kernels always apply the
+// scale (a cell with s = 1 multiplies by one).
+static float fp16x3_operand_scale(float sigma2) {
+    if (!(sigma2 > 0.f) || !(sigma2 < INFINITY)) return 1.f;
+    int e = 0;
+    (void)frexpf(sigma2, &e);             // sigma2 in [2^(e-1), 2^e)
+    const int E = e - 1;
+    int k = (-2 - E) >= 0 ? (-2 - E + 1) / 2 : -((E + 2) / 2);      // ceil((-2 - E) / 2)
+    k = k > 60 ? 60 : (k < -60 ? -60 : k);
+    return ldexpf(1.f, k);
+}
+
+void set_operand_scale(FusedParams& p, int prec) {
+    p.scaled = prec == AERIAL_PREC_FP16X3 ? 1 : 0;
+    for (int i = 0; i < p.nCells; i++) {
+        FusedCell& f = p.cell[i];
+        f.scale = 1.f;
+        if (p.fmt != AERIAL_FMT_CF32) continue;
+        float s = 1.f;
+        if (prec == AERIAL_PREC_FP16) s = aerial_fp16_operand_scale(f.sigma2);
+        else if (prec == AERIAL_PREC_FP16X3) s = fp16x3_operand_scale(f.sigma2);
+        if (s != 1.f) {
+            f.scale = s;
+            f.sigma2 = f.sigma2 * s * s;      // exact: s is a power of two
+            p.scaled = 1;
+        }
+    }
 }
 
 struct LaunchShape {
@@ -1544,28 +1648,28 @@ static void fill_plan(const void* func, const FusedParams& p, int warpBytes, Lau
     out.smem = sh.warps * warpBytes;
 }
 
-template <int P, int LTF>
+template <int P, int LTF, bool SC>
 static int plan_v(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
-    const int s = allow_max_smem<fused_eq_kernel<P, LTF>>();
+    const int s = allow_max_smem<fused_eq_kernel<P, LTF, SC>>();
     if (s) return s;
-    fill_plan(reinterpret_cast<const void*>(fused_eq_kernel<P, LTF>), p, warpBytes, sh, out);
+    fill_plan(reinterpret_cast<const void*>(fused_eq_kernel<P, LTF, SC>), p, warpBytes, sh, out);
     return AERIAL_OK;
 }
 
-template <int P, int LTF, int NCH>
+template <int P, int LTF, int NCH, bool SC>
 static int plan_a(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
-    const int s = allow_max_smem<fused_eq_kernel_a<P, LTF, NCH>>();
+    const int s = allow_max_smem<fused_eq_kernel_a<P, LTF, NCH, SC>>();
     if (s) return s;
-    fill_plan(reinterpret_cast<const void*>(fused_eq_kernel_a<P, LTF, NCH>), p, warpBytes, sh, out);
+    fill_plan(reinterpret_cast<const void*>(fused_eq_kernel_a<P, LTF, NCH, SC>), p, warpBytes, sh, out);
     return AERIAL_OK;
 }
 
-template <int P, int LTF>
+template <int P, int LTF, bool SC>
 static int plan_an(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
     switch (p.exactChunks) {
-        case 2: return plan_a<P, LTF, 2>(p, warpBytes, sh, out);
-        case 4: return plan_a<P, LTF, 4>(p, warpBytes, sh, out);
-        default: return plan_a<P, LTF, 8>(p, warpBytes, sh, out);
+        case 2: return plan_a<P, LTF, 2, SC>(p, warpBytes, sh, out);
+        case 4: return plan_a<P, LTF, 4, SC>(p, warpBytes, sh, out);
+        default: return plan_a<P, LTF, 8, SC>(p, warpBytes, sh, out);
     }
 }
 
@@ -1586,7 +1690,7 @@ static int plan_hn(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPl
     }
 }
 
-template <int P>
+template <int P, bool SC>
 static int plan_p(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
     if (p.fmt == AERIAL_FMT_CF16) {
         if (P != AERIAL_PREC_FP16) return AERIAL_ERR_UNSUPPORTED;
@@ -1596,18 +1700,18 @@ static int plan_p(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPla
     }
     if (p.exactChunks) {
         switch (p.exactTile) {
-            case 2: return plan_an<P, 2>(p, warpBytes, sh, out);
-            case 4: return plan_an<P, 4>(p, warpBytes, sh, out);
-            case 8: return plan_an<P, 8>(p, warpBytes, sh, out);
-            default: return plan_an<P, 16>(p, warpBytes, sh, out);
+            case 2: return plan_an<P, 2, SC>(p, warpBytes, sh, out);
+            case 4: return plan_an<P, 4, SC>(p, warpBytes, sh, out);
+            case 8: return plan_an<P, 8, SC>(p, warpBytes, sh, out);
+            default: return plan_an<P, 16, SC>(p, warpBytes, sh, out);
         }
     }
     switch (p.exactTile) {
-        case 2: return plan_v<P, 2>(p, warpBytes, sh, out);
-        case 4: return plan_v<P, 4>(p, warpBytes, sh, out);
-        case 8: return plan_v<P, 8>(p, warpBytes, sh, out);
-        case 16: return plan_v<P, 16>(p, warpBytes, sh, out);
-        default: return plan_v<P, 0>(p, warpBytes, sh, out);
+        case 2: return plan_v<P, 2, SC>(p, warpBytes, sh, out);
+        case 4: return plan_v<P, 4, SC>(p, warpBytes, sh, out);
+        case 8: return plan_v<P, 8, SC>(p, warpBytes, sh, out);
+        case 16: return plan_v<P, 16, SC>(p, warpBytes, sh, out);
+        default: return plan_v<P, 0, SC>(p, warpBytes, sh, out);
     }
 }
 
@@ -1616,9 +1720,12 @@ int plan_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, La
     if ((long)sh.warps * warpBytes * sh.ctasPerSm > 227 * 1024 || (long)sh.warps * warpBytes > 227 * 1024)
         return AERIAL_ERR_UNSUPPORTED;
     switch (prec) {
-        case AERIAL_PREC_FP16: return plan_p<AERIAL_PREC_FP16>(p, warpBytes, sh, out);
-        case AERIAL_PREC_BF16: return plan_p<AERIAL_PREC_BF16>(p, warpBytes, sh, out);
-        case AERIAL_PREC_BF16X3: return plan_p<AERIAL_PREC_BF16X3>(p, warpBytes, sh, out);
+        case AERIAL_PREC_FP16:
+            return p.scaled ? plan_p<AERIAL_PREC_FP16, true>(p, warpBytes, sh, out)
+                            : plan_p<AERIAL_PREC_FP16, false>(p, warpBytes, sh, out);
+        case AERIAL_PREC_BF16: return plan_p<AERIAL_PREC_BF16, false>(p, warpBytes, sh, out);
+        case AERIAL_PREC_BF16X3: return plan_p<AERIAL_PREC_BF16X3, false>(p, warpBytes, sh, out);
+        case AERIAL_PREC_FP16X3: return plan_p<AERIAL_PREC_FP16X3, true>(p, warpBytes, sh, out);
         default: return AERIAL_ERR_UNSUPPORTED;
     }
 }
@@ -1663,6 +1770,7 @@ extern "C" int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, 
     LaunchShape sh;
     int prec;
     resolve_tuning(tuning, warpBytes, prec, sh);
+    set_operand_scale(p, prec);
     return launch_fused(p, warpBytes, prec, sh, to_stream(stream));
 }
 
@@ -1681,6 +1789,7 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
     if (s) return s;
     cudaStream_t st = to_stream(stream);
     const int prec = best->precision;
+    set_operand_scale(p, prec);
     LaunchShape cand[16];
     int nc = 0;
     for (int w : {2, 3, 4, 6, 8}) {
@@ -1758,6 +1867,8 @@ struct aerial_eq_graph {
     cudaGraphNode_t node = nullptr;
     FusedParams params;
     LaunchPlan plan;
+    int prec = AERIAL_PREC_FP16;
+    LaunchShape shape{};
 };
 
 static cudaKernelNodeParams node_params(aerial_eq_graph* g, void** args) {
@@ -1779,10 +1890,9 @@ extern "C" int aerial_eq_graph_create(const aerial_cell_desc* cells, int nCells,
     int warpBytes = 0;
     int s = build_fused_params(cells, nCells, g->params, warpBytes);
     if (!s) {
-        LaunchShape sh;
-        int prec;
-        resolve_tuning(tuning, warpBytes, prec, sh);
-        s = plan_fused(g->params, warpBytes, prec, sh, g->plan);
+        resolve_tuning(tuning, warpBytes, g->prec, g->shape);
+        set_operand_scale(g->params, g->prec);
+        s = plan_fused(g->params, warpBytes, g->prec, g->shape, g->plan);
     }
     cudaError_t e = cudaSuccess;
     if (!s) e = cudaGraphCreate(&g->graph, 0);
@@ -1815,7 +1925,15 @@ extern "C" int aerial_eq_graph_update(aerial_eq_graph* g, const aerial_cell_desc
             a.vecH != b.vecH || a.vecY != b.vecY || np.fmt != g->params.fmt)
             return AERIAL_ERR_UNSUPPORTED;      // a new shape or format needs a new graph
     }
+    // The new noise levels may move a cell in or out of FP16 operand scaling,
+    // which selects another kernel instantiation: re-plan the node (an
+    // executable graph's kernel node may change its function).
+    set_operand_scale(np, g->prec);
+    LaunchPlan pl;
+    s = plan_fused(np, warpBytes, g->prec, g->shape, pl);
+    if (s) return s;
     g->params = np;
+    g->plan = pl;
     void* args[] = {&g->params};
     cudaKernelNodeParams kp = node_params(g, args);
     cudaError_t e = cudaGraphExecKernelNodeSetParams(g->exec, g->node, &kp);
@@ -1844,25 +1962,25 @@ namespace aeq {
 // shared-memory limit, so the first launch of a variant inside a latency-
 // critical loop does not pay module loading.
 // ---------------------------------------------------------------------------
-template <int P, int LTF>
+template <int P, int LTF, bool SC>
 static int prepare_v() {
     cudaFuncAttributes at;
-    const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel<P, LTF>);
-    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel<P, LTF>>() : rt_status(e);
+    const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel<P, LTF, SC>);
+    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel<P, LTF, SC>>() : rt_status(e);
 }
 
-template <int P, int LTF, int NCH>
+template <int P, int LTF, int NCH, bool SC>
 static int prepare_a() {
     cudaFuncAttributes at;
-    const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_a<P, LTF, NCH>);
-    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_a<P, LTF, NCH>>() : rt_status(e);
+    const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_a<P, LTF, NCH, SC>);
+    return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_a<P, LTF, NCH, SC>>() : rt_status(e);
 }
 
-template <int P, int LTF>
+template <int P, int LTF, bool SC>
 static int prepare_an() {
-    int s = prepare_a<P, LTF, 2>();
-    if (!s) s = prepare_a<P, LTF, 4>();
-    if (!s) s = prepare_a<P, LTF, 8>();
+    int s = prepare_a<P, LTF, 2, SC>();
+    if (!s) s = prepare_a<P, LTF, 4, SC>();
+    if (!s) s = prepare_a<P, LTF, 8, SC>();
     return s;
 }
 
@@ -1873,22 +1991,23 @@ static int prepare_h() {
     return e == cudaSuccess ? allow_max_smem<fused_eq_kernel_h<LTF, NCH>>() : rt_status(e);
 }
 
-template <int P>
+template <int P, bool SC = false>
 static int prepare_p() {
-    int s = prepare_an<P, 2>();
-    if (!s) s = prepare_an<P, 4>();
-    if (!s) s = prepare_an<P, 8>();
-    if (!s) s = prepare_an<P, 16>();
-    if (!s) s = prepare_v<P, 0>();
-    if (!s) s = prepare_v<P, 2>();
-    if (!s) s = prepare_v<P, 4>();
-    if (!s) s = prepare_v<P, 8>();
-    if (!s) s = prepare_v<P, 16>();
+    int s = prepare_an<P, 2, SC>();
+    if (!s) s = prepare_an<P, 4, SC>();
+    if (!s) s = prepare_an<P, 8, SC>();
+    if (!s) s = prepare_an<P, 16, SC>();
+    if (!s) s = prepare_v<P, 0, SC>();
+    if (!s) s = prepare_v<P, 2, SC>();
+    if (!s) s = prepare_v<P, 4, SC>();
+    if (!s) s = prepare_v<P, 8, SC>();
+    if (!s) s = prepare_v<P, 16, SC>();
     return s;
 }
 
 int prepare_fused_kernels() {
     int s = prepare_p<AERIAL_PREC_FP16>();
+    if (!s) s = prepare_p<AERIAL_PREC_FP16, true>();
     if (!s) s = prepare_h<4, 2>();
     if (!s) s = prepare_h<4, 4>();
     if (!s) s = prepare_h<4, 8>();
@@ -1900,6 +2019,7 @@ int prepare_fused_kernels() {
     if (!s) s = prepare_h<16, 8>();
     if (!s) s = prepare_p<AERIAL_PREC_BF16>();
     if (!s) s = prepare_p<AERIAL_PREC_BF16X3>();
+    if (!s) s = prepare_p<AERIAL_PREC_FP16X3, true>();
     return s;
 }
 

@@ -215,13 +215,43 @@ typedef struct {
     int format;                /* AERIAL_FMT_*; 0 (zero-initialised) = CF32 */
 } aerial_cell_desc;
 
-/* Operand precision of the tensor-core products. */
+/* Operand precision of the tensor-core products.
+ *
+ * Input range.  BF16 and BF16X3 keep the FP32 exponent range.  FP16 keeps 11
+ * significant bits only between 2^-14 and 65504, so the complex64 path scales
+ * each cell's H and Y_rx by an exact power of two s before rounding them to
+ * FP16 whenever its sigma2 lies outside [2^-16, 2^7), bringing s^2 sigma2 into
+ * [2^-10, 2^-8), and uses s^2 sigma2 as the noise variance.  Scaling H, Y_rx
+ * and sigma2 together by any power of two therefore leaves Y_eq, the noise
+ * estimates and the LLRs unchanged.  The scale comes from sigma2 alone: it
+ * assumes sigma2 is the noise of the same samples, and within the window the
+ * raw operands cover received samples up to about 75 dB above the noise.
+ * sigma2 = 0 (zero forcing) takes no scale, so H and Y_rx must then lie within
+ * the FP16 range themselves.  AERIAL_FMT_CF16 cells are read as stored: their
+ * producer chooses the scale (aerial_fp16_operand_scale gives the one the
+ * complex64 path would use). */
 enum {
     AERIAL_PREC_FP16 = 0,      /* FP16 operands, FP32 accumulation */
     AERIAL_PREC_BF16 = 1,      /* BF16 operands, FP32 accumulation */
     AERIAL_PREC_BF16X3 = 2,    /* BF16 hi/lo split, 3 products, FP32 accumulation */
-    AERIAL_PREC_FP32 = 3       /* FP32 CUDA-core products (no tensor cores) */
+    AERIAL_PREC_FP32 = 3,      /* FP32 CUDA-core products: the plain chain
+                                  (aerial_pusch_eq_plain, the serving loop's
+                                  plain mode); the fused entry points return
+                                  AERIAL_ERR_UNSUPPORTED */
+    AERIAL_PREC_FP16X3 = 4     /* FP16 hi/lo split (about 22 significant bits),
+                                  3 products, FP32 accumulation; complex64
+                                  cells only, operands always normalized by a
+                                  power of two to s^2 sigma2 in [1/4, 1) so the
+                                  low halves stay normal */
 };
+
+/* The power-of-two operand scale the FP16 path applies to a complex64 cell
+ * with noise variance sigma2 (1 inside the window above, or for sigma2 = 0).
+ * A producer writing complex-half H and Y_rx can store them times this scale
+ * and pass sigma2 times its square.  Host function, no device work.  New:
+ * the reference converts FP32 to FP16 unscaled
+ * (src/aerial_coef_wmma.cu:165-192) on U(-0.5, 0.5) data only. */
+float aerial_fp16_operand_scale(float sigma2);
 
 /* Launch shape; zero fields take the autotuned / default value.  A shape
  * whose CTAs per SM do not fit the launch's shared memory (e.g. one tuned on
@@ -280,9 +310,13 @@ int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, void* works
  * that loads it until exit; a batch whose largest cell needs more (see
  * aerial_pusch_eq_plain_workspace; e.g. a 273-PRB, 128-antenna, 16-layer
  * cell) is rejected with AERIAL_ERR_SCRATCH_LIMIT before anything runs.
- * The first call on each device looks up the array's device address (make
- * that call before any stream capture).  Calls share the array, so calls
- * that overlap on the GPU race; nothing is allocated or freed. */
+ * Malformed cells return AERIAL_ERR_INVALID_ARG (or AERIAL_ERR_UNSUPPORTED
+ * for a complex-half cell) before the size check.  The first call in each
+ * CUDA context looks up the array's device address: once per device, and
+ * again after a cudaDeviceReset or in a second context on the same device,
+ * each of which holds its own copy of the array (make that call before any
+ * stream capture).  Calls share the array, so calls that overlap on the GPU
+ * race; nothing is allocated or freed. */
 #define AERIAL_STATIC_SCRATCH_BYTES (16u << 20)
 int aerial_pusch_eq_plain_static(const aerial_cell_desc* cells, int nCells, void* stream);
 
@@ -352,6 +386,11 @@ typedef struct {
     long srs_updates;
     int64_t budget_used_bytes;
     long pending;
+    /* where the tail comes from (host clock) */
+    float submit_lag_p99_us, submit_lag_max_us;   /* arrival stamp -> submit call (client side) */
+    float dispatch_gap_max_us;    /* longest dispatcher iteration while work was pending or in flight */
+    float launch_call_max_us;     /* longest host call that enqueued a batch */
+    long misses_late_submit;      /* deadline misses submitted more than half a deadline late */
 } aerial_server_statistics;
 
 typedef struct aerial_server aerial_server;

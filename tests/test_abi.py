@@ -120,3 +120,18 @@ def test_host_pipeline_workspace_and_checks_without_gpu():
     assert lib.aerial_pusch_eq_host(arr, 5, None, 2, ws, 1024, None) == 1001         # workspace too small
     assert lib.aerial_pusch_eq_host(arr, 5, None, 2, ctypes.c_void_p(0x200010), 1 << 40, None) == 1001  # misaligned
     assert lib.aerial_pusch_eq_host(bad, 1, None, 0, ws, 1 << 40, None) == 1001
+
+
+def test_fp16_operand_scale_window():
+    """The host-side FP16 operand scale: 1 inside the window the header
+    states, else an exact power of two putting s^2 sigma2 in [2^-10, 2^-8)."""
+    import math
+    pkg = load_pkg()
+    for s2 in (2.0 ** -16, 0.001, 0.01, 1.0, 2.0 ** 7 * 0.999, 0.0, float("inf"), float("nan")):
+        assert pkg.fp16_operand_scale(s2) == 1.0
+    for s2 in (2.0 ** -16 * 0.999, 1e-9, 1e-20, 2.0 ** 7, 1e6, 1e20):
+        s = pkg.fp16_operand_scale(s2)
+        e = math.log2(s)
+        assert s != 1.0 and e == int(e)
+        v = ctypes.c_float(s2).value * s * s          # the float32 sigma2 the kernel sees
+        assert 2.0 ** -10 <= v < 2.0 ** -8, (s2, s, v)

@@ -2,10 +2,14 @@
 Cholesky, LLR epilogue) against the FP64 model and the plain FP32 chain.
 
 Tolerances (stated per precision):
-  FP16 / BF16x3 operands: EVM of Y_eq vs FP64 <= -45 dB (the target bar);
-  observed margins are tighter and asserted where stated.
-  LLR: max |LLR - LLR64| <= 2e-3 * max|LLR64| (relative to the LLR scale);
-  hard decisions identical to FP64 wherever |LLR64| > 1e-2 * max|LLR64|.
+  FP16 / BF16x3 / FP16x3 operands: EVM of Y_eq vs FP64 <= -45 dB (the target
+  bar); observed margins are tighter and asserted where stated.
+  LLR: max |LLR - LLR64| <= 2e-3 * max|LLR64| (relative to the LLR scale).
+  Hard decisions: on full configuration 1 (20 dB) and 2 (25 dB) slots the
+  number of sign flips against FP64 is asserted exactly per path, and every
+  flip must sit within that path's LLR error bound of zero
+  (test_hard_decisions_vs_fp64).  The FP16x3 path and the plain FP32 chain
+  flip none: their hard decisions are identical to FP64.
 """
 from __future__ import annotations
 
@@ -45,13 +49,15 @@ def check_against_fp64(orc, c, llr, yeq, evm_max=-45.0):
     scale = np.abs(l64).max()
     err = np.abs(llr.astype(np.float64) - l64)
     assert err.max() <= 2e-3 * scale, (err.max(), scale)
-    sure = np.abs(l64) > 1e-2 * scale
-    assert np.array_equal((llr < 0)[sure], (l64 < 0)[sure])
+    # a sign flip can only sit within the LLR error of zero
+    flips = (llr < 0) != (l64 < 0)
+    assert np.all(np.abs(l64[flips]) <= 2e-3 * scale)
     return e
 
 
 @pytest.mark.parametrize("cfg,prec,evm_max", [(1, "fp16", -55.0), (2, "fp16", -55.0), (1, "bf16x3", -80.0),
-                                               (2, "bf16x3", -80.0), (2, "bf16", -40.0)])
+                                               (2, "bf16x3", -80.0), (2, "bf16", -40.0), (1, "fp16x3", -100.0),
+                                               (2, "fp16x3", -100.0)])
 def test_fused_configs_vs_fp64(aeq, wl, orc, cuda, cfg, prec, evm_max):
     c = wl.config_cell(cfg, seed=11)
     (llr, yeq), = run_fused(aeq, [c], cuda, prec)
@@ -62,12 +68,42 @@ def test_fused_configs_vs_fp64(aeq, wl, orc, cuda, cfg, prec, evm_max):
     check_against_fp64(orc, c, llr, yeq, evm_max)
 
 
-@pytest.mark.parametrize("prec,evm_max", [("bf16x3", -60.0), ("fp16", -45.0)])
+@pytest.mark.parametrize("prec,evm_max", [("bf16x3", -60.0), ("fp16", -45.0), ("fp16x3", -100.0)])
 def test_fused_cfg3_correlated_channel(aeq, wl, orc, cuda, prec, evm_max):
     """273 PRB x 128 ant x 16 layers, rho = 0.7 correlated, SNR 30 dB."""
     c = wl.config_cell(3, seed=13)
     (llr, yeq), = run_fused(aeq, [c], cuda, prec)
     check_against_fp64(orc, c, llr, yeq, evm_max)
+
+
+# Hard decisions against FP64 on full slots: (config, path) -> exact number
+# of sign flips for the slot of seed 40 + config, and the path's bound on
+# |LLR64| at a flip (relative to max |LLR64|: the path's LLR error).  The
+# plain chain is the reference's scalar FP32 method (aerial_pusch_eq_plain).
+FLIPS = {(1, "fp16"): None, (2, "fp16"): None, (1, "bf16x3"): None, (2, "bf16x3"): None,
+         (1, "fp16x3"): 0, (2, "fp16x3"): 0, (1, "plain"): 0, (2, "plain"): 0}
+FLIP_BOUND = {"fp16": 1e-3, "bf16x3": 1e-4, "fp16x3": 1e-5, "plain": 1e-3}
+
+
+@pytest.mark.parametrize("cfg,path", sorted(FLIPS))
+def test_hard_decisions_vs_fp64(aeq, wl, orc, cuda, cfg, path):
+    c = wl.config_cell(cfg, seed=40 + cfg)
+    if path == "plain":
+        H, Y = c.H.to(cuda), c.Y.to(cuda)
+        llr_t = torch.full((c.llr_numel,), float("nan"), dtype=torch.float32, device=cuda)
+        d = aeq.cell_desc(H, Y, llr_t, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+        ws = torch.empty(aeq.pusch_eq_plain_workspace([d]), dtype=torch.uint8, device=cuda)
+        aeq.pusch_eq_plain([d], ws)
+        torch.cuda.synchronize()
+        llr = llr_t.cpu().numpy()
+    else:
+        (llr, _), = run_fused(aeq, [c], cuda, path, want_yeq=False)
+    _, _, l64 = oracle64(orc, c)
+    assert np.all(np.isfinite(llr))
+    flips = (llr < 0) != (l64 < 0)
+    scale = np.abs(l64).max()
+    assert int(flips.sum()) == FLIPS[(cfg, path)], f"{int(flips.sum())} flips of {flips.size}"
+    assert np.all(np.abs(l64[flips]) <= FLIP_BOUND[path] * scale)
 
 
 EDGE = [  # (nPRB, nAnt, nLayers, nSym, qam)
