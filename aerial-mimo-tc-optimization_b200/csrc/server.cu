@@ -55,7 +55,7 @@ struct SrvReq {
     // SRS update operands
     const aerial_ch2 *srs = nullptr, *W = nullptr, *focc = nullptr;
     int K = 0, P = 0, F = 0, nSrs = 1;
-    int64_t arrival = 0, launched = 0, done = 0;
+    int64_t arrival = 0, submitted = 0, launched = 0, done = 0;
     int status = AERIAL_OK;
     bool admitted = false, finished = false;
 };
@@ -92,6 +92,10 @@ struct aerial_server {
     // statistics
     std::vector<int64_t> lat;          // completion - arrival (ns) of finished slots
     std::vector<int64_t> qlat, slat;   // arrival -> launch, launch -> completion
+    std::vector<int64_t> sublag;       // arrival stamp -> submit call (client side)
+    int64_t gapMax = 0;                // longest dispatcher iteration while work was pending or in flight
+    int64_t launchCallMax = 0;         // longest host call that enqueued a batch
+    long missesLateSubmit = 0;         // misses whose submission alone came half a deadline late
     int64_t firstArrival = 0, lastDone = 0;
     long resDone = 0, batchesLaunched = 0, slotsLaunched = 0, srsDone = 0, misses = 0;
     int launchError = 0;
@@ -122,10 +126,15 @@ static void finish_batch(aerial_server* s, SrvBatch& b, int status) {
         if (r->kind == 0) {
             s->used -= c.reqBytes;
             const int64_t l = r->done - r->arrival;
+            const int64_t deadline = (int64_t)(s->cfg.deadline_us * 1000.0);
             s->lat.push_back(l);
             s->qlat.push_back(r->launched - r->arrival);
             s->slat.push_back(r->done - r->launched);
-            if (l > (int64_t)(s->cfg.deadline_us * 1000.0)) s->misses++;
+            s->sublag.push_back(r->submitted - r->arrival);
+            if (l > deadline) {
+                s->misses++;
+                if (2 * (r->submitted - r->arrival) > deadline) s->missesLateSubmit++;
+            }
             s->resDone += c.res;
             s->lastDone = std::max(s->lastDone, t);
         } else {
@@ -246,7 +255,9 @@ static void dispatcher(aerial_server* s) {
     cudaSetDevice(s->device);
     Formed f;
     std::unique_lock<std::mutex> lk(s->mu, std::defer_lock);
+    int64_t lastIter = 0;                 // start of the previous iteration that had work (0: idle)
     while (true) {
+        const int64_t iterStart = now_ns();
         bool progress = false;
         // completions (the busy flags and events are the dispatcher's own)
         for (SrvBatch& b : s->batches) {
@@ -288,14 +299,19 @@ static void dispatcher(aerial_server* s) {
             lk.unlock();
             if (!formed) continue;
             progress = true;
+            const int64_t c0 = now_ns();
             const int status = launch_formed(s, (int)i, f);
-            if (status) {
+            const int64_t callNs = now_ns() - c0;
+            if (status || callNs > s->launchCallMax) {
                 lk.lock();
-                s->launchError = status;
-                finish_batch(s, b, status);
-                s->inflightBatches--;
+                s->launchCallMax = std::max(s->launchCallMax, callNs);
+                if (status) {
+                    s->launchError = status;
+                    finish_batch(s, b, status);
+                    s->inflightBatches--;
+                }
                 lk.unlock();
-                s->doneCv.notify_all();
+                if (status) s->doneCv.notify_all();
             }
         }
         bool anyBusy = false;
@@ -306,9 +322,21 @@ static void dispatcher(aerial_server* s) {
             return;
         }
         const bool waiting = !s->pending.empty() && !s->paused;   // e.g. inside a batching window
-        if (!anyBusy && !progress && !waiting) s->cv.wait_for(lk, std::chrono::milliseconds(2));
+        // the host's view of the loop: the longest step between two
+        // iterations that had work (a descheduled dispatcher shows here)
+        if (lastIter && (anyBusy || waiting)) s->gapMax = std::max(s->gapMax, iterStart - lastIter);
+        lastIter = (anyBusy || waiting || progress) ? iterStart : 0;
+        if (!anyBusy && !progress && !waiting) {
+            // idle: sleep until a submission (or stop) notifies; the timeout
+            // only bounds a missed wake-up
+            s->cv.wait_for(lk, std::chrono::milliseconds(2));
+            lk.unlock();
+            continue;
+        }
         lk.unlock();
-        if (anyBusy || waiting) std::this_thread::yield();
+        // work in flight or pending: poll again at once (a yield keeps the
+        // core available to the submitting threads on a busy host)
+        std::this_thread::yield();
     }
 }
 
@@ -456,7 +484,8 @@ extern "C" int aerial_server_submit(aerial_server* s, int cellId, const aerial_c
     SrvReq* r = new SrvReq();
     r->Y = Y_rx;
     r->llr = llr;
-    r->arrival = arrival_ns > 0 ? arrival_ns : now_ns();
+    r->submitted = now_ns();
+    r->arrival = arrival_ns > 0 ? arrival_ns : r->submitted;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (cellId < 0 || cellId >= (int)s->cells.size()) { delete r; return AERIAL_ERR_NOT_FOUND; }
@@ -497,7 +526,7 @@ extern "C" int aerial_server_srs_update_n(aerial_server* s, int cellId, const ae
     r->focc = FOCC;
     r->K = K;
     r->F = foccLen;
-    r->arrival = now_ns();
+    r->arrival = r->submitted = now_ns();
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (cellId < 0 || cellId >= (int)s->cells.size()) { delete r; return AERIAL_ERR_NOT_FOUND; }
@@ -594,7 +623,12 @@ extern "C" int aerial_server_stats(aerial_server* s, aerial_server_statistics* o
         };
         st.queue_p99_us = p99(s->qlat);
         st.service_p99_us = p99(s->slat);
+        st.submit_lag_p99_us = p99(s->sublag);
+        st.submit_lag_max_us = (float)(*std::max_element(s->sublag.begin(), s->sublag.end()) * 1e-3);
     }
+    st.dispatch_gap_max_us = (float)(s->gapMax * 1e-3);
+    st.launch_call_max_us = (float)(s->launchCallMax * 1e-3);
+    st.misses_late_submit = s->missesLateSubmit;
     st.deadline_misses = s->misses;
     st.res_done = s->resDone;
     st.span_s = (s->lastDone > s->firstArrival) ? (double)(s->lastDone - s->firstArrival) * 1e-9 : 0.0;
@@ -614,7 +648,9 @@ extern "C" int aerial_server_reset_stats(aerial_server* s) {
     s->lat.clear();
     s->qlat.clear();
     s->slat.clear();
+    s->sublag.clear();
+    s->gapMax = s->launchCallMax = 0;
     s->firstArrival = s->lastDone = 0;
-    s->resDone = s->batchesLaunched = s->slotsLaunched = s->srsDone = s->misses = 0;
+    s->resDone = s->batchesLaunched = s->slotsLaunched = s->srsDone = s->misses = s->missesLateSubmit = 0;
     return AERIAL_OK;
 }

@@ -63,13 +63,14 @@ def parse():
     ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
                     help="benchmark configuration (2 = the headline 100 MHz cell)")
     ap.add_argument("--slots", type=int, default=0, help="cell-slots per step per GPU (0 = the config's default)")
-    ap.add_argument("--precision", default="", choices=["", "fp16", "bf16", "bf16x3"])
+    ap.add_argument("--precision", default="", choices=["", "fp16", "bf16", "bf16x3", "fp16x3"])
     ap.add_argument("--io", default="cf32", choices=["cf32", "fp16"],
                     help="storage of H / Y_rx / LLRs: cf32 = the drop-in complex64 layout (default); fp16 = complex "
                          "half in, __half LLRs out (configs 1, 2 and 3 with FP16 operands), reported as its own line")
     ap.add_argument("--duration", type=float, default=1.0, help="serving run length in seconds (config 5)")
     ap.add_argument("--window-us", type=float, default=0.0, help="serving batching window (config 5; 0 = launch at once)")
     ap.add_argument("--min-batch", type=int, default=0, help="serving minimum batch before the window ends")
+    ap.add_argument("--serve-streams", type=int, default=0, help="serving batches in flight (0 = default)")
     ap.add_argument("--srs-symbols", type=int, default=4, choices=[1, 2, 4],
                     help="SRS symbols averaged by each serving SRS update (config 5)")
     ap.add_argument("--soak", type=float, default=1.5, help="seconds of untimed load before timing (clock steady state)")
@@ -157,21 +158,35 @@ def host_cell(wl, cfg: int):
     return wl.multicell(16, seed=42)[0]
 
 
+def cell_seeds(cfg: int, slots: int, rank: int):
+    """The generator seed of each cell of a rank's step.  Ranks draw from
+    disjoint seed sets (weak scaling: every rank equalizes its own slots):
+    1000 rank + 17 i + 1 never repeats across ranks for i < 1000, and the
+    16-cell batch's per-cell seeds (base + 1000 i) stay below the next rank's
+    base of 1,000,000 rank."""
+    if cfg in (2, 3):
+        return [1000 * rank + 17 * i + 1 for i in range(slots)]
+    if cfg == 1:
+        per = -(-slots // 64)
+        return [1000 * rank + 17 * i + 1 for i in range(-(-slots // per))]
+    if cfg == 4:
+        base = 42 + 1_000_000 * rank
+        return [base + 1000 * i for i in range(slots)]
+    raise ValueError(cfg)
+
+
 def build_cells(wl, cfg: int, slots: int, rank: int, dev):
     """The step's cell-slots.  Slots of one configuration share sigma2, so for
     the small configuration 1 consecutive slots are laid out contiguously and
     described as one cell of slots x 24 PRBs (at most 64 descriptors a launch)."""
-    if cfg == 2:
-        return [wl.config_cell(2, seed=1000 * rank + 17 * i + 1, device=dev) for i in range(slots)]
-    if cfg == 3:
-        return [wl.config_cell(3, seed=1000 * rank + 17 * i + 1, device=dev) for i in range(slots)]
+    seeds = cell_seeds(cfg, slots, rank)
+    if cfg in (2, 3):
+        return [wl.config_cell(cfg, seed=sd, device=dev) for sd in seeds]
     if cfg == 1:
         per = -(-slots // 64)
-        n = -(-slots // per)
-        return [wl.make_cell(24 * per, 32, 4, 11, 16, 20.0, "iid", seed=1000 * rank + 17 * i + 1, device=dev)
-                for i in range(n)]
+        return [wl.make_cell(24 * per, 32, 4, 11, 16, 20.0, "iid", seed=sd, device=dev) for sd in seeds]
     if cfg == 4:
-        return wl.multicell(slots, seed=42 + 1000 * rank, device=dev)
+        return wl.multicell(slots, seed=seeds[0], device=dev)
     raise ValueError(cfg)
 
 
@@ -413,6 +428,9 @@ def main():
     cpu_base = None
     if rank == 0 and world == 1 and not a.no_extras:
         extras = bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a)
+        if a.config == 2:
+            extras["path_rates"] = path_rates(aeq, descs, res_per_step, bytes_per_step, stream)
+            extras["other_configs"] = other_configs(aeq, wl, dev, stream, a)
         if a.config == 4:
             extras["tiles"] = compare_tiles(aeq, descs, tun, stream, a, flush)
             extras["per_cell_streams_vs_batched"] = compare_streams(aeq, descs, tun, a, flush)
@@ -439,8 +457,20 @@ def main():
         if not half:
             try:   # the oracle as the checker of slot 0; reported, never fatal for the timing line
                 extras["accuracy_vs_fp64"] = accuracy_vs_fp64(orc, aeq, cells, llrs, descs, tun, stream)
+                if a.config == 2 and not a.no_extras:
+                    c3 = build_cells(wl, 3, 1, 0, dev)
+                    l3 = [torch.empty(c3[0].llr_numel, dtype=torch.float32, device=dev)]
+                    d3 = [aeq.cell_desc(c3[0].H, c3[0].Y, l3[0], c3[0].sigma2, c3[0].nPRB, c3[0].nAnt,
+                                        c3[0].nLayers, c3[0].nSym, c3[0].nPamBits)]
+                    extras["accuracy_vs_fp64_config3"] = accuracy_vs_fp64(
+                        orc, aeq, c3, l3, d3, aeq.make_tuning("bf16x3"), stream)
             except Exception as e:
                 extras["accuracy_vs_fp64"] = {"error": str(e)}
+        if a.config == 2 and not a.no_extras:
+            try:   # the reference's own kernels on this GPU: a baseline, from the checker libraries
+                extras["reference_kernels_on_b200"] = reference_kernels_on_b200(aeq, wl, dev)
+            except Exception as e:
+                extras["reference_kernels_on_b200"] = {"error": str(e)}
 
     if graph is not None:
         graph.close()
@@ -476,102 +506,153 @@ def main():
     print(json.dumps(line), flush=True)
 
 
-def run_serving(a, aeq, wl, dev):
-    """Configuration 5: 40 cells submit slots as Poisson arrivals (mean one
-    slot per 500 us per cell) to the serving loop; every 20th slot of a cell
-    is preceded by an SRS channel update (filter multiply, K = 12, one port per
-    layer, averaged over 4 SRS symbols).  The same arrival trace is served by
-    the fused batched loop and by the plain FP32 chain run request by request."""
-    import numpy as np
-    import torch
+class ServingWorkload:
+    """Configuration 5's cells and buffers: 40 cells with shapes drawn as the
+    16-cell batch, two received slots per cell (alternated), a ring of 16 LLR
+    outputs per cell, and SRS operands (K = 12, one port per layer, averaged
+    over `srs_syms` SRS symbols)."""
 
-    n_cells, per_slot_s, srs_every, srs_syms = 40, 500e-6, 20, a.srs_symbols
-    shapes = wl.multicell_shapes(n_cells, seed=5)
-    cells, Ys, rings, srs_ops = [], [], [], []
-    for i, (p, A, L, q, snr) in enumerate(shapes):
-        c = wl.make_cell(p, A, L, 11, q, snr, "iid", seed=5000 + i, device=dev)
-        extra = wl.make_cell(p, A, L, 11, q, snr, "iid", seed=7000 + i, device=dev)
-        cells.append(c)
-        Ys.append([c.Y, extra.Y])
-        rings.append([torch.empty(c.llr_numel, dtype=torch.float32, device=dev) for _ in range(16)])
-        g = torch.Generator(device=dev)
-        g.manual_seed(9000 + i)
-        nblk = c.nSC // 12
-        srs_ops.append([(torch.randn(n, generator=g, device=dev) * 0.5).half().view(torch.int16).contiguous()
-                        for n in (2 * srs_syms * nblk * A * 12, 2 * 12 * 12, 2 * L * 12)])
-    rng = np.random.default_rng(11)
-    arrivals = []
-    for ci in range(n_cells):
-        t = rng.exponential(per_slot_s)
-        while t < a.duration:
-            arrivals.append((t, ci))
-            t += rng.exponential(per_slot_s)
-    arrivals.sort()
-    lib = aeq.lib()
+    def __init__(self, aeq, wl, dev, srs_syms, n_cells=40):
+        import torch
 
-    def serve(mode, window_us, min_batch):
-        srv = aeq.Server(memory_budget_bytes=16 << 30, streams=3, max_batch=64, precision=a.precision,
+        self.aeq, self.n_cells, self.srs_syms = aeq, n_cells, srs_syms
+        shapes = wl.multicell_shapes(n_cells, seed=5)
+        self.cells, self.Ys, self.rings, self.srs_ops = [], [], [], []
+        for i, (p, A, L, q, snr) in enumerate(shapes):
+            c = wl.make_cell(p, A, L, 11, q, snr, "iid", seed=5000 + i, device=dev)
+            extra = wl.make_cell(p, A, L, 11, q, snr, "iid", seed=7000 + i, device=dev)
+            self.cells.append(c)
+            self.Ys.append([c.Y, extra.Y])
+            self.rings.append([torch.empty(c.llr_numel, dtype=torch.float32, device=dev) for _ in range(16)])
+            g = torch.Generator(device=dev)
+            g.manual_seed(9000 + i)
+            nblk = c.nSC // 12
+            self.srs_ops.append([(torch.randn(n, generator=g, device=dev) * 0.5).half().view(torch.int16).contiguous()
+                                 for n in (2 * srs_syms * nblk * A * 12, 2 * 12 * 12, 2 * L * 12)])
+
+    def arrivals(self, duration, n_active, per_slot_s=500e-6, seed=11):
+        """Poisson slot arrivals of the first n_active cells, mean one per per_slot_s each."""
+        import numpy as np
+
+        rng = np.random.default_rng(seed)
+        out = []
+        for ci in range(n_active):
+            t = rng.exponential(per_slot_s)
+            while t < duration:
+                out.append((t, ci))
+                t += rng.exponential(per_slot_s)
+        out.sort()
+        return out
+
+    def serve(self, arrivals, mode, precision, streams, window_us=0.0, min_batch=0, srs_every=20):
+        """Replay an arrival trace against a fresh server; its statistics."""
+        import gc
+
+        import torch
+
+        aeq = self.aeq
+        lib = aeq.lib()
+        srv = aeq.Server(memory_budget_bytes=16 << 30, streams=streams, max_batch=64, precision=precision,
                          mode=mode, deadline_us=500.0, batch_window_us=window_us, min_batch=min_batch)
-        ids = []
-        for c in cells:
+        active = sorted({ci for _, ci in arrivals})
+        ids = {}
+        for ci in active:
+            c = self.cells[ci]
             k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
             srv.set_channel(k, c.H, c.sigma2)
-            ids.append(k)
-        # one untimed slot per cell (first launch of every shape), then reset the statistics by
-        # draining and polling before the trace starts
-        for ci, k in enumerate(ids):
-            srv.submit(k, Ys[ci][0], rings[ci][0])
+            ids[ci] = k
+        # one untimed slot per cell (first launch of every shape), then reset the statistics
+        for ci in active:
+            srv.submit(ids[ci], self.Ys[ci][0], self.rings[ci][0])
         srv.drain(60000)
         srv.poll(max_out=4096)
         srv.reset_stats()
-        yp = [[ctypes.c_void_p(y.data_ptr()) for y in ys] for ys in Ys]
-        rp = [[ctypes.c_void_p(r.data_ptr()) for r in ring] for ring in rings]
-        sp = [[ctypes.c_void_p(t.data_ptr()) for t in ops] for ops in srs_ops]
-        count = [0] * n_cells
+        yp = {ci: [ctypes.c_void_p(y.data_ptr()) for y in self.Ys[ci]] for ci in active}
+        rp = {ci: [ctypes.c_void_p(r.data_ptr()) for r in self.rings[ci]] for ci in active}
+        sp = {ci: [ctypes.c_void_p(t.data_ptr()) for t in self.srs_ops[ci]] for ci in active}
+        count = dict.fromkeys(active, 0)
         handle = srv._h
+        submit, srs_update = lib.aerial_server_submit, lib.aerial_server_srs_update_n
         torch.cuda.synchronize()
         t0 = time.monotonic_ns() + 20_000_000
+        plan = [(t0 + int(t * 1e9), ci) for t, ci in arrivals]
         errors = 0
-        lag = []
-        for t, ci in arrivals:
-            target = t0 + int(t * 1e9)
-            now = time.monotonic_ns()
-            while now < target:
-                now = time.monotonic_ns()
-            lag.append(now - target)
-            k = count[ci]
-            count[ci] += 1
-            if k and k % srs_every == 0:
-                errors += lib.aerial_server_srs_update_n(handle, ids[ci], sp[ci][0], srs_syms, sp[ci][1], sp[ci][2],
-                                                         12, 12, None) != 0
-            errors += lib.aerial_server_submit(handle, ids[ci], yp[ci][k % 2], rp[ci][k % 16], target, None) != 0
+        gc_was = gc.isenabled()
+        gc.disable()                    # no collector pause inside the trace (the client is Python)
+        try:
+            for target, ci in plan:
+                while time.monotonic_ns() < target:
+                    pass
+                k = count[ci]
+                count[ci] = k + 1
+                if k and k % srs_every == 0:
+                    errors += srs_update(handle, ids[ci], sp[ci][0], self.srs_syms, sp[ci][1], sp[ci][2],
+                                         12, 12, None) != 0
+                errors += submit(handle, ids[ci], yp[ci][k % 2], rp[ci][k % 16], target, None) != 0
+        finally:
+            if gc_was:
+                gc.enable()
         srv.drain(600000)
         st = srv.stats()
         srv.close()
         st["submit_errors"] = int(errors)
-        lag.sort()
-        st["client_submit_lag_p99_us"] = lag[int(0.99 * (len(lag) - 1))] * 1e-3 if lag else 0.0
         st["miss_rate"] = st["deadline_misses"] / max(1, st["slots_done"])
+        st["slots_offered"] = len(arrivals)
+        st["streams"], st["batch_window_us"], st["min_batch"] = streams, window_us, min_batch
         return st
 
-    fused = serve(aeq.SERVER_FUSED, a.window_us, a.min_batch)
-    plain = serve(aeq.SERVER_PLAIN, 0.0, 0)
-    keep = ("slots_done", "p50_us", "p99_us", "max_us", "mean_us", "queue_p99_us", "service_p99_us",
-            "deadline_misses", "miss_rate", "res_per_s", "batches", "mean_batch", "srs_updates", "submit_errors",
-            "client_submit_lag_p99_us")
+
+SERVE_KEYS = ("slots_offered", "slots_done", "p50_us", "p99_us", "max_us", "mean_us", "queue_p99_us",
+              "service_p99_us", "deadline_misses", "miss_rate", "res_per_s", "batches", "mean_batch", "srs_updates",
+              "submit_errors", "submit_lag_p99_us", "submit_lag_max_us", "dispatch_gap_max_us", "launch_call_max_us",
+              "misses_late_submit", "streams", "batch_window_us", "min_batch")
+
+# Configuration 5's dispatcher settings: batches in flight and batching window.
+SERVE_STREAMS, SERVE_WINDOW_US, SERVE_MIN_BATCH = 2, 0.0, 0
+# Cells whose Poisson load the plain FP32 chain, request by request, sustains
+# (the kernel comparison runs both paths on this lighter trace).
+SERVE_LIGHT_CELLS = 4
+
+
+def serving_summary(a, aeq, wl, dev, duration, streams, window_us, min_batch, compare_plain=True):
+    """Configuration 5 on one trace: the fused batched loop at the full 40-cell
+    load; and, on a lighter trace of SERVE_LIGHT_CELLS cells that the plain
+    FP32 chain sustains, both paths, so their p99 compares kernels rather
+    than an unbounded queue."""
+    w = ServingWorkload(aeq, wl, dev, a.srs_symbols)
+    full = w.serve(w.arrivals(duration, w.n_cells), aeq.SERVER_FUSED, a.precision, streams, window_us, min_batch)
+    out = {"fused_batched": {k: full[k] for k in SERVE_KEYS}}
+    if compare_plain:
+        light = w.arrivals(duration, SERVE_LIGHT_CELLS)
+        lf = w.serve(light, aeq.SERVER_FUSED, a.precision, streams, window_us, min_batch)
+        lp = w.serve(light, aeq.SERVER_PLAIN, a.precision, streams, 0.0, 0)
+        out["light_load"] = {
+            "cells": SERVE_LIGHT_CELLS,
+            "fused_batched": {k: lf[k] for k in SERVE_KEYS},
+            "plain_fp32_per_request": {k: lp[k] for k in SERVE_KEYS},
+            "p99_ratio_plain_over_fused": lp["p99_us"] / max(lf["p99_us"], 1e-9)}
+    return out
+
+
+def run_serving(a, aeq, wl, dev):
+    """Configuration 5: 40 cells submit slots as Poisson arrivals (mean one
+    slot per 500 us per cell) to the serving loop; every 20th slot of a cell
+    is preceded by an SRS channel update (filter multiply, K = 12, one port per
+    layer, averaged over 4 SRS symbols)."""
+    streams = a.serve_streams or SERVE_STREAMS
+    res = serving_summary(a, aeq, wl, dev, a.duration, streams, a.window_us, a.min_batch)
+    fused = res["fused_batched"]
     line = {
         "metric": "serving: equalized REs/s with p99 slot latency (deadline 500 us)", "value": fused["res_per_s"],
         "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "benchmark_config": 5,
-        "config": {"workload": (f"{n_cells} cells, Poisson slot arrivals (mean one per 500 us per cell) for "
+        "config": {"workload": (f"40 cells, Poisson slot arrivals (mean one per 500 us per cell) for "
                                 f"{a.duration:.1f} s, shapes drawn as the 16-cell batch, SRS update (filter multiply "
-                                f"averaged over {srs_syms} SRS symbols) every {srs_every} slots, 16 GB admission "
-                                f"budget, 3 streams, up to 64 slots a launch"),
-                   "slots_offered": len(arrivals), "precision": a.precision},
-        "fused_batched": dict({k: fused[k] for k in keep}, batch_window_us=a.window_us, min_batch=a.min_batch),
-        "plain_fp32_per_request": {k: plain[k] for k in keep},
-        "p99_ratio_plain_over_fused": plain["p99_us"] / max(fused["p99_us"], 1e-9),
+                                f"averaged over {a.srs_symbols} SRS symbols) every 20 slots, 16 GB admission "
+                                f"budget, {streams} streams, up to 64 slots a launch"),
+                   "precision": a.precision},
         "data": "synthetic (seeded, generated on device)",
     }
+    line.update(res)
     print(json.dumps(line), flush=True)
 
 
@@ -829,7 +910,9 @@ def accuracy_vs_fp64(orc, aeq, cells, llrs, descs, tun, stream):
     """Checker: slot 0 against the FP64 model of the oracle, through the fused
     launch at the bench's operand precision (the top-level keys), and under
     `by_path` at every operand precision and through the plain FP32 chain
-    (the reference's method), so the precisions compare at the same EVM."""
+    (the reference's method), so the precisions compare at the same EVM.
+    `hard_bit_mismatch` counts every sign flip against FP64, unmasked;
+    `flip_max_abs_llr64_rel` is the largest |LLR64| at a flip over max |LLR64|."""
     import numpy as np
     import torch
 
@@ -846,19 +929,183 @@ def accuracy_vs_fp64(orc, aeq, cells, llrs, descs, tun, stream):
         torch.cuda.synchronize()
         y = yeq.cpu().numpy().astype(np.complex128)
         l = llr.cpu().numpy().astype(np.float64)
+        flips = (l < 0) != (l64 < 0)
+        scale = float(np.abs(l64).max())
         return {"evm_db": float(10 * np.log10(np.sum(np.abs(y - y64) ** 2) / np.sum(np.abs(y64) ** 2))),
-                "llr_max_abs_err": float(np.abs(l - l64).max()), "llr_scale": float(np.abs(l64).max()),
-                "hard_bit_mismatch": int(np.sum((l < 0) != (l64 < 0))), "bits": int(l.size),
+                "llr_max_abs_err": float(np.abs(l - l64).max()), "llr_scale": scale,
+                "hard_bit_mismatch": int(np.sum(flips)), "bits": int(l.size),
+                "flip_max_abs_llr64_rel": float(np.abs(l64[flips]).max() / scale) if flips.any() else 0.0,
                 "ber_vs_tx": float(np.mean((l < 0).astype(np.uint8) != bits))}
 
     out = run(lambda d: aeq.pusch_eq_fused([d], tun, stream))
     by = {}
-    for name in ("fp16", "bf16", "bf16x3"):
+    for name in ("fp16", "bf16", "bf16x3", "fp16x3"):
         by["fused_" + name] = run(lambda d: aeq.pusch_eq_fused([d], aeq.make_tuning(name), stream))
     ws = torch.empty(aeq.pusch_eq_plain_workspace(descs[:1]), dtype=torch.uint8, device=c.H.device)
     by["plain_fp32_chain"] = run(lambda d: aeq.pusch_eq_plain([d], ws, stream))
     out["by_path"] = by
     return out
+
+
+def path_rates(aeq, descs, res_per_step, bytes_per_step, stream, k=20):
+    """The headline step (same slots, same launch) at each operand precision:
+    mean launch time, REs/s and HBM fraction, so the accuracy of each path in
+    `accuracy_vs_fp64.by_path` sits next to its cost."""
+    peak, _ = measured_peaks()
+    out = {}
+    for name in ("fp16", "bf16", "bf16x3", "fp16x3"):
+        t = aeq.make_tuning(name)
+        us = _time_launches(lambda: aeq.pusch_eq_fused(descs, t, stream), stream, k)
+        out["fused_" + name] = {"us_per_launch": us, "res_per_s": res_per_step / (us * 1e-6),
+                                "hbm_frac": bytes_per_step / (us * 1e-6) / 1e9 / peak}
+    return out
+
+
+def _timed_flushed(fn, stream, flush, k=20):
+    """Mean of k event-timed launches, L2 flushed before each (inputs near or
+    below the L2 size)."""
+    import torch
+
+    for _ in range(3):
+        fn()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+    for i in range(k):
+        if flush is not None:
+            flush.fill_(float(i))
+        ev[i][0].record(stream)
+        fn()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    return 1e3 * statistics.mean(x.elapsed_time(y) for x, y in ev)
+
+
+def other_configs(aeq, wl, dev, stream, a):
+    """Configurations 3, 4 and 5 in compact form for the default line, each a
+    few seconds: the 12-slot precision-stress launch per operand precision;
+    the uneven 16-cell batch as a CUDA graph replay, autotuned against the
+    fixed default shape; and one second of the serving loop."""
+    import torch
+
+    peak, _ = measured_peaks()
+    out = {}
+    # configuration 3: 12 slots of 273 PRB x 128 antennas x 16 layers (1.3 GB: larger than L2)
+    cells = build_cells(wl, 3, 12, 0, dev)
+    llrs = [torch.empty(c.llr_numel, dtype=torch.float32, device=dev) for c in cells]
+    descs = [aeq.cell_desc(c.H, c.Y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+             for c, l in zip(cells, llrs)]
+    res = sum(c.n_re for c in cells)
+    nbytes = sum(c.algorithmic_bytes() for c in cells)
+    c3 = {"workload": WORKLOADS[3], "slots": len(cells)}
+    for name in ("bf16x3", "fp16x3", "fp16"):
+        t = aeq.make_tuning(name)
+        us = _time_launches(lambda: aeq.pusch_eq_fused(descs, t, stream), stream, 10)
+        c3[name] = {"us_per_launch": us, "res_per_s": res / (us * 1e-6),
+                    "hbm_frac": nbytes / (us * 1e-6) / 1e9 / peak}
+    out["config3"] = c3
+    del cells, llrs, descs
+    torch.cuda.empty_cache()
+    # configuration 4: the uneven 16-cell batch, one persistent launch replayed as a CUDA graph
+    cells = build_cells(wl, 4, 16, 0, dev)
+    llrs = [torch.empty(c.llr_numel, dtype=torch.float32, device=dev) for c in cells]
+    descs = [aeq.cell_desc(c.H, c.Y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits)
+             for c, l in zip(cells, llrs)]
+    res = sum(c.n_re for c in cells)
+    nbytes = sum(c.algorithmic_bytes() for c in cells)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    tuned, _ = aeq.autotune(descs, "fp16")
+    fixed = aeq.make_tuning("fp16")
+    g = aeq.FusedGraph(descs, tuned)
+    try:
+        us = _timed_flushed(lambda: g.launch(stream), stream, flush)
+    finally:
+        g.close()
+    out["config4"] = {
+        "workload": WORKLOADS[4], "launch": "CUDA graph replay of the persistent launch, L2 flushed before each",
+        "us_per_launch": us, "res_per_s": res / (us * 1e-6), "hbm_frac": nbytes / (us * 1e-6) / 1e9 / peak,
+        "autotuned_us": _timed_flushed(lambda: aeq.pusch_eq_fused(descs, tuned, stream), stream, flush),
+        "fixed_default_us": _timed_flushed(lambda: aeq.pusch_eq_fused(descs, fixed, stream), stream, flush),
+        "autotuned": {"warps_per_cta": tuned.warps_per_cta, "ctas_per_sm": tuned.ctas_per_sm,
+                      "sc_per_group": tuned.sc_per_group}}
+    del cells, llrs, descs, flush
+    torch.cuda.empty_cache()
+    # configuration 5: one second of the serving loop
+    a5 = argparse.Namespace(**vars(a))
+    a5.precision = DEFAULT_PRECISION[5]
+    out["config5"] = serving_summary(a5, aeq, wl, dev, 1.0, SERVE_STREAMS, SERVE_WINDOW_US, SERVE_MIN_BATCH)
+    out["config5"]["duration_s"] = 1.0
+    return out
+
+
+def reference_kernels_on_b200(aeq, wl, dev, slots=64):
+    """Baseline: the reference's own kernels, compiled unchanged from its
+    sources into the checker libraries (oracle/_ref), on this GPU over the
+    headline step's 64 cell-slots: gram_scalar -> coef_apply_v2_wmma -> llr_v3
+    (three launches, no MMSE solve: the reference has none), against one fused
+    launch of this library with the solve.  The reference's C and the LLR
+    input are random (its benchmarks do not chain data).  Median of 20
+    event-timed repetitions after 3 warm-ups; 1.3 GB of inputs (larger than
+    L2).  Shapes: src/aerial_bottleneck.cu:174-179, src/aerial_coef_wmma.cu:400-404,
+    src/llr/aerial_llr_v3.cu:292."""
+    import torch
+
+    reflib = os.path.join(ROOT, "oracle", "_ref")
+    need = [os.path.join(reflib, f"libref_{n}.so") for n in ("gram", "coef", "llr_v3")]
+    if not all(os.path.exists(x) for x in need):
+        return {"unavailable": "oracle/_ref not built (make -C oracle ref needs the reference sources)"}
+    VP, CI = ctypes.c_void_p, ctypes.c_int
+    lg, lc, ll = (ctypes.CDLL(x) for x in need)
+    lg.ref_gram_launch.argtypes = [VP, VP, VP, CI]
+    lc.ref_coef_launch.argtypes = [CI, VP, VP, VP, CI, CI]
+    ll.ref_llr_v3_launch.argtypes = [CI, VP, VP, VP, CI, CI]
+    nSC1, S, L, A, nb = 1584, 11, 8, 64, 4
+    cells = [wl.config_cell(2, seed=17 * i + 1, device=dev) for i in range(slots)]
+    nS = nSC1 * slots
+    Hs = torch.cat([x.H for x in cells])
+    Ys = torch.cat([x.Y for x in cells])
+    Ms = Hs.conj().transpose(1, 2).contiguous()
+    Gs = torch.empty(nS, L, L, dtype=torch.complex64, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    Cs = torch.complex(torch.rand((nS, L, A), generator=g, device=dev) - 0.5,
+                       torch.rand((nS, L, A), generator=g, device=dev) - 0.5)
+    Os = torch.empty(nS, L, S, dtype=torch.complex64, device=dev)
+    Ns = nS * L * S
+    soft = ((torch.rand(2 * Ns, generator=g, device=dev) - 0.5) * 1.4).half()
+    ni = torch.rand(Ns, generator=g, device=dev) * 10 + 1
+    lo = torch.empty(Ns * 2 * nb, dtype=torch.float16, device=dev)
+    llrs = [torch.empty(x.llr_numel, dtype=torch.float32, device=dev) for x in cells]
+    descs = [aeq.cell_desc(x.H, x.Y, l, x.sigma2, x.nPRB, x.nAnt, x.nLayers, x.nSym, x.nPamBits)
+             for x, l in zip(cells, llrs)]
+    tun = aeq.make_tuning("fp16")
+    stream = torch.cuda.current_stream()    # the checker libraries launch on the default stream
+
+    def ref_chain():
+        lg.ref_gram_launch(Ms.data_ptr(), Hs.data_ptr(), Gs.data_ptr(), nS)
+        lc.ref_coef_launch(2, Cs.data_ptr(), Ys.data_ptr(), Os.data_ptr(), nS, S)
+        ll.ref_llr_v3_launch(3, soft.data_ptr(), ni.data_ptr(), lo.data_ptr(), Ns, nb)
+
+    def med(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        t = []
+        for _ in range(20):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda._sleep(200000)     # the GPU stays busy while the host enqueues
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t.append(1e3 * e0.elapsed_time(e1))
+        return statistics.median(t)
+
+    t_ref = med(ref_chain)
+    t_fused = med(lambda: aeq.pusch_eq_fused(descs, tun, stream))
+    return {"slots": slots, "subcarriers": nS,
+            "reference_gram_coefv2_llrv3_us": t_ref, "reference_res_per_s": nS * S / (t_ref * 1e-6),
+            "fused_us": t_fused, "fused_res_per_s": nS * S / (t_fused * 1e-6), "speedup": t_ref / t_fused,
+            "note": "reference: three unfused launches without a solve, from oracle/_ref; fused: Gram + MMSE "
+                    "solve + apply + LLR in one launch"}
 
 
 def _time_launches(fn, stream, k=50):
