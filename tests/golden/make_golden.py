@@ -1,7 +1,7 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
-Run in a checkout where the reference tree is present (default
-/root/reference, override with AERIAL_REF) after ``make -C oracle ref``:
+Run with AERIAL_REF naming the reference tree, after ``make -C oracle ref
+REF=<that tree>``:
 
     python tests/golden/make_golden.py            # CPU fixtures
     python tests/golden/make_golden.py --gpu      # + outputs of the reference's
@@ -38,7 +38,14 @@ ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
-REF = os.environ.get("AERIAL_REF", "/root/reference")
+REF = os.environ.get("AERIAL_REF", "")
+
+
+def require_ref():
+    """The reference tree the fixtures are generated from (AERIAL_REF)."""
+    if not REF or not os.path.isdir(os.path.join(REF, "src")):
+        sys.exit("make_golden.py: set AERIAL_REF to the reference tree (the directory holding src/ and results/)")
+    return REF
 REFLIB = os.path.join(ROOT, "oracle", "_ref")
 VP = ctypes.c_void_p
 CI = ctypes.c_int
@@ -53,6 +60,7 @@ SRS_CFGS = [(24, 4, 8), (24, 2, 8), (12, 4, 12), (12, 2, 12)]
 
 
 def cpu_fixtures():
+    require_ref()
     lib = ctypes.CDLL(os.path.join(REFLIB, "libref_llr_v3.so"))
     lib.ref_llr_v3_cpu_ref.argtypes = [VP, VP, VP, CI, CI]
     N = 139392
