@@ -429,8 +429,12 @@ def main():
     if rank == 0 and world == 1 and not a.no_extras:
         extras = bench_extras(aeq, wl, cells, llrs, descs, tun, stream, a)
         if a.config == 2:
-            extras["path_rates"] = path_rates(aeq, descs, res_per_step, bytes_per_step, stream)
-            extras["other_configs"] = other_configs(aeq, wl, dev, stream, a)
+            for key, fn in (("path_rates", lambda: path_rates(aeq, descs, res_per_step, bytes_per_step, stream)),
+                            ("other_configs", lambda: other_configs(aeq, wl, dev, stream, a))):
+                try:   # reported beside the headline; never fatal for the timing line
+                    extras[key] = fn()
+                except Exception as e:
+                    extras[key] = {"error": f"{type(e).__name__}: {e}"}
         if a.config == 4:
             extras["tiles"] = compare_tiles(aeq, descs, tun, stream, a, flush)
             extras["per_cell_streams_vs_batched"] = compare_streams(aeq, descs, tun, a, flush)
