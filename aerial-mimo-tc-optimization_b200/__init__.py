@@ -326,10 +326,11 @@ def _cells_array(cells):
     return arr, n
 
 
-def make_tuning(precision=PREC_FP16, warps_per_cta=0, ctas_per_sm=0) -> Tuning:
+def make_tuning(precision=PREC_FP16, warps_per_cta=0, ctas_per_sm=0, sc_per_group=0) -> Tuning:
+    """Operand precision, launch shape and group cap (0 = default for each)."""
     if isinstance(precision, str):
         precision = PREC_NAMES[precision]
-    return Tuning(int(precision), int(warps_per_cta), int(ctas_per_sm), 0)
+    return Tuning(int(precision), int(warps_per_cta), int(ctas_per_sm), int(sc_per_group))
 
 
 def pusch_eq_fused(cells, tuning: Tuning | None = None, stream=None):
@@ -403,7 +404,7 @@ def pusch_eq_host(cells, workspace, tuning: Tuning | None = None, cells_per_batc
 
 
 def autotune(cells, precision=PREC_FP16, stream=None):
-    """Pick the fastest launch shape for these cells; returns (Tuning, microseconds)."""
+    """Pick the fastest group cap and launch shape for these cells; returns (Tuning, microseconds)."""
     arr, n = _cells_array(cells)
     t = make_tuning(precision)
     us = ctypes.c_float(0.0)

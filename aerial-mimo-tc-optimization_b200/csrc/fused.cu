@@ -33,16 +33,13 @@ namespace aeq {
 
 constexpr int kMaxCells = AERIAL_MAX_CELLS;
 
-// Subcarriers per group: 32 / LT fills every lane of the solve, but for the
-// 1-, 2- and 4-layer tiles that makes one warp's operand pass over a group
-// 32, 16 or 8 subcarriers long, and a small uneven batch then waits on those
-// few long groups.  Capping the group at 4 keeps groups short (the uneven
-// 16-cell batch: 90 -> 74 us; large batches unchanged); the idle solve lanes
-// cost little at those tile sizes.
-#ifndef AEQ_MAX_GROUP_SC
-#define AEQ_MAX_GROUP_SC 4
-#endif
-constexpr int kMaxGroupSC = AEQ_MAX_GROUP_SC;
+// Subcarriers per group: GS = min(32 / LT, cap).  32 / LT fills every lane
+// of the FP32 solve and of the LLR epilogue (LT lanes per subcarrier); a
+// smaller cap shortens each group's operand pass (GS x chunks items), which
+// an uneven batch needs so that no warp is left with a few long groups.  The
+// default 8 fills every lane for tiles of 4 layers and more; the cap is a
+// tuning parameter (aerial_tuning.sc_per_group, searched by the autotuner).
+constexpr int kDefaultGroupCap = 8;
 
 struct FusedCell {
     const float2* H;
@@ -53,7 +50,7 @@ struct FusedCell {
     float sigma2;    // noise variance in the units the kernel sees (times scale^2)
     float scale;     // power-of-two operand scale (FP16 operands), else 1
     int nSC, A, L, nSym, nPam, LT, vecY, vecH, lgHalfL;
-    int GS;          // subcarriers per group = min(32 / LT, kMaxGroupSC)
+    int GS;          // subcarriers per group = min(32 / LT, group cap)
     int nChunk;      // 16-antenna chunks per subcarrier
     int hrs;         // staged channel-row stride (bytes)
     PamLut lut;
@@ -69,49 +66,9 @@ struct FusedParams {
     int exactChunks; // with an exact tile: every cell has nAnt == 16 * exactChunks (2, 4, 8), else 0
     int fmt;         // AERIAL_FMT_* shared by every cell
     int scaled;      // some cell's FP16 operands are scaled (selects the kernel)
+    int halfMixed;   // complex-half cells in a mixed batch (fused_eq_kernel_hg)
     long totalGroups;
 };
-
-// ---------------------------------------------------------------------------
-// operand packing
-// ---------------------------------------------------------------------------
-template <int P>
-__device__ __forceinline__ uint32_t pack2(float re, float im) {
-    if constexpr (P == AERIAL_PREC_FP16) {
-        __half2 h = __floats2half2_rn(re, im);
-        return *reinterpret_cast<uint32_t*>(&h);
-    } else {
-        __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
-        return *reinterpret_cast<uint32_t*>(&h);
-    }
-}
-// (re, im) -> (-im, re): swap the halves and flip the sign bit of the new low half.
-__device__ __forceinline__ uint32_t jrot(uint32_t p) { return __byte_perm(p, 0, 0x1032) ^ 0x8000u; }
-
-// bf16 hi/lo split of a complex pair: x = hi + lo to ~16 mantissa bits.
-__device__ __forceinline__ void split_bf16(float re, float im, uint32_t& hi, uint32_t& lo) {
-    __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
-    float2 hf = __bfloat1622float2(h);
-    __nv_bfloat162 l = __floats2bfloat162_rn(re - hf.x, im - hf.y);
-    hi = *reinterpret_cast<uint32_t*>(&h);
-    lo = *reinterpret_cast<uint32_t*>(&l);
-}
-// fp16 hi/lo split: x = hi + lo to ~22 significant bits, for operands the
-// host has normalized (set_operand_scale) so that lo stays a normal half.
-__device__ __forceinline__ void split_fp16(float re, float im, uint32_t& hi, uint32_t& lo) {
-    __half2 h = __floats2half2_rn(re, im);
-    float2 hf = __half22float2(h);
-    __half2 l = __floats2half2_rn(re - hf.x, im - hf.y);
-    hi = *reinterpret_cast<uint32_t*>(&h);
-    lo = *reinterpret_cast<uint32_t*>(&l);
-}
-template <int P>
-__device__ __forceinline__ void split2(float re, float im, uint32_t& hi, uint32_t& lo) {
-    if constexpr (P == AERIAL_PREC_FP16X3)
-        split_fp16(re, im, hi, lo);
-    else
-        split_bf16(re, im, hi, lo);
-}
 
 // Packed FP32 pairs (fma.rn.f32x2 and friends, two IEEE operations per
 // instruction on sm_100a).
@@ -140,6 +97,54 @@ __device__ __forceinline__ float4 scale4(float4 v, unsigned long long ss) {
     const float2 a = upk2(mul2(pk2(v.x, v.y), ss));
     const float2 b = upk2(mul2(pk2(v.z, v.w), ss));
     return make_float4(a.x, a.y, b.x, b.y);
+}
+
+// ---------------------------------------------------------------------------
+// operand packing
+// ---------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ uint32_t pack2(float re, float im) {
+    if constexpr (P == AERIAL_PREC_FP16) {
+        __half2 h = __floats2half2_rn(re, im);
+        return *reinterpret_cast<uint32_t*>(&h);
+    } else {
+        __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+}
+// (re, im) -> (-im, re): swap the halves and flip the sign bit of the new low half.
+__device__ __forceinline__ uint32_t jrot(uint32_t p) { return __byte_perm(p, 0, 0x1032) ^ 0x8000u; }
+
+// (x.re, x.im) - (h.re, h.im) as one packed FP32 subtraction (exact here:
+// h is x rounded to fewer bits).
+__device__ __forceinline__ float2 sub2(float re, float im, float2 h) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(re, im)), "l"(pk2(h.x, h.y)));
+    return upk2(d);
+}
+// bf16 hi/lo split of a complex pair: x = hi + lo to ~16 mantissa bits.
+__device__ __forceinline__ void split_bf16(float re, float im, uint32_t& hi, uint32_t& lo) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
+    const float2 r = sub2(re, im, __bfloat1622float2(h));
+    __nv_bfloat162 l = __floats2bfloat162_rn(r.x, r.y);
+    hi = *reinterpret_cast<uint32_t*>(&h);
+    lo = *reinterpret_cast<uint32_t*>(&l);
+}
+// fp16 hi/lo split: x = hi + lo to ~22 significant bits, for operands the
+// host has normalized (set_operand_scale) so that lo stays a normal half.
+__device__ __forceinline__ void split_fp16(float re, float im, uint32_t& hi, uint32_t& lo) {
+    __half2 h = __floats2half2_rn(re, im);
+    const float2 r = sub2(re, im, __half22float2(h));
+    __half2 l = __floats2half2_rn(r.x, r.y);
+    hi = *reinterpret_cast<uint32_t*>(&h);
+    lo = *reinterpret_cast<uint32_t*>(&l);
+}
+template <int P>
+__device__ __forceinline__ void split2(float re, float im, uint32_t& hi, uint32_t& lo) {
+    if constexpr (P == AERIAL_PREC_FP16X3)
+        split_fp16(re, im, hi, lo);
+    else
+        split_bf16(re, im, hi, lo);
 }
 
 template <int P>
@@ -821,6 +826,11 @@ __device__ __forceinline__ int group_valid(const FusedCell& cl, long grp) {
     return (int)min((long)cl.GS, (long)cl.nSC - (grp - cl.group0) * cl.GS);
 }
 
+// Group of round r of warp gw in the snake walk (see fused_eq_kernel).
+__device__ __forceinline__ long snake_group(int r, long gw, long nw) {
+    return (long)r * nw + ((r & 1) ? nw - 1 - gw : gw);
+}
+
 // LTF = 0: any mix of cells.  LTF in {2, 4, 8, 16}: every cell has
 // nLayers == LTF and 16-byte aligned H / Y_rx (the host checks), so the layer
 // tile, strides and masks are compile-time constants.
@@ -842,6 +852,11 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     const long nw = (long)gridDim.x * warpsPerCta;
     const long total = p.totalGroups;
     if (gw >= total) return;
+    // Snake walk: in round r this warp takes group r nw + gw (r even) or
+    // r nw + nw - 1 - gw (r odd).  The host orders cells by group cost, most
+    // expensive first, so each warp's rounds pair an expensive group with a
+    // cheap one and the warps of an uneven batch finish together.
+    int pr = 0, cr = 0;
 
     // ---- producer cursor (registers): group, cell, subcarrier, chunk ----
     // Per-lane staging offsets are fixed for the whole launch (exact tile) or
@@ -917,7 +932,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
                     pys += pYsc;
                 } else {
                     pq = 0;
-                    pg += nw;
+                    pg = snake_group(++pr, gw, nw);
                     if (pg < total) {
                         while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
                         load_pcell();
@@ -1047,7 +1062,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
             }
         }
         q = 0;
-        grp += nw;
+        grp = snake_group(++cr, gw, nw);
         if (grp >= total) break;
         while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
         load_ccell();
@@ -1235,7 +1250,8 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_a(const __grid_constan
 // (16 antennas) whose 8-byte antenna-pair granules are XOR-swizzled by
 // (sym & 2) << 1; both make every fragment read of a warp conflict-free.
 // ---------------------------------------------------------------------------
-__host__ __device__ constexpr int hrs16_of(int L) { return L == 16 ? 80 : L == 8 ? 48 : 16; }
+// (2 layers: 8-byte rows, contiguous, so one 16-byte copy stages two rows)
+__host__ __device__ constexpr int hrs16_of(int L) { return L == 16 ? 80 : L == 8 ? 48 : L == 4 ? 16 : 8; }
 
 struct ScPtrH {
     const char* h;   // the lane's channel piece of the subcarrier's first chunk
@@ -1429,6 +1445,187 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_h(const __grid_constan
 }
 
 // ---------------------------------------------------------------------------
+// FP16 I/O for a mixed batch: any mix of complex-half cells whose layers fill
+// their tile (2, 4, 8 or 16) and whose antenna counts are multiples of 16.
+// Staging, fragment reads and epilogue are fused_eq_kernel_h's per cell (the
+// layer tile by switch, the chunk count at run time); the work walk is the
+// mixed-batch kernel's snake order over cost-sorted cells.
+// ---------------------------------------------------------------------------
+// Chunk j of one subcarrier: h / y are the lane's pieces of its first chunk.
+template <int LF>
+__device__ __forceinline__ void stage_chunk_hr(uint32_t st, uint32_t hLaneS, uint32_t yLaneS, const char* h,
+                                               const char* y, int yk, int j, int A, int lane) {
+    constexpr int NP = CHUNK * LF / 4;                 // 16-byte channel pieces per chunk
+    if (NP >= 32 || lane < NP) cp_async16(st + hLaneS, h + j * CHUNK * LF * 4);
+    if (NP > 32) cp_async16(st + hLaneS + 8 * hrs16_of(LF), h + j * CHUNK * LF * 4 + 512);
+    if (yk > 0) cp_async16(st + yLaneS, y + j * 64);
+    if (yk > 1) cp_async16(st + yLaneS + 512, y + j * 64 + 8 * A * 4);
+}
+
+// The lane's channel-piece offset in a stage for layer tile LT.
+__host__ __device__ constexpr uint32_t h_lane_stage(int LT, int lane) {
+    return LT == 16 ? (lane >> 2) * hrs16_of(16) + (lane & 3) * 16
+         : LT == 8  ? (lane >> 1) * hrs16_of(8) + (lane & 1) * 16
+         : LT == 4  ? lane * hrs16_of(4)
+                    : lane * 16;                       // 2 layers: rows 2 lane, 2 lane + 1
+}
+
+__global__ void __launch_bounds__(256, 2) fused_eq_kernel_hg(const __grid_constant__ FusedParams p) {
+    constexpr int NST = 2;
+    extern __shared__ float4 smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int warpsPerCta = blockDim.x >> 5;
+    const int g = lane >> 2, c = lane & 3;
+    const int warpBytes = p.epiBytes + NST * p.stageBytes;
+    const int smemOff = wib * (warpBytes / 8);
+    float2* sm = reinterpret_cast<float2*>(smem_raw) + smemOff;
+    const uint32_t stBase =
+        (uint32_t)__cvta_generic_to_shared(reinterpret_cast<char*>(smem_raw) + (long)wib * warpBytes + p.epiBytes);
+    const long gw = (long)blockIdx.x * warpsPerCta + wib;
+    const long nw = (long)gridDim.x * warpsPerCta;
+    const long total = p.totalGroups;
+    if (gw >= total) return;
+    const int s0 = lane >> 2, q4 = lane & 3;
+
+    // ---- producer cursor: group (snake walk), cell, subcarrier, chunk ----
+    long pg = gw;
+    int pr = 0, pci = 0;
+    while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
+    int pq = 0, pch = 0, pslot = 0, pValid, pNCh, pLT, pYk, pA, pHscB, pYscB;
+    uint32_t pHLaneS, pYLaneS;
+    const char* ph;
+    const char* py;
+    auto load_pcell = [&]() {
+        const FusedCell& cl = p.cell[pci];
+        const int hrs = hrs16_of(cl.L);
+        pValid = group_valid(cl, pg);
+        pLT = cl.LT;
+        pA = cl.A;
+        pNCh = cl.nChunk;
+        pHscB = cl.A * cl.L * 4;
+        pYscB = cl.nSym * cl.A * 4;
+        const long sc = (pg - cl.group0) * cl.GS;
+        ph = reinterpret_cast<const char*>(cl.H) + sc * pHscB + 16 * lane;
+        py = reinterpret_cast<const char*>(cl.Y) + sc * pYscB + (s0 * cl.A + 4 * q4) * 4;
+        pYk = (s0 < cl.nSym ? 1 : 0) + (s0 + 8 < cl.nSym ? 1 : 0);
+        pHLaneS = h_lane_stage(pLT, lane);
+        pYLaneS = CHUNK * hrs + s0 * 64 + ((q4 ^ (((s0 >> 1) & 1) << 1)) << 4);
+    };
+    load_pcell();
+    auto produce = [&]() {
+        if (pg < total) {
+            const uint32_t st = stBase + pslot * p.stageBytes;
+            switch (pLT) {
+                case 2: stage_chunk_hr<2>(st, pHLaneS, pYLaneS, ph, py, pYk, pch, pA, lane); break;
+                case 4: stage_chunk_hr<4>(st, pHLaneS, pYLaneS, ph, py, pYk, pch, pA, lane); break;
+                case 8: stage_chunk_hr<8>(st, pHLaneS, pYLaneS, ph, py, pYk, pch, pA, lane); break;
+                default: stage_chunk_hr<16>(st, pHLaneS, pYLaneS, ph, py, pYk, pch, pA, lane); break;
+            }
+            if (++pch == pNCh) {
+                pch = 0;
+                if (++pq < pValid) {
+                    ph += pHscB;
+                    py += pYscB;
+                } else {
+                    pq = 0;
+                    pg = snake_group(++pr, gw, nw);
+                    if (pg < total) {
+                        while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
+                        load_pcell();
+                    }
+                }
+            }
+        }
+        cp_async_commit();
+        pslot = pslot == NST - 1 ? 0 : pslot + 1;
+    };
+    produce();
+
+    // ---- consumer ----
+    long grp = gw;
+    int cr = 0, ci = 0;
+    while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+    int q = 0, ch = 0, cslot = 0, nValid, cNCh, cLT;
+    bool z2;
+    uint32_t yo[2][2], hoff;
+    auto load_ccell = [&]() {
+        const FusedCell& cl = p.cell[ci];
+        const int hrs = hrs16_of(cl.L);
+        nValid = group_valid(cl, grp);
+        cNCh = cl.nChunk;
+        cLT = cl.LT;
+        z2 = cl.nSym > 8;
+        hoff = 2 * c * hrs + 4 * g;
+#pragma unroll
+        for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) {
+                const int r = 8 * nt + g;
+                const int ra = r < cl.nSym ? r : 0;      // rows past nSym are not staged: read row 0 instead
+                yo[kk][nt] = CHUNK * hrs + ra * 64 + (((4 * kk + c) ^ ((ra & 2) << 1)) << 3);
+            }
+    };
+    load_ccell();
+    float gacc[3][4], zacc[2][2][4];
+    auto clear_acc = [&]() {
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) gacc[b][e] = 0.f;
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
+    };
+    clear_acc();
+    while (true) {
+        __syncwarp();                              // every lane is done with the slot refilled now
+        produce();
+        cp_async_wait<NST - 1>();                  // this chunk's copies (own lane) have landed
+        __syncwarp();                              // ... and every lane's
+        const uint32_t st = stBase + cslot * p.stageBytes;
+        cslot = cslot == NST - 1 ? 0 : cslot + 1;
+        switch (cLT) {
+            case 2: mma_stage_h<2>(st, st + hoff, yo, gacc, zacc, z2); break;
+            case 4: mma_stage_h<4>(st, st + hoff, yo, gacc, zacc, z2); break;
+            case 8: mma_stage_h<8>(st, st + hoff, yo, gacc, zacc, z2); break;
+            default: mma_stage_h<16>(st, st + hoff, yo, gacc, zacc, z2); break;
+        }
+        if (++ch < cNCh) continue;
+        ch = 0;
+        switch (cLT) {
+            case 2: store_acc<2>(sm, gacc, zacc, q, g, c); break;
+            case 4: store_acc<4>(sm, gacc, zacc, q, g, c); break;
+            case 8: store_acc<8>(sm, gacc, zacc, q, g, c); break;
+            default: store_acc<16>(sm, gacc, zacc, q, g, c); break;
+        }
+        clear_acc();
+        if (++q < nValid) continue;
+        __syncwarp();
+        {
+            const FusedCell& cl = p.cell[ci];
+            const CellView v = view_of(cl);
+            const long sc0 = (grp - cl.group0) * cl.GS;
+            switch (cLT) {
+                case 2: solve_group<2, AERIAL_PREC_FP16, true>(v, sc0, nValid, smemOff, lane); break;
+                case 4: solve_group<4, AERIAL_PREC_FP16, true>(v, sc0, nValid, smemOff, lane); break;
+                case 8: solve_group<8, AERIAL_PREC_FP16, true>(v, sc0, nValid, smemOff, lane); break;
+                default: solve_group<16, AERIAL_PREC_FP16, true>(v, sc0, nValid, smemOff, lane); break;
+            }
+        }
+        q = 0;
+        grp = snake_group(++cr, gw, nw);
+        if (grp >= total) break;
+        while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
+        load_ccell();
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 static int layer_tile(int L) {
@@ -1473,12 +1670,60 @@ extern "C" float aerial_fp16_operand_scale(float sigma2) {
 
 namespace aeq {
 
+// Estimated cost of one full group of a cell, in rough warp-instruction
+// units from the kernel's structure: the operand phase of GS subcarriers
+// (per 16-antenna chunk: staging, fragment reads and conversions, MMAs; the
+// 16-layer tile has two m-tiles) and the group's epilogue (FP32 solve, then
+// X = G^-1 Z, unbiasing and demapper with one lane per layer row).  Only the
+// order it induces matters (set_groups).
+static long group_cost_of(const FusedCell& c) {
+    const int nmt = c.LT > 8 ? 2 : 1;
+    const long operand = (long)c.GS * c.nChunk * (24 + 26 * nmt);
+    const long solve = c.LT * (c.LT / 2 + 2 * c.LT + 12);
+    const long emit = (long)((c.nSym + 1) / 2) * (5 * c.LT + 4 * (3 * c.nPam + 4));
+    return operand + solve + emit;
+}
+
+// Group size of every cell (min(32 / LT, cap)) and the first group index of
+// each.  Cells are ordered by group cost, most expensive first (stable, so
+// equal shapes keep their order and a parameter block built again from the
+// same cells comes out identical): with the mixed-batch kernels' snake walk
+// over the groups this spreads an uneven batch evenly over the warps.  A
+// cell's outputs do not depend on its position.
+void set_groups(FusedParams& p, int cap) {
+    if (cap < 1) cap = kDefaultGroupCap;
+    long cost[AERIAL_MAX_CELLS];
+    for (int i = 0; i < p.nCells; i++) {
+        FusedCell& f = p.cell[i];
+        f.GS = 32 / f.LT < cap ? 32 / f.LT : cap;
+        cost[i] = group_cost_of(f);
+    }
+    for (int i = 1; i < p.nCells; i++) {          // insertion sort, descending, stable
+        const FusedCell f = p.cell[i];
+        const long cf = cost[i];
+        int j = i - 1;
+        while (j >= 0 && cost[j] < cf) {
+            p.cell[j + 1] = p.cell[j];
+            cost[j + 1] = cost[j];
+            j--;
+        }
+        p.cell[j + 1] = f;
+        cost[j + 1] = cf;
+    }
+    long g0 = 0;
+    for (int i = 0; i < p.nCells; i++) {
+        FusedCell& f = p.cell[i];
+        f.group0 = g0;
+        g0 += (f.nSC + f.GS - 1) / f.GS;
+    }
+    p.totalGroups = g0;
+}
+
 // warpBytes: the per-warp shared memory of the launch (epilogue region of the
 // largest layer-tile footprint present, which is not monotonic in the tile,
 // plus the kernel's operand stages).
 int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p, int& warpBytes) {
     if (!cells || nCells < 1 || nCells > kMaxCells) return AERIAL_ERR_INVALID_ARG;
-    long g0 = 0;
     warpBytes = 0;
     for (int i = 0; i < nCells; i++) {
         const aerial_cell_desc& c = cells[i];
@@ -1510,17 +1755,14 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
             f.lgHalfL = (half > 0 && (half & (half - 1)) == 0) ? __builtin_ctz(half) : -1;
         }
         f.lut = pam_lut(c.nPamBits);
-        f.group0 = g0;
-        f.GS = 32 / f.LT < kMaxGroupSC ? 32 / f.LT : kMaxGroupSC;
         f.nChunk = (c.nAnt + CHUNK - 1) / CHUNK;
         f.hrs = hrs_of(c.nLayers);
         // LLR rows of 2*nPam floats are written as float4 for nPam 2/4: need 16 B alignment
         if ((c.nPamBits == 2 || c.nPamBits == 4) && ((uintptr_t)c.llr & 15)) return AERIAL_ERR_INVALID_ARG;
-        g0 += (nSC + f.GS - 1) / f.GS;
     }
     p.nCells = nCells;
     p.scaled = 0;
-    p.totalGroups = g0;
+    set_groups(p, kDefaultGroupCap);
     p.fmt = cells[0].format;
     for (int i = 0; i < nCells; i++)
         if (cells[i].format != p.fmt || (p.fmt != AERIAL_FMT_CF32 && p.fmt != AERIAL_FMT_CF16))
@@ -1537,17 +1779,29 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
         for (int i = 1; i < nCells && same; i++) same = p.cell[i].A == a;
         if (same) p.exactChunks = a / CHUNK;
     }
+    p.halfMixed = 0;
     if (p.fmt == AERIAL_FMT_CF16) {
-        // half-format cells run the FP16 I/O kernel: exact 4-, 8- or 16-layer
-        // tile, 32 / 64 / 128 antennas, 16-byte aligned H and Y_rx
+        // half-format cells run an FP16 I/O kernel: a uniform batch of exact
+        // 4-, 8- or 16-layer tiles with 32 / 64 / 128 antennas takes the
+        // unrolled one; any other mix whose cells fill 2-, 4-, 8- or 16-layer
+        // tiles with a multiple of 16 antennas takes the mixed-batch one.
+        // H and Y_rx must be 16-byte aligned.
         if (p.exactTile == 16) {
             const int a = p.cell[0].A;
             bool same = a == 32 || a == 64 || a == 128;
             for (int i = 1; i < nCells && same; i++) same = p.cell[i].A == a;
             p.exactChunks = same ? a / CHUNK : 0;
         }
-        if ((p.exactTile != 4 && p.exactTile != 8 && p.exactTile != 16) || !p.exactChunks)
-            return AERIAL_ERR_UNSUPPORTED;
+        if ((p.exactTile != 4 && p.exactTile != 8 && p.exactTile != 16) || !p.exactChunks) {
+            for (int i = 0; i < nCells; i++) {
+                const FusedCell& f = p.cell[i];
+                if (f.L != f.LT || f.LT < 2 || f.A % CHUNK || ((uintptr_t)f.H & 15) || ((uintptr_t)f.Y & 15))
+                    return AERIAL_ERR_UNSUPPORTED;
+            }
+            p.halfMixed = 1;
+            p.exactTile = 0;
+            p.exactChunks = 0;
+        }
         int b = 0;
         for (int i = 0; i < nCells; i++) {
             const int v = CHUNK * hrs16_of(p.cell[i].L) + 64 * p.cell[i].nSym;
@@ -1694,6 +1948,12 @@ template <int P, bool SC>
 static int plan_p(const FusedParams& p, int warpBytes, LaunchShape sh, LaunchPlan& out) {
     if (p.fmt == AERIAL_FMT_CF16) {
         if (P != AERIAL_PREC_FP16) return AERIAL_ERR_UNSUPPORTED;
+        if (p.halfMixed) {
+            const int s = allow_max_smem<fused_eq_kernel_hg>();
+            if (s) return s;
+            fill_plan(reinterpret_cast<const void*>(fused_eq_kernel_hg), p, warpBytes, sh, out);
+            return AERIAL_OK;
+        }
         return p.exactTile == 4   ? plan_hn<4>(p, warpBytes, sh, out)
              : p.exactTile == 8   ? plan_hn<8>(p, warpBytes, sh, out)
                                   : plan_hn<16>(p, warpBytes, sh, out);
@@ -1743,11 +2003,13 @@ int launch_fused(const FusedParams& p, int warpBytes, int prec, LaunchShape sh, 
 // A shape tuned on one batch may be applied to another whose cells need more
 // shared memory per warp (a host-pipeline sub-batch, say): its CTAs per SM
 // are then reduced to what fits instead of failing the launch.
-static void resolve_tuning(const aerial_tuning* tuning, int warpBytes, int& prec, LaunchShape& sh) {
+static void resolve_tuning(const aerial_tuning* tuning, int warpBytes, int& prec, LaunchShape& sh, int& gsCap) {
     sh = default_shape(warpBytes);
     prec = AERIAL_PREC_FP16;
+    gsCap = kDefaultGroupCap;
     if (tuning) {
         prec = tuning->precision;
+        if (tuning->sc_per_group > 0) gsCap = tuning->sc_per_group;
         if (tuning->warps_per_cta) sh.warps = tuning->warps_per_cta;
         if (tuning->ctas_per_sm) sh.ctasPerSm = tuning->ctas_per_sm;
         if (sh.warps >= 1 && sh.ctasPerSm > 1 && (long)sh.warps * warpBytes * sh.ctasPerSm > kSmemPerSm) {
@@ -1768,44 +2030,60 @@ extern "C" int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, 
     int s = build_fused_params(cells, nCells, p, warpBytes);
     if (s) return s;
     LaunchShape sh;
-    int prec;
-    resolve_tuning(tuning, warpBytes, prec, sh);
+    int prec, gsCap;
+    resolve_tuning(tuning, warpBytes, prec, sh, gsCap);
+    if (gsCap != kDefaultGroupCap) set_groups(p, gsCap);
     set_operand_scale(p, prec);
     return launch_fused(p, warpBytes, prec, sh, to_stream(stream));
 }
 
 // ---------------------------------------------------------------------------
-// Autotuner: time each candidate launch shape on the caller's cells and keep
-// the fastest.  Candidates are (warps per CTA, CTAs per SM) pairs whose
-// shared memory fits one SM; each is timed with CUDA events over a few
-// launches after one warm-up launch.
+// Autotuner: time each candidate tile and launch shape on the caller's cells
+// and keep the fastest.  Candidates are the group cap (subcarriers solved
+// together per warp: 8, 32 or 4, for batches with tiles of 4 layers or fewer,
+// where the cap changes anything) crossed with (warps per CTA, CTAs per SM)
+// pairs whose shared memory fits one SM; each is timed with CUDA events over
+// a few launches after one warm-up launch.  The reference's analogue is its
+// templated shape sweep over antennas and symbols (src/coef_scaling.cu:221-250).
 // ---------------------------------------------------------------------------
 extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial_tuning* best, float* bestUs,
                                void* stream) {
     if (!best) return AERIAL_ERR_INVALID_ARG;
-    FusedParams p;
+    FusedParams base, p;
     int warpBytes = 0;
-    int s = build_fused_params(cells, nCells, p, warpBytes);
+    int s = build_fused_params(cells, nCells, base, warpBytes);
     if (s) return s;
     cudaStream_t st = to_stream(stream);
     const int prec = best->precision;
-    set_operand_scale(p, prec);
-    LaunchShape cand[16];
+    struct Cand {
+        LaunchShape sh;
+        int cap;
+    };
+    int caps[3] = {kDefaultGroupCap, 0, 0}, nCaps = 1;
+    bool smallTile = false;
+    for (int i = 0; i < base.nCells; i++) smallTile |= base.cell[i].LT <= 4;
+    if (smallTile) {
+        caps[nCaps++] = 32;
+        caps[nCaps++] = 4;
+    }
+    Cand cand[48];
     int nc = 0;
-    for (int w : {2, 3, 4, 6, 8}) {
-        const int k = max_ctas(w, warpBytes);
-        if (k >= 1) cand[nc++] = {w, k};
-        if (k >= 2) cand[nc++] = {w, k - 1};
+    const LaunchShape def = default_shape(warpBytes);
+    for (int ic = 0; ic < nCaps; ic++) {
+        bool hasDef = false;
+        for (int w : {2, 3, 4, 6, 8}) {
+            const int k = max_ctas(w, warpBytes);
+            if (k >= 1) cand[nc++] = {{w, k}, caps[ic]};
+            if (k >= 2) cand[nc++] = {{w, k - 1}, caps[ic]};
+            hasDef |= w == def.warps && ((k >= 1 && k == def.ctasPerSm) || (k >= 2 && k - 1 == def.ctasPerSm));
+        }
+        if (!hasDef) cand[nc++] = {def, caps[ic]};
     }
     // Rounds interleave the candidates so clock drift under the power cap
     // hits all of them alike; a candidate's time is its best round.  Within
     // 2 % of the fastest, the shape with more resident warps wins (it holds
-    // more operand copies in flight once clocks settle).
-    const LaunchShape def = default_shape(warpBytes);
-    bool hasDef = false;
-    for (int ic = 0; ic < nc; ic++) hasDef |= cand[ic].warps == def.warps && cand[ic].ctasPerSm == def.ctasPerSm;
-    if (!hasDef && nc < 16) cand[nc++] = def;
-    float t[16];
+    // more operand copies in flight once clocks settle), then the default cap.
+    float t[48];
     for (int ic = 0; ic < nc; ic++) t[ic] = 1e30f;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -1813,7 +2091,10 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
     const int rounds = 3, reps = 8;
     for (int rd = 0; rd < rounds && !s; rd++) {
         for (int ic = 0; ic < nc && !s; ic++) {
-            const LaunchShape& sh = cand[ic];
+            const LaunchShape& sh = cand[ic].sh;
+            p = base;                                // unscaled sigma2, default groups
+            set_groups(p, cand[ic].cap);
+            set_operand_scale(p, prec);
             if ((s = launch_fused(p, warpBytes, prec, sh, st))) break;
             cudaEventRecord(e0, st);
             for (int r = 0; r < reps && !s; r++) s = launch_fused(p, warpBytes, prec, sh, st);
@@ -1832,24 +2113,27 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
     }
     float fastest = 1e30f;
     for (int ic = 0; ic < nc; ic++) fastest = t[ic] < fastest ? t[ic] : fastest;
-    LaunchShape bestS = def;
+    Cand bestC{def, kDefaultGroupCap};
     float bestT = 1e30f;
     int bestWarps = -1;
     for (int ic = 0; ic < nc; ic++) {
         if (t[ic] > fastest * 1.02f) continue;
-        const int w = cand[ic].warps * cand[ic].ctasPerSm;
-        if (w > bestWarps || (w == bestWarps && t[ic] < bestT)) {
+        const int w = cand[ic].sh.warps * cand[ic].sh.ctasPerSm;
+        const bool better = w > bestWarps ||
+                            (w == bestWarps && cand[ic].cap == kDefaultGroupCap && bestC.cap != kDefaultGroupCap) ||
+                            (w == bestWarps && cand[ic].cap == bestC.cap && t[ic] < bestT);
+        if (better) {
             bestWarps = w;
             bestT = t[ic];
-            bestS = cand[ic];
+            bestC = cand[ic];
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (s) return s;
-    best->warps_per_cta = bestS.warps;
-    best->ctas_per_sm = bestS.ctasPerSm;
-    best->sc_per_group = 0;
+    best->warps_per_cta = bestC.sh.warps;
+    best->ctas_per_sm = bestC.sh.ctasPerSm;
+    best->sc_per_group = bestC.cap;
     if (bestUs) *bestUs = bestT * 1000.f;
     return AERIAL_OK;
 }
@@ -1869,6 +2153,7 @@ struct aerial_eq_graph {
     LaunchPlan plan;
     int prec = AERIAL_PREC_FP16;
     LaunchShape shape{};
+    int gsCap = kDefaultGroupCap;
 };
 
 static cudaKernelNodeParams node_params(aerial_eq_graph* g, void** args) {
@@ -1890,7 +2175,8 @@ extern "C" int aerial_eq_graph_create(const aerial_cell_desc* cells, int nCells,
     int warpBytes = 0;
     int s = build_fused_params(cells, nCells, g->params, warpBytes);
     if (!s) {
-        resolve_tuning(tuning, warpBytes, g->prec, g->shape);
+        resolve_tuning(tuning, warpBytes, g->prec, g->shape, g->gsCap);
+        if (g->gsCap != kDefaultGroupCap) set_groups(g->params, g->gsCap);
         set_operand_scale(g->params, g->prec);
         s = plan_fused(g->params, warpBytes, g->prec, g->shape, g->plan);
     }
@@ -1928,6 +2214,7 @@ extern "C" int aerial_eq_graph_update(aerial_eq_graph* g, const aerial_cell_desc
     // The new noise levels may move a cell in or out of FP16 operand scaling,
     // which selects another kernel instantiation: re-plan the node (an
     // executable graph's kernel node may change its function).
+    if (g->gsCap != kDefaultGroupCap) set_groups(np, g->gsCap);
     set_operand_scale(np, g->prec);
     LaunchPlan pl;
     s = plan_fused(np, warpBytes, g->prec, g->shape, pl);
@@ -2007,6 +2294,11 @@ static int prepare_p() {
 
 int prepare_fused_kernels() {
     int s = prepare_p<AERIAL_PREC_FP16>();
+    if (!s) {
+        cudaFuncAttributes at;
+        const cudaError_t e = cudaFuncGetAttributes(&at, fused_eq_kernel_hg);
+        s = e == cudaSuccess ? allow_max_smem<fused_eq_kernel_hg>() : rt_status(e);
+    }
     if (!s) s = prepare_p<AERIAL_PREC_FP16, true>();
     if (!s) s = prepare_h<4, 2>();
     if (!s) s = prepare_h<4, 4>();

@@ -196,10 +196,12 @@ int aerial_chest_interp_h(aerial_ch2* H, const aerial_ch2* Yp, const aerial_ch2*
  *                   -- the drop-in layout.
  *  AERIAL_FMT_CF16: H, Y_rx, Y_eq complex half (aerial_ch2), LLRs __half --
  *                   half the bytes; the LLR storage of the reference's
- *                   demapper (src/llr/aerial_llr_v3.cu:84-108).  Supported for
- *                   launches whose cells all have the same nLayers of 4, 8 or
- *                   16 and nAnt 32, 64 or 128, with FP16 operands (else
- *                   AERIAL_ERR_UNSUPPORTED). */
+ *                   demapper (src/llr/aerial_llr_v3.cu:84-108).  Supported,
+ *                   with FP16 operands, for any mix of cells whose nLayers is
+ *                   2, 4, 8 or 16 and whose nAnt is a multiple of 16, with
+ *                   16-byte aligned H and Y_rx (else AERIAL_ERR_UNSUPPORTED);
+ *                   uniform batches of 4, 8 or 16 layers and 32, 64 or 128
+ *                   antennas take an unrolled kernel. */
 enum { AERIAL_FMT_CF32 = 0, AERIAL_FMT_CF16 = 1 };
 
 /* One cell-slot.  nSC = 12 * nPRB.  Y_eq may be NULL.  Pointer types name
@@ -260,7 +262,10 @@ typedef struct {
     int precision;             /* AERIAL_PREC_* */
     int warps_per_cta;         /* 0 = default */
     int ctas_per_sm;           /* 0 = default */
-    int sc_per_group;          /* reserved, 0 */
+    int sc_per_group;          /* cap on the subcarriers a warp solves together
+                                  (min(32 / layer tile, cap)); 0 = default (8:
+                                  every lane of the solve busy for tiles of 4
+                                  layers and more) */
 } aerial_tuning;
 
 /* Equalize nCells cell-slots in ONE persistent launch (cells may differ in
@@ -433,8 +438,9 @@ int aerial_server_inject_alloc_failure(aerial_server* server, int nth);
 /* Autotuner                                                                  */
 /* ------------------------------------------------------------------------ */
 
-/* Time the fused kernel on `cells` for each candidate launch shape and
- * write the fastest into *best (precision is taken from *best on entry).
+/* Time the fused kernel on `cells` for each candidate group cap and launch
+ * shape and write the fastest into *best (precision is taken from *best on
+ * entry; sc_per_group, warps_per_cta and ctas_per_sm are written).
  * Runs synchronously on `stream`.  Returns the best time in microseconds via
  * *bestUs (may be NULL). */
 int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial_tuning* best, float* bestUs,

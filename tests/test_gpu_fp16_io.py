@@ -58,6 +58,32 @@ def test_fp16_io_equals_complex64_path_rounded(aeq, wl, cuda, L, A):
         assert torch.equal(y16, torch.view_as_real(y32).to(torch.float16))
 
 
+def test_fp16_io_mixed_batch_equals_complex64_path_rounded(aeq, wl, cuda):
+    """Mixed batches in FP16 I/O (the configuration 4 cells: 2-, 4- and
+    8-layer tiles with 16, 32 and 64 antennas, plus 48- and 256-antenna and
+    16-layer cells) take the mixed-batch FP16 I/O kernel; every cell equals
+    the complex64 path's result rounded to half, bit for bit."""
+    cells = wl.multicell(16, seed=77)
+    cells += [wl.make_cell(2, 48, 2, 11, 64, 18.0, seed=78), wl.make_cell(1, 16, 16, 9, 256, 28.0, seed=79),
+              wl.make_cell(1, 256, 4, 16, 4, 12.0, seed=80)]
+    for batch in (cells[:16], cells[16:], cells):
+        out32, out16 = run_pair(aeq, batch, cuda)
+        for (_, _, l32, y32), (_, _, l16, y16) in zip(out32, out16):
+            assert torch.isfinite(l16.float()).all()
+            assert torch.equal(l16, l32.to(torch.float16))
+            assert torch.equal(y16, torch.view_as_real(y32).to(torch.float16))
+
+
+def test_fp16_io_mixed_batch_alone_and_in_mix(aeq, wl, cuda):
+    """A half-format cell's results do not depend on the batch around it."""
+    cells = wl.multicell(16, seed=81)
+    _, mixed = run_pair(aeq, cells, cuda)
+    for i in (0, 7, 15):
+        _, alone = run_pair(aeq, [cells[i]], cuda)
+        assert torch.equal(alone[0][2], mixed[i][2])
+        assert torch.equal(alone[0][3], mixed[i][3])
+
+
 def test_fp16_io_vs_fp64(aeq, wl, orc, cuda):
     """The headline cell in FP16 I/O against the FP64 model of its own
     (half-rounded) inputs, at the FP16 bar."""
@@ -96,12 +122,14 @@ def test_fp16_io_unsupported_cases(aeq, wl, cuda):
         l16 = torch.empty(c.llr_numel, dtype=torch.float16, device=cuda)
         return (H16, Y16, l16), aeq.cell_desc(H16, Y16, l16, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits,
                                              fmt=fmt)
-    k1, d_l2 = desc(wl.make_cell(1, 32, 2, 11, 16, 20.0, seed=1))          # 2 layers
-    k2, d_a48 = desc(wl.make_cell(1, 48, 8, 11, 16, 20.0, seed=2))         # 48 antennas
+    k1, d_l3 = desc(wl.make_cell(1, 32, 3, 11, 16, 20.0, seed=1))          # 3 layers: not a full tile
+    k2, d_a40 = desc(wl.make_cell(1, 40, 8, 11, 16, 20.0, seed=2))         # 40 antennas: not 16k
     k3, d_ok = desc(wl.make_cell(1, 64, 8, 11, 16, 20.0, seed=3))
-    for d in (d_l2, d_a48):
+    for d in (d_l3, d_a40):
         with pytest.raises(aeq.AerialError):
             aeq.pusch_eq_fused([d], aeq.make_tuning("fp16"))
+        with pytest.raises(aeq.AerialError):                                # also inside a mixed batch
+            aeq.pusch_eq_fused([d_ok, d], aeq.make_tuning("fp16"))
     with pytest.raises(aeq.AerialError):                                    # FP16 operands only
         aeq.pusch_eq_fused([d_ok], aeq.make_tuning("bf16x3"))
     c = wl.make_cell(1, 64, 8, 11, 16, 20.0, seed=4)

@@ -176,6 +176,34 @@ def test_prb_range_split_equals_whole_cell(aeq, wl, cuda, cfg, n):
         np.testing.assert_array_equal(y_.cpu().numpy(), whole[1])
 
 
+@pytest.mark.parametrize("prec", ["fp16", "bf16x3"])
+def test_group_cap_does_not_change_results(aeq, wl, cuda, prec):
+    """The group cap (subcarriers a warp solves together, aerial_tuning.
+    sc_per_group) and the launch shape only regroup the work: every cell's
+    LLRs and Y_eq are bit-identical for caps 1, 4, 8 and 32 and for the
+    autotuner's choice, in an uneven batch that includes 1-, 2- and 3-layer
+    tiles (masked rows) and tail antennas."""
+    cells = wl.multicell(16, seed=27) + [wl.make_cell(2, 33, 1, 7, 4, 15.0, seed=28),
+                                         wl.make_cell(1, 20, 3, 13, 16, 22.0, seed=29)]
+    ref = run_fused(aeq, cells, cuda, prec)
+    for cap in (1, 4, 32):
+        got = run_fused(aeq, cells, cuda, tuning=aeq.make_tuning(prec, sc_per_group=cap))
+        for a, b in zip(ref, got):
+            np.testing.assert_array_equal(a[0], b[0])
+            np.testing.assert_array_equal(a[1], b[1])
+    descs, keep = [], []
+    for c in cells:
+        H, Y = c.H.to(cuda), c.Y.to(cuda)
+        l = torch.empty(c.llr_numel, dtype=torch.float32, device=cuda)
+        keep += [H, Y, l]
+        descs.append(aeq.cell_desc(H, Y, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits))
+    tuned, us = aeq.autotune(descs, prec)
+    assert tuned.sc_per_group in (4, 8, 32) and us > 0
+    got = run_fused(aeq, cells, cuda, tuning=tuned)
+    for a, b in zip(ref, got):
+        np.testing.assert_array_equal(a[0], b[0])
+
+
 def test_multicell_vs_fp64(aeq, wl, orc, cuda):
     cells = wl.multicell(16, seed=29)
     res = run_fused(aeq, cells, cuda, "fp16")
