@@ -7,9 +7,9 @@ Tolerances (stated per precision):
   LLR: max |LLR - LLR64| <= 2e-3 * max|LLR64| (relative to the LLR scale).
   Hard decisions: on full configuration 1 (20 dB) and 2 (25 dB) slots the
   number of sign flips against FP64 is asserted exactly per path, and every
-  flip must sit within that path's LLR error bound of zero
-  (test_hard_decisions_vs_fp64).  The FP16x3 path and the plain FP32 chain
-  flip none: their hard decisions are identical to FP64.
+  flip must sit where |LLR64| is below that path's bound (relative to
+  max |LLR64|: FP16 1e-4, BF16x3 and FP16x3 1e-6, plain chain 1e-6)
+  (test_hard_decisions_vs_fp64).  At 20 dB no path flips a bit.
 """
 from __future__ import annotations
 
@@ -80,9 +80,14 @@ def test_fused_cfg3_correlated_channel(aeq, wl, orc, cuda, prec, evm_max):
 # of sign flips for the slot of seed 40 + config, and the path's bound on
 # |LLR64| at a flip (relative to max |LLR64|: the path's LLR error).  The
 # plain chain is the reference's scalar FP32 method (aerial_pusch_eq_plain).
-FLIPS = {(1, "fp16"): None, (2, "fp16"): None, (1, "bf16x3"): None, (2, "bf16x3"): None,
-         (1, "fp16x3"): 0, (2, "fp16x3"): 0, (1, "plain"): 0, (2, "plain"): 0}
-FLIP_BOUND = {"fp16": 1e-3, "bf16x3": 1e-4, "fp16x3": 1e-5, "plain": 1e-3}
+# At 20 dB (configuration 1) every path's hard decisions equal FP64's.  At
+# 25 dB the config 2 slot holds bits whose |LLR64| is a few 1e-7 of the
+# maximum: below every reduced-precision path's error, so they flip; the
+# plain chain's flips on the config 3 slot (tests of bench.py) show that even
+# FP32 cannot decide bits at 1e-8.
+FLIPS = {(1, "fp16"): 0, (2, "fp16"): 64, (1, "bf16x3"): 0, (2, "bf16x3"): 2,
+         (1, "fp16x3"): 0, (2, "fp16x3"): 1, (1, "plain"): 0, (2, "plain"): 0}
+FLIP_BOUND = {"fp16": 1e-4, "bf16x3": 1e-6, "fp16x3": 1e-6, "plain": 1e-6}
 
 
 @pytest.mark.parametrize("cfg,path", sorted(FLIPS))
