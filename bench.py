@@ -1040,6 +1040,69 @@ def other_configs(aeq, wl, dev, stream, a):
     return out
 
 
+def reference_stages_on_b200(aeq, dev, med):
+    """Single launches at the reference's own shapes (L2-warm, the kernel time
+    alone): its coef_apply V1 / V2 / V3 (src/aerial_coef_wmma.cu:400-407),
+    gram_scalar (src/aerial_bottleneck.cu:174-179), llr V1 / V3 at 256-QAM
+    (src/llr/aerial_llr_v3.cu:292) and SRS filter V1 / V2 (66 blocks, K = 24,
+    4 ports, FOCC length 8: src/srs/srs_wmma_bench.cu:347), each beside this
+    library's entry point for the same stage."""
+    import torch
+
+    reflib = os.path.join(ROOT, "oracle", "_ref")
+    VP, CI = ctypes.c_void_p, ctypes.c_int
+    lc = ctypes.CDLL(os.path.join(reflib, "libref_coef.so"))
+    lg = ctypes.CDLL(os.path.join(reflib, "libref_gram.so"))
+    ll = ctypes.CDLL(os.path.join(reflib, "libref_llr_v3.so"))
+    ls = ctypes.CDLL(os.path.join(reflib, "libref_srs.so"))
+    lc.ref_coef_launch.argtypes = [CI, VP, VP, VP, CI, CI]
+    lg.ref_gram_launch.argtypes = [VP, VP, VP, CI]
+    ll.ref_llr_v3_launch.argtypes = [CI, VP, VP, VP, CI, CI]
+    ls.ref_srs_launch.argtypes = [CI, VP, VP, VP, VP, CI, CI]
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+
+    def crand(*shape):
+        return torch.complex(torch.rand(shape, generator=g, device=dev) - 0.5,
+                             torch.rand(shape, generator=g, device=dev) - 0.5)
+
+    nSC, S, L, A = 1584, 11, 8, 64
+    out = {}
+    C, Y = crand(nSC, L, A), crand(nSC, S, A)
+    O = torch.empty(nSC, L, S, dtype=torch.complex64, device=dev)
+    p = (C.data_ptr(), Y.data_ptr(), O.data_ptr(), nSC, S)
+    out["coef_apply"] = {
+        "reference_v1_scalar": med(lambda: lc.ref_coef_launch(1, *p)),
+        "reference_v2_wmma": med(lambda: lc.ref_coef_launch(2, *p)),
+        "reference_v3_wmma": med(lambda: lc.ref_coef_launch(3, *p)),
+        "aerial_coef_apply (bit-exact V1)": med(lambda: aeq.coef_apply(C, Y, O, nSC, S, L, A)),
+        "aerial_coef_apply_tc (V2 semantics)": med(lambda: aeq.coef_apply_tc(C, Y, O, nSC, S, L, A))}
+    H = crand(nSC, A, L)
+    M = H.conj().transpose(1, 2).contiguous()
+    G = torch.empty(nSC, L, L, dtype=torch.complex64, device=dev)
+    out["gram"] = {"reference_gram_scalar": med(lambda: lg.ref_gram_launch(M.data_ptr(), H.data_ptr(), G.data_ptr(),
+                                                                           nSC)),
+                   "aerial_gram": med(lambda: aeq.gram(H, 0.01, G, nSC, A, L))}
+    N, nb = nSC * L * S, 4
+    soft = ((torch.rand(2 * N, generator=g, device=dev) - 0.5) * 1.4).half()
+    ni = torch.rand(N, generator=g, device=dev) * 10 + 1
+    lo = torch.empty(N * 2 * nb, dtype=torch.float16, device=dev)
+    lp = (soft.data_ptr(), ni.data_ptr(), lo.data_ptr(), N, nb)
+    out["llr_256qam"] = {"reference_v1": med(lambda: ll.ref_llr_v3_launch(1, *lp)),
+                         "reference_v3": med(lambda: ll.ref_llr_v3_launch(3, *lp)),
+                         "aerial_llr (bit-exact V1)": med(lambda: aeq.llr(soft, ni, lo, N, nb))}
+    K, P, F, nBlk = 24, 4, 8, 66
+    srs = ((torch.rand(nBlk * A * K * 2, generator=g, device=dev) - 0.5) * 1.4).half()
+    W = ((torch.rand(K * K * 2, generator=g, device=dev) - 0.5) * 1.4).half()
+    fo = ((torch.rand(P * F * 2, generator=g, device=dev) - 0.5) * 1.4).half()
+    he = torch.empty(nBlk * A * K * P * 2, dtype=torch.float16, device=dev)
+    sp = (he.data_ptr(), srs.data_ptr(), W.data_ptr(), fo.data_ptr(), A, nBlk)
+    out["srs_filter"] = {"reference_v1_scalar": med(lambda: ls.ref_srs_launch(1, *sp)),
+                         "reference_v2_wmma": med(lambda: ls.ref_srs_launch(2, *sp)),
+                         "aerial_srs_filter": med(lambda: aeq.srs_filter(he, srs, W, fo, A, nBlk, K, P, F))}
+    return out
+
+
 def reference_kernels_on_b200(aeq, wl, dev, slots=64):
     """Baseline: the reference's own kernels, compiled unchanged from its
     sources into the checker libraries (oracle/_ref), on this GPU over the
@@ -1105,7 +1168,8 @@ def reference_kernels_on_b200(aeq, wl, dev, slots=64):
 
     t_ref = med(ref_chain)
     t_fused = med(lambda: aeq.pusch_eq_fused(descs, tun, stream))
-    return {"slots": slots, "subcarriers": nS,
+    stages = reference_stages_on_b200(aeq, dev, med)
+    return {"per_stage_us": stages, "slots": slots, "subcarriers": nS,
             "reference_gram_coefv2_llrv3_us": t_ref, "reference_res_per_s": nS * S / (t_ref * 1e-6),
             "fused_us": t_fused, "fused_res_per_s": nS * S / (t_fused * 1e-6), "speedup": t_ref / t_fused,
             "note": "reference: three unfused launches without a solve, from oracle/_ref; fused: Gram + MMSE "
