@@ -340,6 +340,15 @@ static void dispatcher(aerial_server* s) {
     }
 }
 
+// Room for kStatsReserve latency samples and for as many unpolled requests
+// before any container under the lock has to grow (8 bytes a sample per
+// statistic, a few MB in all); beyond that they still grow.
+constexpr size_t kStatsReserve = 1 << 18;
+static void reserve_tables(aerial_server* s) {
+    s->byId.reserve(kStatsReserve);
+    for (std::vector<int64_t>* v : {&s->lat, &s->qlat, &s->slat, &s->sublag}) v->reserve(kStatsReserve);
+}
+
 extern "C" int aerial_server_create(const aerial_server_config* cfg, aerial_server** out) {
     if (!cfg || !out || cfg->memory_budget_bytes <= 0 || cfg->streams < 1 || cfg->streams > 16 ||
         cfg->max_batch < 1 || cfg->deadline_us <= 0.f)
@@ -368,6 +377,11 @@ extern "C" int aerial_server_create(const aerial_server_config* cfg, aerial_serv
             return rt_status(e);
         }
     }
+    // Containers that grow with the requests in flight or not yet polled are
+    // sized up front: growing one (a hash-table rehash, a vector copy) under
+    // the server's lock stalled submissions and the dispatcher together for
+    // about a millisecond at a time.
+    reserve_tables(s);
     s->th = std::thread(dispatcher, s);
     *out = s;
     return AERIAL_OK;

@@ -68,8 +68,9 @@ def parse():
                     help="storage of H / Y_rx / LLRs: cf32 = the drop-in complex64 layout (default); fp16 = complex "
                          "half in, __half LLRs out (configs 1, 2 and 3 with FP16 operands), reported as its own line")
     ap.add_argument("--duration", type=float, default=1.0, help="serving run length in seconds (config 5)")
-    ap.add_argument("--window-us", type=float, default=0.0, help="serving batching window (config 5; 0 = launch at once)")
-    ap.add_argument("--min-batch", type=int, default=0, help="serving minimum batch before the window ends")
+    ap.add_argument("--window-us", type=float, default=-1.0,
+                    help="serving batching window (config 5; -1 = the default, 0 = launch at once)")
+    ap.add_argument("--min-batch", type=int, default=-1, help="serving minimum batch before the window ends (-1 = default)")
     ap.add_argument("--serve-streams", type=int, default=0, help="serving batches in flight (0 = default)")
     ap.add_argument("--srs-symbols", type=int, default=4, choices=[1, 2, 4],
                     help="SRS symbols averaged by each serving SRS update (config 5)")
@@ -601,18 +602,21 @@ class ServingWorkload:
         srv.close()
         st["submit_errors"] = int(errors)
         st["miss_rate"] = st["deadline_misses"] / max(1, st["slots_done"])
+        # misses of requests the load generator submitted half a deadline late or more
+        # are the client's; the rest are the server's own
+        st["server_miss_rate"] = (st["deadline_misses"] - st["misses_late_submit"]) / max(1, st["slots_done"])
         st["slots_offered"] = len(arrivals)
         st["streams"], st["batch_window_us"], st["min_batch"] = streams, window_us, min_batch
         return st
 
 
 SERVE_KEYS = ("slots_offered", "slots_done", "p50_us", "p99_us", "max_us", "mean_us", "queue_p99_us",
-              "service_p99_us", "deadline_misses", "miss_rate", "res_per_s", "batches", "mean_batch", "srs_updates",
+              "service_p99_us", "deadline_misses", "miss_rate", "server_miss_rate", "res_per_s", "batches", "mean_batch", "srs_updates",
               "submit_errors", "submit_lag_p99_us", "submit_lag_max_us", "dispatch_gap_max_us", "launch_call_max_us",
               "misses_late_submit", "streams", "batch_window_us", "min_batch")
 
 # Configuration 5's dispatcher settings: batches in flight and batching window.
-SERVE_STREAMS, SERVE_WINDOW_US, SERVE_MIN_BATCH = 2, 0.0, 0
+SERVE_STREAMS, SERVE_WINDOW_US, SERVE_MIN_BATCH = 2, 20.0, 2
 # Cells whose Poisson load the plain FP32 chain, request by request, sustains
 # (the kernel comparison runs both paths on this lighter trace).
 SERVE_LIGHT_CELLS = 4
@@ -644,7 +648,9 @@ def run_serving(a, aeq, wl, dev):
     is preceded by an SRS channel update (filter multiply, K = 12, one port per
     layer, averaged over 4 SRS symbols)."""
     streams = a.serve_streams or SERVE_STREAMS
-    res = serving_summary(a, aeq, wl, dev, a.duration, streams, a.window_us, a.min_batch)
+    window = SERVE_WINDOW_US if a.window_us < 0 else a.window_us
+    min_batch = SERVE_MIN_BATCH if a.min_batch < 0 else a.min_batch
+    res = serving_summary(a, aeq, wl, dev, a.duration, streams, window, min_batch)
     fused = res["fused_batched"]
     line = {
         "metric": "serving: equalized REs/s with p99 slot latency (deadline 500 us)", "value": fused["res_per_s"],
