@@ -310,8 +310,8 @@ def main():
     cells = build_cells(wl, a.config, S, rank, dev)
     half = a.io == "fp16"
     if half:
-        if a.config not in (1, 2, 3) or a.precision != "fp16":
-            raise SystemExit("--io fp16 runs configurations 1, 2 and 3 with fp16 operands "
+        if a.config not in (1, 2, 3, 4) or a.precision != "fp16":
+            raise SystemExit("--io fp16 runs configurations 1-4 with fp16 operands "
                              "(configuration 3: --precision fp16)")
         a.no_extras = True          # the extras run the complex64 plain chain
         # the same slots stored as complex half; the complex64 copies are dropped
