@@ -22,11 +22,16 @@ extern "C" int aerial_version(void) { return 10000; /* 1.0.0 */ }
 
 namespace aeq {
 int prepare_fused_kernels();
+int prepare_srs_kernels();
+int prepare_plain_kernels();
 }
 
 // Load the library's kernels on the current device (see the header).
 extern "C" int aerial_prepare(void) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return AERIAL_ERR_NO_DEVICE;
-    return aeq::prepare_fused_kernels();
+    int s = aeq::prepare_fused_kernels();
+    if (!s) s = aeq::prepare_srs_kernels();
+    if (!s) s = aeq::prepare_plain_kernels();
+    return s;
 }

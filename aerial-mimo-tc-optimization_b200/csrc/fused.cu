@@ -36,10 +36,12 @@ constexpr int kMaxCells = AERIAL_MAX_CELLS;
 // Subcarriers per group: GS = min(32 / LT, cap).  32 / LT fills every lane
 // of the FP32 solve and of the LLR epilogue (LT lanes per subcarrier); a
 // smaller cap shortens each group's operand pass (GS x chunks items), which
-// an uneven batch needs so that no warp is left with a few long groups.  The
-// default 8 fills every lane for tiles of 4 layers and more; the cap is a
-// tuning parameter (aerial_tuning.sc_per_group, searched by the autotuner).
-constexpr int kDefaultGroupCap = 8;
+// an uneven batch needs so that no warp is left with a few long groups: on
+// the uneven 16-cell batch a cap of 4 (idle solve lanes on 1-, 2- and
+// 4-layer tiles) measured 54.3 us against 66.6 us for a cap of 8.
+// The cap is a tuning parameter (aerial_tuning.sc_per_group, searched by the
+// autotuner).
+constexpr int kDefaultGroupCap = 4;
 
 struct FusedCell {
     const float2* H;
@@ -826,11 +828,6 @@ __device__ __forceinline__ int group_valid(const FusedCell& cl, long grp) {
     return (int)min((long)cl.GS, (long)cl.nSC - (grp - cl.group0) * cl.GS);
 }
 
-// Group of round r of warp gw in the snake walk (see fused_eq_kernel).
-__device__ __forceinline__ long snake_group(int r, long gw, long nw) {
-    return (long)r * nw + ((r & 1) ? nw - 1 - gw : gw);
-}
-
 // LTF = 0: any mix of cells.  LTF in {2, 4, 8, 16}: every cell has
 // nLayers == LTF and 16-byte aligned H / Y_rx (the host checks), so the layer
 // tile, strides and masks are compile-time constants.
@@ -852,11 +849,6 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
     const long nw = (long)gridDim.x * warpsPerCta;
     const long total = p.totalGroups;
     if (gw >= total) return;
-    // Snake walk: in round r this warp takes group r nw + gw (r even) or
-    // r nw + nw - 1 - gw (r odd).  The host orders cells by group cost, most
-    // expensive first, so each warp's rounds pair an expensive group with a
-    // cheap one and the warps of an uneven batch finish together.
-    int pr = 0, cr = 0;
 
     // ---- producer cursor (registers): group, cell, subcarrier, chunk ----
     // Per-lane staging offsets are fixed for the whole launch (exact tile) or
@@ -932,7 +924,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
                     pys += pYsc;
                 } else {
                     pq = 0;
-                    pg = snake_group(++pr, gw, nw);
+                    pg += nw;
                     if (pg < total) {
                         while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
                         load_pcell();
@@ -1062,7 +1054,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel(const __grid_constant_
             }
         }
         q = 0;
-        grp = snake_group(++cr, gw, nw);
+        grp += nw;
         if (grp >= total) break;
         while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
         load_ccell();
@@ -1448,8 +1440,8 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_h(const __grid_constan
 // FP16 I/O for a mixed batch: any mix of complex-half cells whose layers fill
 // their tile (2, 4, 8 or 16) and whose antenna counts are multiples of 16.
 // Staging, fragment reads and epilogue are fused_eq_kernel_h's per cell (the
-// layer tile by switch, the chunk count at run time); the work walk is the
-// mixed-batch kernel's snake order over cost-sorted cells.
+// layer tile by switch, the chunk count at run time) and the group walk is
+// the mixed-batch kernel's.
 // ---------------------------------------------------------------------------
 // Chunk j of one subcarrier: h / y are the lane's pieces of its first chunk.
 template <int LF>
@@ -1488,9 +1480,9 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_hg(const __grid_consta
     if (gw >= total) return;
     const int s0 = lane >> 2, q4 = lane & 3;
 
-    // ---- producer cursor: group (snake walk), cell, subcarrier, chunk ----
+    // ---- producer cursor: group, cell, subcarrier, chunk ----
     long pg = gw;
-    int pr = 0, pci = 0;
+    int pci = 0;
     while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
     int pq = 0, pch = 0, pslot = 0, pValid, pNCh, pLT, pYk, pA, pHscB, pYscB;
     uint32_t pHLaneS, pYLaneS;
@@ -1529,7 +1521,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_hg(const __grid_consta
                     py += pYscB;
                 } else {
                     pq = 0;
-                    pg = snake_group(++pr, gw, nw);
+                    pg += nw;
                     if (pg < total) {
                         while (pci + 1 < p.nCells && pg >= p.cell[pci + 1].group0) pci++;
                         load_pcell();
@@ -1544,7 +1536,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_hg(const __grid_consta
 
     // ---- consumer ----
     long grp = gw;
-    int cr = 0, ci = 0;
+    int ci = 0;
     while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
     int q = 0, ch = 0, cslot = 0, nValid, cNCh, cLT;
     bool z2;
@@ -1617,7 +1609,7 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_hg(const __grid_consta
             }
         }
         q = 0;
-        grp = snake_group(++cr, gw, nw);
+        grp += nw;
         if (grp >= total) break;
         while (ci + 1 < p.nCells && grp >= p.cell[ci + 1].group0) ci++;
         load_ccell();
@@ -1670,49 +1662,20 @@ extern "C" float aerial_fp16_operand_scale(float sigma2) {
 
 namespace aeq {
 
-// Estimated cost of one full group of a cell, in rough warp-instruction
-// units from the kernel's structure: the operand phase of GS subcarriers
-// (per 16-antenna chunk: staging, fragment reads and conversions, MMAs; the
-// 16-layer tile has two m-tiles) and the group's epilogue (FP32 solve, then
-// X = G^-1 Z, unbiasing and demapper with one lane per layer row).  Only the
-// order it induces matters (set_groups).
-static long group_cost_of(const FusedCell& c) {
-    const int nmt = c.LT > 8 ? 2 : 1;
-    const long operand = (long)c.GS * c.nChunk * (24 + 26 * nmt);
-    const long solve = c.LT * (c.LT / 2 + 2 * c.LT + 12);
-    const long emit = (long)((c.nSym + 1) / 2) * (5 * c.LT + 4 * (3 * c.nPam + 4));
-    return operand + solve + emit;
-}
-
 // Group size of every cell (min(32 / LT, cap)) and the first group index of
-// each.  Cells are ordered by group cost, most expensive first (stable, so
-// equal shapes keep their order and a parameter block built again from the
-// same cells comes out identical): with the mixed-batch kernels' snake walk
-// over the groups this spreads an uneven batch evenly over the warps.  A
-// cell's outputs do not depend on its position.
+// each, in launch order.  Warps take groups round-robin (warp w: groups w,
+// w + nw, ...).  Measured on the uneven 16-cell batch (configuration 4), same
+// box, against this walk with cap 4 (54.3 us): a snake walk over cells sorted
+// by estimated group cost 56.3 us, sorting alone 56.3-58.3 us, cap 8 with the
+// plain walk 66.6 us; the autotuner's launch shapes recover 54.3 us in every
+// variant, and no variant beats the plain walk.  Outputs are bit-identical
+// across all of them.
 void set_groups(FusedParams& p, int cap) {
     if (cap < 1) cap = kDefaultGroupCap;
-    long cost[AERIAL_MAX_CELLS];
-    for (int i = 0; i < p.nCells; i++) {
-        FusedCell& f = p.cell[i];
-        f.GS = 32 / f.LT < cap ? 32 / f.LT : cap;
-        cost[i] = group_cost_of(f);
-    }
-    for (int i = 1; i < p.nCells; i++) {          // insertion sort, descending, stable
-        const FusedCell f = p.cell[i];
-        const long cf = cost[i];
-        int j = i - 1;
-        while (j >= 0 && cost[j] < cf) {
-            p.cell[j + 1] = p.cell[j];
-            cost[j + 1] = cost[j];
-            j--;
-        }
-        p.cell[j + 1] = f;
-        cost[j + 1] = cf;
-    }
     long g0 = 0;
     for (int i = 0; i < p.nCells; i++) {
         FusedCell& f = p.cell[i];
+        f.GS = 32 / f.LT < cap ? 32 / f.LT : cap;
         f.group0 = g0;
         g0 += (f.nSC + f.GS - 1) / f.GS;
     }
@@ -2040,7 +2003,7 @@ extern "C" int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, 
 // ---------------------------------------------------------------------------
 // Autotuner: time each candidate tile and launch shape on the caller's cells
 // and keep the fastest.  Candidates are the group cap (subcarriers solved
-// together per warp: 8, 32 or 4, for batches with tiles of 4 layers or fewer,
+// together per warp: 4, 8 or 32, for batches with tiles of 4 layers or fewer,
 // where the cap changes anything) crossed with (warps per CTA, CTAs per SM)
 // pairs whose shared memory fits one SM; each is timed with CUDA events over
 // a few launches after one warm-up launch.  The reference's analogue is its
@@ -2063,8 +2026,8 @@ extern "C" int aerial_autotune(const aerial_cell_desc* cells, int nCells, aerial
     bool smallTile = false;
     for (int i = 0; i < base.nCells; i++) smallTile |= base.cell[i].LT <= 4;
     if (smallTile) {
+        caps[nCaps++] = 8;
         caps[nCaps++] = 32;
-        caps[nCaps++] = 4;
     }
     Cand cand[48];
     int nc = 0;

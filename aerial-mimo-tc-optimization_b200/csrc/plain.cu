@@ -227,6 +227,31 @@ int launch_llr_f32(const cf* in, const float* ni, float* out, int N, int n, int 
 
 }  // namespace aeq
 
+namespace aeq {
+
+// Load the plain chain's kernels on the current device (aerial_prepare).
+template <typename K>
+static int prepare_one(K* k) {
+    cudaFuncAttributes at;
+    return rt_status(cudaFuncGetAttributes(&at, k));
+}
+int prepare_plain_kernels() {
+    int s = prepare_one(gram_kernel);
+    if (!s) s = prepare_one(mmse_coef_kernel);
+    if (!s) s = prepare_one(coef_apply_kernel);
+    if (!s) s = prepare_one(llr_f16_kernel<1>);
+    if (!s) s = prepare_one(llr_f16_kernel<2>);
+    if (!s) s = prepare_one(llr_f16_kernel<3>);
+    if (!s) s = prepare_one(llr_f16_kernel<4>);
+    if (!s) s = prepare_one(llr_f32_kernel<1>);
+    if (!s) s = prepare_one(llr_f32_kernel<2>);
+    if (!s) s = prepare_one(llr_f32_kernel<3>);
+    if (!s) s = prepare_one(llr_f32_kernel<4>);
+    return s;
+}
+
+}  // namespace aeq
+
 using namespace aeq;
 
 extern "C" int aerial_gram(const aerial_cf32* H, float sigma2, aerial_cf32* G, int nSC, int nAnt, int nLayers,

@@ -40,6 +40,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
+#include <utility>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -784,3 +785,50 @@ extern "C" int aerial_chest_interp_h(aerial_ch2* H, const aerial_ch2* Yp, const 
     if (r != AERIAL_ERR_UNSUPPORTED) return r;
     return launch_srs_chan<kOutChan16>(H, Yp, Wf, OCC, nAnt, nBlocks, nPilot, nOut, nPorts, occLen, to_stream(stream));
 }
+
+namespace aeq {
+
+// Load every filter-kernel instantiation on the current device and raise its
+// shared-memory limit (aerial_prepare): the first launch of a kernel
+// otherwise pays the driver's lazy module loading, milliseconds inside a
+// serving loop's first SRS update.
+template <int KS, int OUTL>
+static int prepare_srs_tc() {
+    constexpr int MT = KS <= 6 ? 2 : 1;
+    cudaFuncAttributes at;
+    const cudaError_t e = cudaFuncGetAttributes(&at, srs_filter_tc_kernel<KS, MT, OUTL>);
+    return e == cudaSuccess ? allow_max_smem<srs_filter_tc_kernel<KS, MT, OUTL>>() : rt_status(e);
+}
+template <int OUTL, int... KS>
+static int prepare_srs_tc_all(std::integer_sequence<int, KS...>) {
+    int s = AERIAL_OK;
+    ((s = s ? s : prepare_srs_tc<KS + 1, OUTL>()), ...);
+    return s;
+}
+template <int KB, int NTL, int OUTL>
+static int prepare_umma() {
+    cudaFuncAttributes at;
+    const cudaError_t e = cudaFuncGetAttributes(&at, chest_umma_kernel<KB, NTL, OUTL>);
+    return e == cudaSuccess ? allow_max_smem<chest_umma_kernel<KB, NTL, OUTL>>() : rt_status(e);
+}
+template <int OUTL>
+static int prepare_umma_all() {
+    int s = prepare_umma<1, 128, OUTL>();
+    if (!s) s = prepare_umma<1, 192, OUTL>();
+    if (!s) s = prepare_umma<2, 128, OUTL>();
+    if (!s) s = prepare_umma<2, 192, OUTL>();
+    if (!s) s = prepare_umma<3, 128, OUTL>();
+    return s;
+}
+
+int prepare_srs_kernels() {
+    int s = prepare_umma_all<kOutEst16>();
+    if (!s) s = prepare_umma_all<kOutChan32>();
+    if (!s) s = prepare_umma_all<kOutChan16>();
+    if (!s) s = prepare_srs_tc_all<kOutEst16>(std::make_integer_sequence<int, 6>{});
+    if (!s) s = prepare_srs_tc_all<kOutChan32>(std::make_integer_sequence<int, 12>{});
+    if (!s) s = prepare_srs_tc_all<kOutChan16>(std::make_integer_sequence<int, 12>{});
+    return s;
+}
+
+}  // namespace aeq

@@ -566,8 +566,12 @@ class ServingWorkload:
             k = srv.add_cell(c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits, c.sigma2)
             srv.set_channel(k, c.H, c.sigma2)
             ids[ci] = k
-        # one untimed slot per cell (first launch of every shape), then reset the statistics
+        # one untimed SRS update and slot per cell (first launch of every shape), then reset the statistics
         for ci in active:
+            ops = self.srs_ops[ci]
+            assert lib.aerial_server_srs_update_n(srv._h, ids[ci], ctypes.c_void_p(ops[0].data_ptr()), self.srs_syms,
+                                                  ctypes.c_void_p(ops[1].data_ptr()), ctypes.c_void_p(ops[2].data_ptr()),
+                                                  12, 12, None) == 0
             srv.submit(ids[ci], self.Ys[ci][0], self.rings[ci][0])
         srv.drain(60000)
         srv.poll(max_out=4096)

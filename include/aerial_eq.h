@@ -263,9 +263,9 @@ typedef struct {
     int warps_per_cta;         /* 0 = default */
     int ctas_per_sm;           /* 0 = default */
     int sc_per_group;          /* cap on the subcarriers a warp solves together
-                                  (min(32 / layer tile, cap)); 0 = default (8:
-                                  every lane of the solve busy for tiles of 4
-                                  layers and more) */
+                                  (min(32 / layer tile, cap)); 0 = default (4:
+                                  short groups, so no warp of an uneven batch
+                                  is left with a few long ones) */
 } aerial_tuning;
 
 /* Equalize nCells cell-slots in ONE persistent launch (cells may differ in
