@@ -1736,9 +1736,11 @@ int build_fused_params(const aerial_cell_desc* cells, int nCells, FusedParams& p
     p.exactChunks = 0;
     if (p.exactTile) {
         const int a = p.cell[0].A;
-        // (16-layer tiles keep the runtime chunk loop: unrolling their
-        // larger k-step bodies measured slower)
-        bool same = p.exactTile <= 8 && (a == 32 || a == 64 || a == 128);
+        // 16-layer tiles unroll too: on the 12-slot 273 PRB x 128 antenna
+        // launch, same box, 277 against 302 us with FP16 operands and 359
+        // against 365 us with BF16X3, bit-identical (the runtime chunk loop
+        // of the 16-layer tile spills registers, the unrolled one does not)
+        bool same = a == 32 || a == 64 || a == 128;
         for (int i = 1; i < nCells && same; i++) same = p.cell[i].A == a;
         if (same) p.exactChunks = a / CHUNK;
     }
