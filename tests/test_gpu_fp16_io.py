@@ -84,6 +84,38 @@ def test_fp16_io_mixed_batch_alone_and_in_mix(aeq, wl, cuda):
         assert torch.equal(alone[0][3], mixed[i][3])
 
 
+def test_fp16_io_mixed_batch_host_pipeline_and_graph(aeq, wl, cuda):
+    """A mixed half-format batch through aerial_pusch_eq_host (host buffers,
+    sub-batches over three streams) and as a CUDA graph replay equals the
+    resident direct launch, bit for bit."""
+    cells = wl.multicell(16, seed=83)
+    _, ref = run_pair(aeq, cells, cuda, want_yeq=False)
+    hd, hl, keep = [], [], []
+    for c, (H16, Y16, _, _) in zip(cells, ref):
+        hH, hY = H16.cpu().pin_memory(), Y16.cpu().pin_memory()
+        l = torch.full((c.llr_numel,), float("nan"), dtype=torch.float16).pin_memory()
+        keep += [hH, hY]
+        hl.append(l)
+        hd.append(aeq.host_cell_desc(hH, hY, l, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits,
+                                     fmt=aeq.FMT_CF16))
+    ws = torch.empty(aeq.pusch_eq_host_workspace(hd, 5), dtype=torch.uint8, device=cuda)
+    aeq.pusch_eq_host(hd, ws, aeq.make_tuning("fp16"), 5)
+    torch.cuda.synchronize()
+    for l, (_, _, l16, _) in zip(hl, ref):
+        assert torch.equal(l, l16.cpu())
+    descs, outs = [], []
+    for c, (H16, Y16, _, _) in zip(cells, ref):
+        l16 = torch.full((c.llr_numel,), float("nan"), dtype=torch.float16, device=cuda)
+        outs.append(l16)
+        descs.append(aeq.cell_desc(H16, Y16, l16, c.sigma2, c.nPRB, c.nAnt, c.nLayers, c.nSym, c.nPamBits,
+                                   fmt=aeq.FMT_CF16))
+    with aeq.FusedGraph(descs, aeq.make_tuning("fp16")) as g:
+        g.launch()
+        torch.cuda.synchronize()
+    for o, (_, _, l16, _) in zip(outs, ref):
+        assert torch.equal(o, l16)
+
+
 def test_fp16_io_vs_fp64(aeq, wl, orc, cuda):
     """The headline cell in FP16 I/O against the FP64 model of its own
     (half-rounded) inputs, at the FP16 bar."""
