@@ -563,18 +563,8 @@ __device__ __forceinline__ float rcp_nr(float x) {
     return y * fmaf(-x, y, 2.f);
 }
 
-// Row of LT complex values <-> shared memory (16-byte pieces; rows start
+// Row of LT complex values from shared memory (16-byte pieces; rows start
 // 16-byte aligned, WarpSmem keeps every row stride even).
-template <int LT>
-__device__ __forceinline__ void put_row(float2* row, const float2 (&r)[LT]) {
-    if constexpr (LT == 1) {
-        row[0] = r[0];
-    } else {
-#pragma unroll
-        for (int m = 0; m < LT; m += 2)
-            *reinterpret_cast<float4*>(row + m) = make_float4(r[m].x, r[m].y, r[m + 1].x, r[m + 1].y);
-    }
-}
 template <int LT>
 __device__ __forceinline__ void get_row(const float2* row, float2 (&b)[LT]) {
     if constexpr (LT == 1) {
@@ -648,37 +638,64 @@ __device__ __noinline__ void solve_group(const CellView cl, long sc0, int nValid
     // columns accumulate the inverse in the same sweep.  Every lane does
     // LT - 1 useful complex multiply-adds per step (no idle triangle), and the
     // broadcast of row k is LT / 2 shared loads.
-    if (i == 0) put_row<LT>(sG, r);
+    if constexpr (LT == 1) {
+        // one layer: G^-1 = 1 / g
+        r[0] = make_float2(rcp_nr(fmaxf(r[0].x, 1e-30f)), -0.f);
+    } else {
+        // The row is held planar for the sweep: for each column pair h,
+        // X[h] = (Re r_2h, Re r_2h+1) and Y[h] = (Im r_2h, Im r_2h+1), and the
+        // published row k is stored the same way (one 16-byte piece per pair:
+        // Re, Re, Im, Im), so the update
+        //   Re r_j = fma(-fx, Re b_j, fma(fy, Im b_j, Re r_j))
+        //   Im r_j = fma(-fx, Im b_j, fma(-fy, Re b_j, Im r_j))
+        // is four packed FMAs per column pair, in the same order of rounding
+        // as the scalar form.  Column k's updated value is discarded.
+        constexpr int NP = LT / 2;
+        unsigned long long X[NP], Y[NP];
 #pragma unroll
-    for (int k = 0; k < LT; k++) {
-        __syncwarp();
-        const float2* bk = sG + k * W::RS;
-        const float piv = fmaxf(bk[k].x, 1e-30f);
-        const float p = rcp_nr(piv);
-        const bool mine = i == k;
-        const float fx = mine ? 1.f - p : r[k].x * p;
-        const float fy = mine ? 0.f : r[k].y * p;
-        // row k streamed in pairs (keeps the 16-layer tile within registers)
-#pragma unroll
-        for (int j0 = 0; j0 < LT; j0 += (LT == 1 ? 1 : 2)) {
-            float2 b[2];
-            if constexpr (LT == 1) {
-                b[0] = bk[0];
-            } else {
-                const float4 t = *reinterpret_cast<const float4*>(bk + j0);
-                b[0] = make_float2(t.x, t.y);
-                b[1] = make_float2(t.z, t.w);
-            }
-#pragma unroll
-            for (int u = 0; u < (LT == 1 ? 1 : 2); u++) {
-                const int j = j0 + u;
-                if (j == k) continue;
-                r[j].x = fmaf(-fx, b[u].x, fmaf(fy, b[u].y, r[j].x));
-                r[j].y = fmaf(-fx, b[u].y, fmaf(-fy, b[u].x, r[j].y));
-            }
+        for (int h = 0; h < NP; h++) {
+            X[h] = pk2(r[2 * h].x, r[2 * h + 1].x);
+            Y[h] = pk2(r[2 * h].y, r[2 * h + 1].y);
         }
-        r[k] = make_float2(mine ? p : -fx, -fy);
-        if (k + 1 < LT && i == k + 1) put_row<LT>(sG + (k + 1) * W::RS, r);
+        auto put_planar = [&](float2* row) {
+#pragma unroll
+            for (int h = 0; h < NP; h++) {
+                const float2 x = upk2(X[h]), y = upk2(Y[h]);
+                *reinterpret_cast<float4*>(row + 2 * h) = make_float4(x.x, x.y, y.x, y.y);
+            }
+        };
+        if (i == 0) put_planar(sG);
+#pragma unroll
+        for (int k = 0; k < LT; k++) {
+            __syncwarp();
+            const float* bk = reinterpret_cast<const float*>(sG + k * W::RS);
+            const float piv = fmaxf(bk[4 * (k >> 1) + (k & 1)], 1e-30f);
+            const float p = rcp_nr(piv);
+            const bool mine = i == k;
+            const float2 xk = upk2(X[k >> 1]), yk = upk2(Y[k >> 1]);
+            const float rkx = (k & 1) ? xk.y : xk.x, rky = (k & 1) ? yk.y : yk.x;
+            const float fx = mine ? 1.f - p : rkx * p;
+            const float fy = mine ? 0.f : rky * p;
+            const unsigned long long nfx = pk2(-fx, -fx), pfy = pk2(fy, fy), nfy = pk2(-fy, -fy);
+#pragma unroll
+            for (int h = 0; h < NP; h++) {
+                const float4 t = *reinterpret_cast<const float4*>(bk + 4 * h);
+                const unsigned long long bx = pk2(t.x, t.y), by = pk2(t.z, t.w);
+                X[h] = fma2(nfx, bx, fma2(pfy, by, X[h]));
+                Y[h] = fma2(nfx, by, fma2(nfy, bx, Y[h]));
+            }
+            const float nx = mine ? p : -fx, ny = -fy;
+            const float2 xs = upk2(X[k >> 1]), ys = upk2(Y[k >> 1]);
+            X[k >> 1] = (k & 1) ? pk2(xs.x, nx) : pk2(nx, xs.y);
+            Y[k >> 1] = (k & 1) ? pk2(ys.x, ny) : pk2(ny, ys.y);
+            if (k + 1 < LT && i == k + 1) put_planar(sG + (k + 1) * W::RS);
+        }
+#pragma unroll
+        for (int h = 0; h < NP; h++) {
+            const float2 x = upk2(X[h]), y = upk2(Y[h]);
+            r[2 * h] = make_float2(x.x, y.x);
+            r[2 * h + 1] = make_float2(x.y, y.y);
+        }
     }
     float gii = r[0].x;
 #pragma unroll
