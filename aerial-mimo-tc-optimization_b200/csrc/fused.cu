@@ -1116,8 +1116,13 @@ __device__ __forceinline__ void stage_chunk(uint32_t st, uint32_t hLaneS, uint32
         if (k < s.yk) cp_async16(st + yLaneS + 512 * k, s.y + CHUNK * j + 4 * k * A);
 }
 
+// Register budget: 128 per thread (16 resident warps) for tiles up to 8
+// layers; the 16-layer tile's shared memory admits 12 resident warps at most,
+// so it takes what it needs (140 registers, no spills in its 16 x 16 solve):
+// 12-slot precision-stress launch 334 against 341-343 us with BF16X3 operands,
+// same box, bit-identical.
 template <int P, int LTF, int NCH, bool SC = false>
-__global__ void __launch_bounds__(256, 2) fused_eq_kernel_a(const __grid_constant__ FusedParams p) {
+__global__ void __launch_bounds__(256, LTF == 16 ? 1 : 2) fused_eq_kernel_a(const __grid_constant__ FusedParams p) {
     constexpr int NST = stages_of_a(LTF, NCH);
     constexpr int A = CHUNK * NCH;
     constexpr int HRS = hrs_of(LTF);
