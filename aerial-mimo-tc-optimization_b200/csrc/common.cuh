@@ -1,5 +1,7 @@
 // common.cuh -- shared device/host helpers of the B200 equalization library.
 #pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
@@ -35,6 +37,39 @@ inline cudaStream_t to_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 constexpr int kMaxDevices = 64;                 // devices with cached per-device state
 constexpr int kMaxSmemPerCta = 227 * 1024;      // B200 dynamic shared memory per block
+
+// cuCtxGetCurrent / cuCtxGetId from the driver, looked up once.
+struct CtxQuery {
+    PFN_cuCtxGetCurrent_v4000 current = nullptr;
+    PFN_cuCtxGetId_v12000 id = nullptr;
+};
+inline const CtxQuery& ctx_query() {
+    static std::once_flag once;
+    static CtxQuery q;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult r;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r) == cudaSuccess &&
+            r == cudaDriverEntryPointSuccess)
+            q.current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &r) == cudaSuccess &&
+            r == cudaDriverEntryPointSuccess)
+            q.id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+    });
+    return q;
+}
+
+// Unique ID of the calling thread's current context, 0 if there is none yet
+// or the driver cannot say.
+inline unsigned long long current_ctx_id() {
+    const CtxQuery& q = ctx_query();
+    if (!q.current || !q.id) return 0;
+    CUcontext ctx = nullptr;
+    if (q.current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    unsigned long long id = 0;
+    return q.id(ctx, &id) == CUDA_SUCCESS ? id : 0;
+}
 
 // SM count of the current device, looked up once per device.
 inline int sm_count() {

@@ -371,44 +371,9 @@ extern "C" int aerial_pusch_eq_plain(const aerial_cell_desc* cells, int nCells, 
 // call, so nothing needs clearing, but calls that overlap on the GPU (two
 // streams, two threads) race on it.
 // ---------------------------------------------------------------------------
-#include <cuda.h>
-#include <cudaTypedefs.h>
 #include <mutex>
 
 static __device__ __align__(256) unsigned char g_plain_static_scratch[AERIAL_STATIC_SCRATCH_BYTES];
-
-// cuCtxGetCurrent / cuCtxGetId from the driver, looked up once.
-struct CtxQuery {
-    PFN_cuCtxGetCurrent_v4000 current = nullptr;
-    PFN_cuCtxGetId_v12000 id = nullptr;
-};
-static const CtxQuery& ctx_query() {
-    static std::once_flag once;
-    static CtxQuery q;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult r;
-        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &r) == cudaSuccess &&
-            r == cudaDriverEntryPointSuccess)
-            q.current = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
-        p = nullptr;
-        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &r) == cudaSuccess &&
-            r == cudaDriverEntryPointSuccess)
-            q.id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
-    });
-    return q;
-}
-
-// Unique ID of the calling thread's current context, 0 if there is none yet
-// or the driver cannot say.
-static unsigned long long current_ctx_id() {
-    const CtxQuery& q = ctx_query();
-    if (!q.current || !q.id) return 0;
-    CUcontext ctx = nullptr;
-    if (q.current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
-    unsigned long long id = 0;
-    return q.id(ctx, &id) == CUDA_SUCCESS ? id : 0;
-}
 
 static int static_scratch_address(void** out) {
     static std::mutex mu;
