@@ -273,6 +273,14 @@ typedef struct {
  * (copied into the launch's parameters); its buffers are device pointers.
  * Results per subcarrier do not depend on which other cells share the
  * launch.  nCells <= AERIAL_MAX_CELLS.  tuning may be NULL.
+ * Work distribution: a uniform batch (every cell the same 2/4/8/16-layer
+ * tile and 32/64/128 antennas) hands its groups of subcarriers to warps from
+ * a counter in the library's device memory, one counter per stream that
+ * launches and per graph (64 per device), so launches that may overlap never
+ * share one; a launch being stream-captured, one that finds no counter free,
+ * mixed batches, and every launch while the environment variable
+ * AERIAL_STATIC_WALK is set to a non-zero value use a fixed round-robin
+ * assignment instead.  The outputs are the same bit for bit either way.
  * No reference counterpart as one kernel: the reference chains gram_scalar,
  * coef_apply and a demapper as separate launches (src/pipeline_overlap.cu:293-301). */
 int aerial_pusch_eq_fused(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
@@ -328,8 +336,11 @@ int aerial_pusch_eq_plain_static(const aerial_cell_desc* cells, int nCells, void
 /* The same fused launch as an executable CUDA graph (one kernel node, built
  * without stream capture).  aerial_eq_graph_update re-points the node at new
  * buffers / sigma2 of cells with the same shapes (AERIAL_ERR_UNSUPPORTED if a
- * shape changes); launching replays the graph on `stream`.  No counterpart in
- * the reference (it has no graphs). */
+ * shape changes); launching replays the graph on `stream`.  A graph of a
+ * uniform batch holds its own work counter (see aerial_pusch_eq_fused) until
+ * it is destroyed; replays of one graph must not overlap one another, which
+ * CUDA already ensures for launches of one executable graph.  No counterpart
+ * in the reference (it has no graphs). */
 typedef struct aerial_eq_graph aerial_eq_graph;
 int aerial_eq_graph_create(const aerial_cell_desc* cells, int nCells, const aerial_tuning* tuning,
                            aerial_eq_graph** out);
