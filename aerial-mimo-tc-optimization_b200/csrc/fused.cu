@@ -2050,19 +2050,26 @@ struct WalkSlot {
     cudaEvent_t last = nullptr;      // recorded behind the slot's latest launch
 };
 struct WalkTable {
-    std::mutex m;
-    unsigned long long ctx = 0;      // context the slots' events belong to
+    unsigned long long ctx = 0;      // context the slots (and their events) belong to, 0 if unused
     WalkSlot s[kWalkSlots];
 };
-static WalkTable g_walk_tables[kMaxDevices];
+// A device's tables, one per context (the device's primary context, or a
+// new one after a device reset): a table is never handed to another context,
+// and a launch in a fifth context on one device takes the static walk.
+constexpr int kWalkContexts = 4;
+struct WalkDevice {
+    std::mutex m;
+    WalkTable t[kWalkContexts];
+};
+static WalkDevice g_walk_devices[kMaxDevices];
 
 static bool walk_static_forced() {
     const char* e = std::getenv("AERIAL_STATIC_WALK");
     return e && e[0] && !(e[0] == '0' && e[1] == 0);
 }
 
-// The current device's table with its lock taken, or nullptr (static walk).
-// Entries made in another context (before a device reset) are dropped.
+// The current context's table with its device's lock taken, or nullptr
+// (static walk).
 static WalkTable* walk_table_locked(std::unique_lock<std::mutex>& lk, int* devOut = nullptr) {
     if (walk_static_forced()) return nullptr;
     int dev = 0;
@@ -2073,11 +2080,19 @@ static WalkTable* walk_table_locked(std::unique_lock<std::mutex>& lk, int* devOu
     if (dev < 0 || dev >= kMaxDevices) return nullptr;
     const unsigned long long ctx = current_ctx_id();
     if (ctx == 0) return nullptr;
-    WalkTable* t = &g_walk_tables[dev];
-    lk = std::unique_lock<std::mutex>(t->m);
-    if (t->ctx != ctx) {
-        for (WalkSlot& w : t->s) w = WalkSlot{};
-        t->ctx = ctx;
+    WalkDevice& d = g_walk_devices[dev];
+    lk = std::unique_lock<std::mutex>(d.m);
+    WalkTable* t = nullptr;
+    for (WalkTable& c : d.t)
+        if (c.ctx == ctx) t = &c;
+    for (int k = 0; k < kWalkContexts && !t; k++)
+        if (d.t[k].ctx == 0) {
+            t = &d.t[k];
+            t->ctx = ctx;
+        }
+    if (!t) {
+        lk.unlock();
+        return nullptr;
     }
     if (devOut) *devOut = dev;
     return t;
@@ -2303,14 +2318,14 @@ struct aerial_eq_graph {
     LaunchShape shape{};
     int gsCap = kDefaultGroupCap;
     int dev = -1;                    // device of the graph's walk slot (params.walkSlot)
+    WalkTable* walk = nullptr;       // table of that slot
 };
 
 static void release_walk_slot(aerial_eq_graph* g) {
     const int i = g->params.walkSlot;
-    if (i < 0 || g->dev < 0 || g->dev >= kMaxDevices) return;
-    WalkTable& t = g_walk_tables[g->dev];
-    std::lock_guard<std::mutex> lk(t.m);
-    t.s[i].graph = false;            // reusable once the event behind its last replay completes
+    if (i < 0 || !g->walk) return;
+    std::lock_guard<std::mutex> lk(g_walk_devices[g->dev].m);
+    g->walk->s[i].graph = false;     // reusable once the event behind its last replay completes
 }
 
 static cudaKernelNodeParams node_params(aerial_eq_graph* g, void** args) {
@@ -2345,6 +2360,7 @@ extern "C" int aerial_eq_graph_create(const aerial_cell_desc* cells, int nCells,
         if (i >= 0) {
             t->s[i].graph = true;
             t->s[i].stream = 0;
+            g->walk = t;
         }
         g->params.walkSlot = i;
     }
@@ -2400,12 +2416,11 @@ extern "C" int aerial_eq_graph_update(aerial_eq_graph* g, const aerial_cell_desc
 extern "C" int aerial_eq_graph_launch(aerial_eq_graph* g, void* stream) {
     if (!g) return AERIAL_ERR_INVALID_ARG;
     const int i = g->params.walkSlot;
-    if (i < 0 || g->dev < 0 || g->dev >= kMaxDevices) return rt_status(cudaGraphLaunch(g->exec, to_stream(stream)));
-    WalkTable& t = g_walk_tables[g->dev];
-    std::lock_guard<std::mutex> lk(t.m);
+    if (i < 0 || !g->walk) return rt_status(cudaGraphLaunch(g->exec, to_stream(stream)));
+    std::lock_guard<std::mutex> lk(g_walk_devices[g->dev].m);
     const cudaError_t e = cudaGraphLaunch(g->exec, to_stream(stream));
     if (e != cudaSuccess) return rt_status(e);
-    return walk_record(&t, i, to_stream(stream));
+    return walk_record(g->walk, i, to_stream(stream));
 }
 
 extern "C" int aerial_eq_graph_destroy(aerial_eq_graph* g) {
