@@ -2356,7 +2356,9 @@ extern "C" int aerial_eq_graph_create(const aerial_cell_desc* cells, int nCells,
         // the graph's own walk slot: its replays are ordered among themselves
         std::unique_lock<std::mutex> lk;
         WalkTable* t = walk_applies(g->params) ? walk_table_locked(lk, &g->dev) : nullptr;
-        const int i = t ? walk_free_slot(t) : -1;
+        int held = 0;                // graphs hold at most kWalkSlots - 16: streams keep slots
+        for (int k = 0; t && k < kWalkSlots; k++) held += t->s[k].graph ? 1 : 0;
+        const int i = t && held < kWalkSlots - 16 ? walk_free_slot(t) : -1;
         if (i >= 0) {
             t->s[i].graph = true;
             t->s[i].stream = 0;

@@ -176,3 +176,33 @@ def test_captured_launch_takes_the_static_walk(aeq, wl, cuda):
             g.replay()
             torch.cuda.synchronize()
             assert same(outs, ref)
+
+
+def test_many_graphs_leave_slots_for_streams(aeq, wl, cuda):
+    """Graphs reserve at most 48 of the 64 counters: with 56 graphs alive,
+    the extra graphs and a direct launch on a new stream still complete
+    every group."""
+    batch = Batch(aeq, wl, cuda, "unrolled_8_layers", seed=5)
+    ref = reference(aeq, batch, "fp16")
+    with walk(static=False):
+        graphs, outs = [], []
+        try:
+            for _ in range(56):
+                descs, o = batch.outputs()
+                graphs.append(aeq.FusedGraph(descs, aeq.make_tuning("fp16")))
+                outs.append(o)
+            for g in graphs[::5] + graphs[-3:]:
+                g.launch()
+            descs, direct = batch.outputs()
+            st = torch.cuda.Stream()
+            torch.cuda.synchronize()
+            with torch.cuda.stream(st):
+                aeq.pusch_eq_fused(descs, aeq.make_tuning("fp16"))
+            torch.cuda.synchronize()
+            for k, o in enumerate(outs):
+                if k % 5 == 0 or k >= 53:
+                    assert same(o, ref)
+            assert same(direct, ref)
+        finally:
+            for g in graphs:
+                g.close()
