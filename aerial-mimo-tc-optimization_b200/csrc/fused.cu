@@ -2101,8 +2101,9 @@ static WalkTable* walk_table_locked(std::unique_lock<std::mutex>& lk, int* devOu
 // The unrolled kernels (uniform batches) take the dynamic walk: they ask for
 // their next group a subcarrier ahead of needing it.  The mixed-tile kernels'
 // producer cursor would ask at the moment it stages the group, and on the
-// uneven 16-cell batch that measured slower (57.4-58.2 against 54.3 us), so
-// they keep the static walk.
+// uneven 16-cell batch that measured slower (57.4-58.2 against 54.3 us; with
+// the ticket taken a whole group ahead still 58.4 against 54.2 us), so they
+// keep the static walk.
 static bool walk_applies(const FusedParams& p) { return p.exactChunks != 0 && !p.halfMixed; }
 
 static bool walk_slot_idle(WalkSlot& w) {
@@ -2154,8 +2155,8 @@ int launch_fused(FusedParams& p, int warpBytes, int prec, LaunchShape sh, cudaSt
     int s = plan_fused(p, warpBytes, prec, sh, pl);
     if (s) return s;
     std::unique_lock<std::mutex> lk;
-    WalkTable* t = walk_table_locked(lk);
-    p.walkSlot = t && walk_applies(p) ? walk_slot_for_stream(t, st) : -1;
+    WalkTable* t = walk_applies(p) ? walk_table_locked(lk) : nullptr;
+    p.walkSlot = t ? walk_slot_for_stream(t, st) : -1;
     void* args[] = {&p};
     const cudaError_t e = cudaLaunchKernel(pl.func, pl.grid, pl.block, args, (size_t)pl.smem, st);
     if (e != cudaSuccess) return rt_status(e);
