@@ -191,6 +191,18 @@ def build_cells(wl, cfg: int, slots: int, rank: int, dev):
     raise ValueError(cfg)
 
 
+def work_walk(cells) -> str:
+    """How the timed launch hands groups of subcarriers to warps: uniform
+    batches of the unrolled kernels take tickets from a per-stream counter,
+    mixed batches (and every launch under AERIAL_STATIC_WALK=1) walk
+    round-robin.  Outputs are identical either way."""
+    shapes = {(c.nLayers, c.nAnt) for c in cells}
+    uniform = len(shapes) == 1 and cells[0].nLayers in (2, 4, 8, 16) and cells[0].nAnt in (32, 64, 128)
+    if uniform and os.environ.get("AERIAL_STATIC_WALK", "0") in ("", "0"):
+        return "dynamic: groups handed to warps from a per-stream counter"
+    return "static round-robin"
+
+
 def max_over_ranks(values, world: int, device=None):
     """Element-wise max of per-rank timings (ms) across the process group.
 
@@ -500,6 +512,7 @@ def main():
                                                          "ctas_per_sm": tun.ctas_per_sm},
                    "launch": "CUDA graph replay of the persistent launch" if graph is not None
                              else "one persistent launch per step",
+                   "work_walk": work_walk(cells),
                    "parallelism": f"independent cell-slots per GPU x{world}"},
         "roofline": roof,
         "cpu_baseline": cpu_base,
