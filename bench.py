@@ -436,6 +436,24 @@ def main():
             if not torch.equal(hL[i], llrs[i].cpu()):
                 raise RuntimeError(f"end-to-end LLRs of cell {i} differ from the resident launch")
         e2e["parity"] = "host-buffer LLRs equal the resident launch's (checked on the first and last cell)"
+        # the box's own host link: the step's inputs copied alone, one stream,
+        # from the same pinned buffers onto the device copies they came from
+        link_ms = []
+        for _ in range(2):
+            c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c0.record(stream)
+            with torch.cuda.stream(stream):
+                for c, h, y in zip(cells, hH, hY):
+                    c.H.copy_(h, non_blocking=True)
+                    c.Y.copy_(y, non_blocking=True)
+            c1.record(stream)
+            torch.cuda.synchronize()
+            link_ms.append(c0.elapsed_time(c1))
+        link_gbs = in_bytes_per_step / (min(link_ms) / 1e3) / 1e9
+        e2e["h2d_link_gbs"] = link_gbs
+        e2e["h2d_link_frac"] = in_bytes_per_step / (e2e_ms / k2 / 1e3) / 1e9 / link_gbs
+        e2e["link"] = ("h2d_link_gbs: the step's H and Y_rx copied alone from pinned memory on one stream; "
+                       "h2d_link_frac: the end-to-end step's input bytes per second over that")
 
     extras = {}
     cpu_base = None
