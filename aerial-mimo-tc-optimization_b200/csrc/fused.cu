@@ -1267,7 +1267,13 @@ __global__ void __launch_bounds__(256, LTF == 16 ? 1 : 2) fused_eq_kernel_a(cons
             for (int nt = 0; nt < 2; nt++)
 #pragma unroll
                 for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
-#pragma unroll
+        // The 16-layer tile's chunk body is large (three MMAs per product with
+        // BF16X3): fully unrolled over 8 chunks the loop outgrows the
+        // instruction cache (no_instruction stalls 0.88 cycles per issue on
+        // the precision-stress launch); unrolled by 2, same box,
+        // bit-identical: BF16X3 315.7 -> 299.5 us, FP16 256.4 -> 238.0 us
+        // (by 4: 303.5 and 248.2 us).
+#pragma unroll(LTF == 16 ? 2 : NCH)
         for (int k = 0; k < NCH; k++) {
             __syncwarp();                              // every lane is done with the slot refilled now
             const uint32_t pst = stBase + pslot * p.stageBytes;
