@@ -1270,10 +1270,10 @@ __global__ void __launch_bounds__(256, LTF == 16 ? 1 : 2) fused_eq_kernel_a(cons
         // The 16-layer tile's chunk body is large (three MMAs per product with
         // BF16X3): fully unrolled over 8 chunks the loop outgrows the
         // instruction cache (no_instruction stalls 0.88 cycles per issue on
-        // the precision-stress launch); unrolled by 2, same box,
-        // bit-identical: BF16X3 315.7 -> 299.5 us, FP16 256.4 -> 238.0 us
-        // (by 4: 303.5 and 248.2 us).
-#pragma unroll(LTF == 16 ? 2 : NCH)
+        // the precision-stress launch).  Same box, bit-identical, BF16X3 /
+        // FP16 operands: unrolled by 8 315.7 / 256.4 us, by 4 303.5 / 248.2,
+        // by 2 299.5 / 238.0, not unrolled 293-295 / 240 us.
+#pragma unroll(LTF == 16 ? 1 : NCH)
         for (int k = 0; k < NCH; k++) {
             __syncwarp();                              // every lane is done with the slot refilled now
             const uint32_t pst = stBase + pslot * p.stageBytes;
@@ -1485,7 +1485,10 @@ __global__ void __launch_bounds__(256, 2) fused_eq_kernel_h(const __grid_constan
             for (int nt = 0; nt < 2; nt++)
 #pragma unroll
                 for (int e = 0; e < 4; e++) zacc[mt][nt][e] = 0.f;
-#pragma unroll
+        // 16 layers: unrolled by 2 for the instruction cache (the 12-slot
+        // complex-half precision-stress launch 180.7 -> 174.6 us, same box,
+        // bit-identical)
+#pragma unroll(LTF == 16 ? 2 : NCH)
         for (int k = 0; k < NCH; k++) {
             __syncwarp();                              // every lane is done with the slot refilled now
             const uint32_t pst = stBase + pslot * p.stageBytes;
