@@ -1272,8 +1272,10 @@ __global__ void __launch_bounds__(256, LTF == 16 ? 1 : 2) fused_eq_kernel_a(cons
         // instruction cache (no_instruction stalls 0.88 cycles per issue on
         // the precision-stress launch).  Same box, bit-identical, BF16X3 /
         // FP16 operands: unrolled by 8 315.7 / 256.4 us, by 4 303.5 / 248.2,
-        // by 2 299.5 / 238.0, not unrolled 293-295 / 240 us.
-#pragma unroll(LTF == 16 ? 1 : NCH)
+        // by 2 299.5 / 238.0, not unrolled 293-295 / 240 us.  The 8-layer
+        // tile with 128 antennas (8 chunks) is unrolled by 4: 16 cells of
+        // 106 PRB, BF16X3 94.7-96.6 -> 92.6-92.8 us (FP16 88.5 us either way).
+#pragma unroll(LTF == 16 ? 1 : (LTF == 8 && NCH == 8 ? 4 : NCH))
         for (int k = 0; k < NCH; k++) {
             __syncwarp();                              // every lane is done with the slot refilled now
             const uint32_t pst = stBase + pslot * p.stageBytes;
