@@ -48,11 +48,11 @@ BATCHES = {
 class Batch:
     """Device inputs of a batch and one set of output buffers."""
 
-    def __init__(self, aeq, wl, cuda, kind, seed=0):
+    def __init__(self, aeq, wl, cuda, kind, seed=0, shapes=None):
         half = kind.startswith("half")
         self.aeq, self.cuda, self.half = aeq, cuda, half
         self.inputs = []
-        for i, (p, a, l, s, q) in enumerate(BATCHES[kind]):
+        for i, (p, a, l, s, q) in enumerate(shapes if shapes is not None else BATCHES[kind]):
             c = wl.make_cell(p, a, l, s, q, 25.0, seed=900 + 31 * i + seed)
             if half:
                 self.inputs.append((c, half_pairs(c.H).to(cuda), half_pairs(c.Y).to(cuda)))
@@ -110,18 +110,14 @@ def test_dynamic_walk_equals_static_walk_repeatedly(aeq, wl, cuda, kind, prec):
 def test_fewer_groups_than_warps(aeq, wl, cuda, shape):
     """Most warps have no group: they still count themselves done, so the
     counter resets and the next launch starts clean."""
-    BATCHES["_tiny"] = [shape]
-    try:
-        batch = Batch(aeq, wl, cuda, "_tiny")
-        ref = reference(aeq, batch, "fp16")
-        with walk(static=False):
-            for _ in range(4):
-                descs, outs = batch.outputs()
-                aeq.pusch_eq_fused(descs, aeq.make_tuning("fp16"))
-                torch.cuda.synchronize()
-                assert same(outs, ref)
-    finally:
-        del BATCHES["_tiny"]
+    batch = Batch(aeq, wl, cuda, "tiny", shapes=[shape])
+    ref = reference(aeq, batch, "fp16")
+    with walk(static=False):
+        for _ in range(4):
+            descs, outs = batch.outputs()
+            aeq.pusch_eq_fused(descs, aeq.make_tuning("fp16"))
+            torch.cuda.synchronize()
+            assert same(outs, ref)
 
 
 def test_concurrent_streams_and_graph_replays(aeq, wl, cuda):
